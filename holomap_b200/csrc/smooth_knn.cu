@@ -1,0 +1,233 @@
+// smooth_knn.cu -- smooth-kNN calibration (rho, sigma) on the device.
+//
+// Reference: src/smooth_knn.rs:23-80 (per-row rho, 64-step binary32 bisection,
+// MIN_K_DIST_SCALE floors), mean at :82-84, and libm::expf reached through
+// src/fmath.rs:119-122.
+//
+// One warp per row.  Lanes evaluate the row's exp terms in parallel; the
+// binary32 partial sum is then formed in the reference's order (j = 1, 2, ...,
+// k-1, each add rounded) by broadcasting the terms, so every lane holds the
+// same psum and all control flow is warp-uniform.  All arithmetic uses
+// explicitly rounded intrinsics and the file is compiled without FMA
+// contraction or flush-to-zero.
+#include <cuda_runtime.h>
+
+#include "hm_internal.cuh"
+
+namespace hm {
+
+// Device port of the libm crate's expf (the FreeBSD msun e_expf method): the
+// same constants and the same sequence of binary32 operations as the oracle's
+// restatement, each rounded to nearest.
+__device__ __forceinline__ float scalbnf_dev(float y, int n) {
+    if (n > 127) {
+        y = __fmul_rn(y, __uint_as_float(0x7f000000u));
+        n -= 127;
+        if (n > 127) {
+            y = __fmul_rn(y, __uint_as_float(0x7f000000u));
+            n -= 127;
+            if (n > 127) n = 127;
+        }
+    } else if (n < -126) {
+        y = __fmul_rn(y, __uint_as_float(0x0c800000u));  // 2^-102
+        n += 102;
+        if (n < -126) {
+            y = __fmul_rn(y, __uint_as_float(0x0c800000u));
+            n += 102;
+            if (n < -126) n = -126;
+        }
+    }
+    return __fmul_rn(y, __uint_as_float((uint32_t)(0x7f + n) << 23));
+}
+
+__device__ __forceinline__ float expf_libm(float x) {
+    const float ln2_hi = __uint_as_float(0x3f317200u);
+    const float ln2_lo = __uint_as_float(0x35bfbe8eu);
+    const float inv_ln2 = __uint_as_float(0x3fb8aa3bu);
+    const float p1 = __uint_as_float(0x3e2aaa8fu);
+    const float p2 = __uint_as_float(0xbb355215u);
+
+    const uint32_t bits = __float_as_uint(x);
+    const bool neg = (bits >> 31) != 0;
+    const uint32_t mag = bits & 0x7fffffffu;
+
+    if (mag >= 0x42aeac50u) {
+        if (mag > 0x7f800000u) return x;
+        if (!neg && mag >= 0x42b17218u) return __fmul_rn(x, __uint_as_float(0x7f000000u));
+        if (neg && mag >= 0x42cff1b5u) return 0.0f;
+    }
+    float hi, lo, r;
+    int k;
+    if (mag > 0x3eb17218u) {
+        if (mag > 0x3f851592u) {
+            float t = __fmul_rn(inv_ln2, x);
+            t = __fadd_rn(t, neg ? -0.5f : 0.5f);
+            k = __float2int_rz(t);
+        } else {
+            k = neg ? -1 : 1;
+        }
+        const float kf = __int2float_rn(k);
+        hi = __fsub_rn(x, __fmul_rn(kf, ln2_hi));
+        lo = __fmul_rn(kf, ln2_lo);
+        r = __fsub_rn(hi, lo);
+    } else if (mag > 0x39000000u) {
+        k = 0;
+        hi = x;
+        lo = 0.0f;
+        r = x;
+    } else {
+        return __fadd_rn(1.0f, x);
+    }
+    const float rr = __fmul_rn(r, r);
+    float poly = __fmul_rn(rr, p2);
+    poly = __fadd_rn(p1, poly);
+    poly = __fmul_rn(rr, poly);
+    const float c = __fsub_rn(r, poly);
+    const float num = __fmul_rn(r, c);
+    const float den = __fsub_rn(2.0f, c);
+    float q = __fdiv_rn(num, den);
+    q = __fsub_rn(q, lo);
+    q = __fadd_rn(q, hi);
+    const float y = __fadd_rn(1.0f, q);
+    return k == 0 ? y : scalbnf_dev(y, k);
+}
+
+// Row values are read per 32-element chunk from global memory (L1 resident
+// after the first pass).
+__global__ void __launch_bounds__(256) smooth_knn_kernel(const float *__restrict__ dists,
+                                                         uint32_t n, uint32_t k, double target,
+                                                         float *__restrict__ sigma,
+                                                         float *__restrict__ rho,
+                                                         uint32_t *__restrict__ zero_count,
+                                                         uint32_t *__restrict__ zero_rows) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (row >= n) return;
+    const float *v = dists + (size_t)row * k;
+    const uint32_t chunks = (k + 31) / 32;
+
+    // rho: first positive distance in row order, else 0 (src/smooth_knn.rs:35)
+    float rh = 0.0f;
+    for (uint32_t ch = 0; ch < chunks; ++ch) {
+        const uint32_t j = ch * 32 + lane;
+        const float x = (j < k) ? v[j] : 0.0f;
+        const unsigned m = __ballot_sync(0xffffffffu, x > 0.0f);
+        if (m) {
+            rh = __shfl_sync(0xffffffffu, x, __ffs(m) - 1);
+            break;
+        }
+    }
+
+    // bisection, binary32 state, hi seeded at f32::MAX (src/smooth_knn.rs:39-65)
+    const float f32max = __uint_as_float(0x7f7fffffu);
+    float lo = 0.0f, hi = f32max, mid = 1.0f;
+    for (int it = 0; it < 64; ++it) {
+        float psum = 0.0f;
+        for (uint32_t ch = 0; ch < chunks; ++ch) {
+            const uint32_t j = ch * 32 + lane;
+            float term = 0.0f;
+            if (j >= 1 && j < k) {
+                const float dd = __fsub_rn(v[j], rh);
+                term = (dd > 0.0f) ? expf_libm(-__fdiv_rn(dd, mid)) : 1.0f;
+            }
+            const uint32_t j_lo = (ch == 0) ? 1u : 0u;
+            const uint32_t j_hi = min(32u, k - ch * 32);
+            for (uint32_t l = j_lo; l < j_hi; ++l)
+                psum = __fadd_rn(psum, __shfl_sync(0xffffffffu, term, (int)l));
+        }
+        const double ps = (double)psum;
+        if (fabs(__dsub_rn(ps, target)) < 1e-5) break;
+        if (ps > target) {
+            hi = mid;
+            mid = __fdiv_rn(__fadd_rn(lo, hi), 2.0f);
+        } else {
+            lo = mid;
+            if (hi >= f32max)
+                mid = __fmul_rn(mid, 2.0f);
+            else
+                mid = __fdiv_rn(__fadd_rn(lo, hi), 2.0f);
+        }
+    }
+
+    float sg = mid;
+    if (rh > 0.0f) {
+        // floor = 1e-3 * mean(row), mean = f32(sequential f64 sum / k)
+        double s = 0.0;
+        for (uint32_t ch = 0; ch < chunks; ++ch) {
+            const uint32_t j = ch * 32 + lane;
+            const float x = (j < k) ? v[j] : 0.0f;
+            const uint32_t j_hi = min(32u, k - ch * 32);
+            for (uint32_t l = 0; l < j_hi; ++l)
+                s = __dadd_rn(s, (double)__shfl_sync(0xffffffffu, x, (int)l));
+        }
+        const float mean_row = __double2float_rn(__ddiv_rn(s, (double)k));
+        const float floor_v = __fmul_rn(1e-3f, mean_row);
+        if (sg < floor_v) sg = floor_v;
+    } else if (lane == 0) {
+        // floored later with the global mean (launch_mean_all_floor)
+        const uint32_t slot = atomicAdd(zero_count, 1u);
+        zero_rows[slot] = row;
+    }
+    if (lane == 0) {
+        sigma[row] = sg;
+        rho[row] = rh;
+    }
+}
+
+int launch_smooth_knn(const float *dists, uint32_t n, uint32_t k, double target, float *sigma,
+                      float *rho, uint32_t *zero_count, uint32_t *zero_rows, cudaStream_t s) {
+    HM_CUDA_TRY(cudaMemsetAsync(zero_count, 0, sizeof(uint32_t), s));
+    const int blocks = (int)((n + 7) / 8);
+    ScopedKernelTimer timer(HM_KCLASS_SMOOTH, s);
+    smooth_knn_kernel<<<blocks, 256, 0, s>>>(dists, n, k, target, sigma, rho, zero_count,
+                                             zero_rows);
+    HM_CUDA_TRY(cudaGetLastError());
+    count_launch();
+    return HM_OK;
+}
+
+// mean_all = f32(sequential binary64 sum of all n*k distances / (n*k))
+// (src/smooth_knn.rs:26, :82-84).  The reference's order is one dependent
+// chain, so one thread forms it; the other 255 threads stage the next values
+// through shared memory.  Runs only when some row had rho == 0.
+__global__ void __launch_bounds__(256) mean_all_floor_kernel(const float *__restrict__ dists,
+                                                             uint64_t total,
+                                                             const uint32_t *__restrict__ zero_count,
+                                                             const uint32_t *__restrict__ zero_rows,
+                                                             float *__restrict__ sigma) {
+    const uint32_t cnt = *zero_count;
+    if (cnt == 0) return;
+    __shared__ float stage[2][2048];
+    __shared__ float floor_v;
+    double s = 0.0;
+    const uint64_t chunk = 2048;
+    for (uint64_t base = 0; base < total; base += chunk) {
+        const int buf = (int)((base / chunk) & 1);
+        const uint64_t len = min(chunk, total - base);
+        for (uint64_t t = threadIdx.x; t < len; t += blockDim.x) stage[buf][t] = dists[base + t];
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (uint64_t t = 0; t < len; ++t) s = __dadd_rn(s, (double)stage[buf][t]);
+        // the double buffer lets the next fill overlap the chain; the barrier
+        // at the top of the iteration after next protects reuse
+    }
+    if (threadIdx.x == 0) {
+        const float mean_all = __double2float_rn(__ddiv_rn(s, (double)total));
+        floor_v = __fmul_rn(1e-3f, mean_all);
+    }
+    __syncthreads();
+    for (uint32_t t = threadIdx.x; t < cnt; t += blockDim.x) {
+        const uint32_t row = zero_rows[t];
+        if (sigma[row] < floor_v) sigma[row] = floor_v;
+    }
+}
+
+int launch_mean_all_floor(const float *dists, uint64_t total, const uint32_t *zero_count,
+                          const uint32_t *zero_rows, float *sigma, cudaStream_t s) {
+    mean_all_floor_kernel<<<1, 256, 0, s>>>(dists, total, zero_count, zero_rows, sigma);
+    HM_CUDA_TRY(cudaGetLastError());
+    count_launch();
+    return HM_OK;
+}
+
+}  // namespace hm

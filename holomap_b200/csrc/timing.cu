@@ -1,0 +1,94 @@
+// timing.cu -- launch counting and optional CUDA-event timing per kernel class.
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <mutex>
+#include <vector>
+
+#include "hm_internal.cuh"
+
+namespace hm {
+
+static std::atomic<uint64_t> g_launches{0};
+static std::atomic<bool> g_timing{false};
+
+struct Pending {
+    cudaEvent_t start, stop;
+};
+struct ClassTimes {
+    std::vector<Pending> pending;   // recorded, not yet read
+    std::vector<cudaEvent_t> open;  // starts waiting for their stop
+    double ms = 0.0;
+    uint64_t launches = 0;
+};
+static std::mutex g_mu;
+static ClassTimes g_classes[HM_KCLASS_COUNT];
+static std::vector<cudaEvent_t> g_free;
+
+void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+bool timing_enabled() { return g_timing.load(std::memory_order_relaxed); }
+
+static cudaEvent_t take_event() {
+    if (!g_free.empty()) {
+        cudaEvent_t e = g_free.back();
+        g_free.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void timing_record(int kclass, cudaStream_t s, bool start) {
+    if (kclass < 0 || kclass >= HM_KCLASS_COUNT) return;
+    std::lock_guard<std::mutex> lk(g_mu);
+    ClassTimes &c = g_classes[kclass];
+    if (start) {
+        cudaEvent_t e = take_event();
+        if (e && cudaEventRecord(e, s) == cudaSuccess) c.open.push_back(e);
+    } else if (!c.open.empty()) {
+        cudaEvent_t st = c.open.back();
+        c.open.pop_back();
+        cudaEvent_t e = take_event();
+        if (e && cudaEventRecord(e, s) == cudaSuccess) c.pending.push_back({st, e});
+    }
+}
+
+}  // namespace hm
+
+using namespace hm;
+
+extern "C" {
+
+int hm_timing_enable(int on) {
+    g_timing.store(on != 0);
+    return HM_OK;
+}
+
+int hm_timing_read(int kernel_class, double *total_ms, uint64_t *launches, int reset) {
+    if (kernel_class < 0 || kernel_class >= HM_KCLASS_COUNT)
+        return set_error(HM_ERR_INVALID, "unknown kernel class %d", kernel_class);
+    std::lock_guard<std::mutex> lk(g_mu);
+    ClassTimes &c = g_classes[kernel_class];
+    for (const Pending &p : c.pending) {
+        float ms = 0.f;
+        if (cudaEventSynchronize(p.stop) == cudaSuccess &&
+            cudaEventElapsedTime(&ms, p.start, p.stop) == cudaSuccess)
+            c.ms += ms;
+        c.launches += 1;
+        g_free.push_back(p.start);
+        g_free.push_back(p.stop);
+    }
+    c.pending.clear();
+    if (total_ms) *total_ms = c.ms;
+    if (launches) *launches = c.launches;
+    if (reset) {
+        c.ms = 0.0;
+        c.launches = 0;
+    }
+    return HM_OK;
+}
+
+uint64_t hm_launch_count(void) { return g_launches.load(); }
+
+}  // extern "C"

@@ -1,0 +1,166 @@
+/*
+ * holomap_cuda.h -- C ABI of libholomap_cuda.so, the B200 (sm_100a) exact kNN +
+ * smooth-kNN engine for holomap.
+ *
+ * The reference has no FFI on this path: its "operator API" is two
+ * crate-private Rust calls made back to back by Holomap::fit_transform,
+ *
+ *     exact_knn(data: &[f32], n_features, k, metric) -> Knn     src/knn.rs:22
+ *     smooth_knn(&knn.dists, k) -> SmoothKnn                     src/smooth_knn.rs:23
+ *
+ * called at src/api.rs:147-148 after the validation at src/api.rs:114-145.
+ * Every entry point below replaces one or both of those calls and returns the
+ * same arrays bit for bit: Knn{indices (u32), dists (f32)} row-major n x k
+ * (src/knn.rs:13-19) and SmoothKnn{sigmas, rhos} (src/smooth_knn.rs:16-19).
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  The caller allocates every output.
+ *   - Return HM_OK (0) or a negative HM_ERR_* code; hm_last_error() gives a
+ *     thread-local message.  Nothing aborts, nothing prints.
+ *   - Preconditions: d >= 1, 1 <= k <= n, every input finite (the domain of
+ *     exact_knn; fit_transform's validation at src/api.rs:114-145 is stricter,
+ *     k >= 2 and n > k).  Violations return HM_ERR_INVALID; a non-finite input
+ *     is reported with its first flat index, like HolomapError::NonFiniteInput
+ *     (src/api.rs:36-43).
+ *   - Host-pointer entry points are synchronous and thread-safe; they copy
+ *     the input to the device once and the outputs back once.
+ *   - Device-pointer entry points (suffix _device) are stream-ordered and
+ *     asynchronous; `stream` is a cudaStream_t passed as void*.
+ */
+#ifndef HOLOMAP_CUDA_H
+#define HOLOMAP_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HM_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define HM_API __attribute__((visibility("default")))
+#else
+#define HM_API
+#endif
+
+/* status codes */
+#define HM_OK 0
+#define HM_ERR_INVALID (-1)     /* argument outside the reference's preconditions */
+#define HM_ERR_OOM (-2)         /* device or pinned allocation failed */
+#define HM_ERR_CUDA (-3)        /* CUDA runtime / driver error */
+#define HM_ERR_TIMEOUT (-4)     /* a bounded device wait or hm_wait expired */
+#define HM_ERR_ADMISSION (-5)   /* serving: job larger than the context's memory budget */
+#define HM_ERR_UNSUPPORTED (-6) /* valid input this build does not handle (message says why) */
+#define HM_ERR_NOT_READY (-7)   /* serving: hm_poll on a job still in flight */
+
+/* metric, the reference's Metric enum (src/metric.rs:8-15) plus one extension */
+#define HM_METRIC_EUCLIDEAN 0
+#define HM_METRIC_COSINE 1
+#define HM_METRIC_MANHATTAN 2 /* extension: no reference metric (src/metric.rs:81) */
+
+/* how the N x N distance bulk is evaluated; every path returns the same bytes */
+#define HM_PATH_AUTO 0        /* autotuner table picks */
+#define HM_PATH_PLAIN 1       /* exact binary64 SIMT over every pair */
+#define HM_PATH_SCREEN_BF16 2 /* tcgen05 BF16 screen + exact rerank */
+#define HM_PATH_SCREEN_TF32 3 /* tcgen05 TF32 screen + exact rerank */
+#define HM_PATH_SCREEN_BF16X3 4 /* tcgen05 split-BF16 (hi*hi + hi*lo + lo*hi) screen + rerank */
+
+/* Optional per-call statistics (pass NULL to skip). */
+typedef struct hm_stats {
+    int32_t path_used;           /* HM_PATH_* actually run */
+    uint32_t col_splits;         /* plain path: column splits per row block */
+    uint64_t candidates_total;   /* screened paths: candidates reranked exactly */
+    uint32_t candidates_max_row; /* screened paths: most candidates in one row */
+    uint32_t candidate_cap;      /* screened paths: per-row candidate capacity */
+    uint64_t overflow_rows;      /* screened paths: rows sent to the exact path */
+    uint64_t zero_rho_rows;      /* rows whose sigma floor used the global mean */
+    double screen_band;          /* screened paths: largest keep band (distance units) */
+    double device_ms;            /* device time of the call's kernels */
+} hm_stats;
+
+/* ----------------------------------------------------------------------------
+ * Host-buffer entry points (synchronous)
+ * ------------------------------------------------------------------------- */
+
+/* Replaces exact_knn (src/knn.rs:22-55).  data: n x d row-major f32.
+ * idx_out / dist_out: n x k.  Row i lists its k nearest points (itself
+ * included, at distance exactly 0) ordered by (distance, index). */
+HM_API int hm_knn(const float *data, uint64_t n, uint32_t d, uint32_t k, int metric,
+           int path, uint32_t *idx_out, float *dist_out, hm_stats *stats);
+
+/* Replaces smooth_knn (src/smooth_knn.rs:23-80).  dists: n x k, each row
+ * ascending as exact_knn returns it.  sigma_out / rho_out: n. */
+HM_API int hm_smooth_knn(const float *dists, uint64_t n, uint32_t k, float *sigma_out,
+                  float *rho_out);
+
+/* Replaces both calls of src/api.rs:147-148 with one device round trip. */
+HM_API int hm_knn_smooth(const float *data, uint64_t n, uint32_t d, uint32_t k, int metric,
+                  int path, uint32_t *idx_out, float *dist_out, float *sigma_out,
+                  float *rho_out, hm_stats *stats);
+
+/* ----------------------------------------------------------------------------
+ * Device-pointer entry points (stream-ordered; same results as above)
+ * ------------------------------------------------------------------------- */
+
+/* Bytes of device scratch hm_knn_smooth_device needs for this problem. */
+HM_API size_t hm_workspace_bytes(uint64_t n, uint32_t d, uint32_t k, int metric, int path);
+
+/* Both stages on device memory.  d_sigma/d_rho may be NULL to skip
+ * smooth-kNN.  d_workspace: hm_workspace_bytes(...) bytes, 256-byte aligned.
+ * stats (optional) is filled only with what is known without a host sync
+ * (path, splits, cap); counts need hm_stats_from_workspace after the stream
+ * has been synchronised. */
+HM_API int hm_knn_smooth_device(const float *d_data, uint64_t n, uint32_t d, uint32_t k,
+                         int metric, int path, uint32_t *d_idx, float *d_dist,
+                         float *d_sigma, float *d_rho, void *d_workspace,
+                         size_t workspace_bytes, void *stream, hm_stats *stats);
+
+/* Reads the counters a finished hm_knn_smooth_device call left in its
+ * workspace (synchronous copy). */
+HM_API int hm_stats_from_workspace(const void *d_workspace, uint64_t n, uint32_t d, uint32_t k,
+                            int metric, int path, hm_stats *stats);
+
+/* smooth-kNN alone on device memory (src/smooth_knn.rs:23-80). d_workspace:
+ * hm_smooth_workspace_bytes(n) bytes. */
+HM_API size_t hm_smooth_workspace_bytes(uint64_t n);
+HM_API int hm_smooth_knn_device(const float *d_dists, uint64_t n, uint32_t k, float *d_sigma,
+                         float *d_rho, void *d_workspace, void *stream);
+
+/* ----------------------------------------------------------------------------
+ * Misc
+ * ------------------------------------------------------------------------- */
+
+/* Thread-local text of the last error on this thread ("" if none). */
+HM_API const char *hm_last_error(void);
+
+/* HM_ABI_VERSION of the loaded library. */
+HM_API int hm_abi_version(void);
+
+/* The path HM_PATH_AUTO resolves to for this problem (autotuner table). */
+HM_API int hm_autotune_path(uint64_t n, uint32_t d, uint32_t k, int metric);
+
+/* ----------------------------------------------------------------------------
+ * Instrumentation (no reference counterpart; the reference has no timers on
+ * this path).  With timing enabled the library records a CUDA event pair, on
+ * the launching stream, around every launch of each kernel class below.
+ * ------------------------------------------------------------------------- */
+#define HM_KCLASS_BULK 0   /* N x N distance bulk: plain kernel or tensor-core screen */
+#define HM_KCLASS_SELECT 1 /* split merge / exact rerank + select */
+#define HM_KCLASS_SMOOTH 2 /* smooth-kNN calibration */
+#define HM_KCLASS_PREP 3   /* input checks, binary64 copy, operand prep */
+#define HM_KCLASS_COUNT 4
+
+HM_API int hm_timing_enable(int on);
+/* Sum of event-timed milliseconds and launch count of one class since the
+ * last reset (synchronises the recorded events). */
+HM_API int hm_timing_read(int kernel_class, double *total_ms, uint64_t *launches, int reset);
+/* Kernels this library has launched since it was loaded (all classes). */
+HM_API uint64_t hm_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HOLOMAP_CUDA_H */

@@ -1,0 +1,37 @@
+"""Extract the reference's stage-1/2 golden vectors into tests/golden/.
+
+The reference (mnmal-ai/holomap) pins its kNN and smooth-kNN stages against
+umap-learn 0.5.12 fixtures, tests/fixtures/stage2_{blobs_euclidean,cosine,
+duplicates_euclidean}.json, produced by its dev/export_stage2_fixtures.py and
+asserted in src/fixture_parity.rs:42-99 (kNN indices exact; distances, rho and
+sigma within 1e-5 * (1 + |expected|)).  This script copies the keys that the
+kNN + smooth-kNN path consumes or produces (data, knn_indices, knn_dists,
+rhos, sigmas and the shape/metric header) so the tests can run where the
+reference checkout is absent.  Run it from the repository root with the
+reference checkout path as its only argument:
+
+    python tests/golden/make_golden.py /path/to/holomap
+"""
+import json
+import sys
+from pathlib import Path
+
+NAMES = ("blobs_euclidean", "cosine", "duplicates_euclidean")
+KEYS = ("name", "metric", "n_neighbors", "n_samples", "n_features", "data",
+        "knn_indices", "knn_dists", "rhos", "sigmas")
+
+
+def main(ref_root: str) -> None:
+    out_dir = Path(__file__).resolve().parent
+    for name in NAMES:
+        src = Path(ref_root) / "tests" / "fixtures" / f"stage2_{name}.json"
+        fixture = json.loads(src.read_text())
+        slim = {k: fixture[k] for k in KEYS}
+        slim["source"] = f"tests/fixtures/stage2_{name}.json (umap-learn 0.5.12 export)"
+        (out_dir / f"stage2_{name}.json").write_text(json.dumps(slim) + "\n")
+        print(f"stage2_{name}.json: n={slim['n_samples']} d={slim['n_features']} "
+              f"k={slim['n_neighbors']} metric={slim['metric']}")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

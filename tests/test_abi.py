@@ -1,0 +1,91 @@
+"""CPU checks of the C ABI: the library loads without a GPU, exports every
+symbol include/holomap_cuda.h declares, and rejects bad arguments the way the
+reference's validation does (src/api.rs:114-145) before touching a device."""
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import holomap_b200 as hm
+from holomap_b200 import _lib
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def declared_symbols():
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = h.read_text()
+        names |= set(re.findall(r"^HM_API\s+[^(]*?\b(hm_\w+)\s*\(", text, flags=re.M))
+    return names
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    assert {"hm_knn", "hm_smooth_knn", "hm_knn_smooth", "hm_last_error"} <= names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = hm.lib()
+    for name in sorted(declared_symbols()):
+        assert hasattr(lib, name), f"{name} declared in include/ but not exported"
+
+
+def test_python_binding_covers_every_symbol():
+    assert declared_symbols() <= set(_lib.SIGNATURES), "binding is missing a declared symbol"
+
+
+def test_abi_version():
+    assert hm.lib().hm_abi_version() == 1
+
+
+@pytest.mark.parametrize("n_features,k,msg", [
+    (0, 3, "not a positive multiple"),     # BadShape (src/api.rs:114-119)
+    (3, 3, "not a positive multiple"),     # 10 % 3 != 0
+    (1, 0, "n_neighbors must be >= 1"),
+    (1, 11, "need at least"),              # TooFewPoints (src/api.rs:135-141)
+])
+def test_invalid_arguments_are_rejected_without_a_device(n_features, k, msg):
+    with pytest.raises(hm.HolomapInvalidInput, match=msg):
+        hm.exact_knn(np.zeros(10, np.float32), n_features, k)
+
+
+def test_unknown_metric_rejected():
+    # FromStr rejects anything but euclidean/cosine(/manhattan here) (src/metric.rs:21-30)
+    with pytest.raises(ValueError):
+        hm.Metric.parse("chebyshev")
+    assert hm.Metric.parse("Cosine") is hm.Metric.COSINE
+    assert str(hm.Metric.EUCLIDEAN) == "euclidean"
+    lib = hm.lib()
+    x = np.zeros(12, np.float32)
+    rc = lib.hm_knn(x.ctypes.data, 4, 3, 2, 7, 0, None, None, None)
+    assert rc == hm.HM_ERR_INVALID
+    assert b"metric" in lib.hm_last_error()
+
+
+def test_k_above_256_is_unsupported_not_wrong():
+    lib = hm.lib()
+    x = np.zeros(300 * 2, np.float32)
+    rc = lib.hm_knn(x.ctypes.data, 300, 2, 257, 0, 1, None, None, None)
+    assert rc == hm.HM_ERR_UNSUPPORTED
+
+
+def test_workspace_sizes_are_plannable_on_cpu():
+    b1 = hm.workspace_bytes(1000, 50, 15, "euclidean", "plain")
+    b2 = hm.workspace_bytes(20000, 128, 15, "euclidean", "plain")
+    assert 0 < b1 < b2
+    # the binary64 copy dominates: n_pad x round_up(d, 16) x 8 bytes
+    assert b2 >= 20000 * 128 * 8
+
+
+def test_smooth_workspace_is_small():
+    assert hm.lib().hm_smooth_workspace_bytes(50000) < 50000 * 4 + 1024
+
+
+def test_null_outputs_rejected():
+    lib = hm.lib()
+    x = np.zeros(40, np.float32)
+    rc = lib.hm_knn(x.ctypes.data, 20, 2, 3, 0, 1, None, None, None)
+    assert rc == hm.HM_ERR_INVALID
