@@ -129,6 +129,8 @@ SIGNATURES = {
     "hm_timing_enable": (_i32, [_i32]),
     "hm_timing_read": (_i32, [_i32, _vp, _vp, _i32]),
     "hm_launch_count": (_u64, []),
+    "hm_knn_smooth_noalloc": (_i32, [_vp, _u64, _u32, _u32, _i32, _vp, _vp, _vp, _vp, _vp]),
+    "hm_noalloc_scratch_bytes": (_sz, []),
 }
 
 KCLASS = {"bulk": 0, "select": 1, "smooth": 2, "prep": 3}

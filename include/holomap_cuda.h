@@ -129,6 +129,31 @@ HM_API int hm_smooth_knn_device(const float *d_dists, uint64_t n, uint32_t k, fl
                          float *d_rho, void *d_workspace, void *stream);
 
 /* ----------------------------------------------------------------------------
+ * Allocation-free entry point.  No counterpart in the reference (its Rust
+ * path allocates its Vecs freely); this exists for callers that cannot call
+ * cudaMalloc: a plugin inside a host engine that has already reserved the
+ * card's memory for its own allocator, or a latency-bound request loop that
+ * must not call the allocator because cudaMalloc/cudaFree can block and
+ * synchronise the device.
+ * ------------------------------------------------------------------------- */
+
+/* Size of the fixed device scratch array inside the library (64 MiB).  Every
+ * GPU that loads the library holds it until the process exits. */
+#define HM_NOALLOC_SCRATCH_BYTES (64ull << 20)
+
+/* The same results as hm_knn_smooth_device on the plain path, with the
+ * caller's device inputs and outputs and no allocation of any kind: scratch
+ * comes from the library's static array.  Problems whose scratch
+ * (hm_workspace_bytes(..., HM_PATH_PLAIN)) exceeds HM_NOALLOC_SCRATCH_BYTES
+ * are rejected with HM_ERR_UNSUPPORTED.  The first call on a device looks up
+ * the array's device address (make it before any stream capture).  All calls
+ * share the array: calls that overlap on the GPU race on it. */
+HM_API int hm_knn_smooth_noalloc(const float *d_data, uint64_t n, uint32_t d, uint32_t k,
+                                 int metric, uint32_t *d_idx, float *d_dist, float *d_sigma,
+                                 float *d_rho, void *stream);
+HM_API size_t hm_noalloc_scratch_bytes(void);
+
+/* ----------------------------------------------------------------------------
  * Misc
  * ------------------------------------------------------------------------- */
 
