@@ -131,6 +131,7 @@ SIGNATURES = {
     "hm_launch_count": (_u64, []),
     "hm_knn_smooth_noalloc": (_i32, [_vp, _u64, _u32, _u32, _i32, _vp, _vp, _vp, _vp, _vp]),
     "hm_noalloc_scratch_bytes": (_sz, []),
+    "hm_debug_set_screen_dump": (_i32, [_vp]),
 }
 
 KCLASS = {"bulk": 0, "select": 1, "smooth": 2, "prep": 3}

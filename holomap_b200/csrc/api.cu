@@ -170,6 +170,8 @@ static int run_knn(const float *d_data, uint64_t n, uint32_t d, uint32_t k, int 
         a.partial = L.splits > 1 ? reinterpret_cast<uint64_t *>(ws + L.off_partial) : nullptr;
         a.idx_out = d_idx;
         a.dist_out = d_dist;
+        a.row_list = nullptr;
+        a.row_count = nullptr;
         HM_TRY(launch_plain_knn(a, metric, L.splits, s));
         if (L.splits > 1)
             HM_TRY(launch_merge_splits(a.partial, (uint32_t)n, k, L.splits, d_idx, d_dist, s));
@@ -259,7 +261,9 @@ static void fill_stats(hm_stats *st, const Layout &L, const Flags &f, uint64_t n
     st->candidates_total = f.screen.candidates;
     st->candidates_max_row = f.screen.max_row;
     st->overflow_rows = f.screen.overflow_rows;
-    st->screen_band = L.path == HM_PATH_PLAIN ? 0.0 : (double)f.screen.band_max;
+    float band = 0.f;
+    memcpy(&band, &f.screen.band_max_bits, sizeof band);
+    st->screen_band = L.path == HM_PATH_PLAIN ? 0.0 : (double)band;
     (void)n;
 }
 

@@ -154,6 +154,12 @@ struct PlainArgs {
     uint64_t *partial;    // [splits][rows][k] keys when splits > 1
     uint32_t *idx_out;    // [rows][k] (rows counted from row_begin)
     float *dist_out;
+    // Row-list mode (exact fallback of the screened path): when row_list is
+    // set, the query rows are row_list[0 .. *row_count) instead of
+    // [row_begin, row_end), outputs are indexed by the row itself, splits
+    // must be 1 and the grid strides over groups of PL_BM listed rows.
+    const uint32_t *row_list;
+    const uint32_t *row_count;
 };
 
 int kpl_for_k(uint32_t k);  // 1, 2, 4, 8 or 0 if k > 256
@@ -162,6 +168,8 @@ int kpl_for_k(uint32_t k);  // 1, 2, 4, 8 or 0 if k > 256
 int launch_prep_plain(const float *x, uint32_t n, uint32_t d, uint32_t ldd, uint32_t n_pad,
                       int metric, double *x64, double *rnorm, cudaStream_t s);
 int launch_plain_knn(const PlainArgs &a, int metric, uint32_t splits, cudaStream_t s);
+// Row-list mode with a persistent grid (the list length lives on the device).
+int launch_plain_knn_rows(const PlainArgs &a, int metric, cudaStream_t s);
 int launch_merge_splits(const uint64_t *partial, uint32_t rows, uint32_t k, uint32_t splits,
                         uint32_t *idx_out, float *dist_out, cudaStream_t s);
 

@@ -116,122 +116,147 @@ __global__ void __launch_bounds__(PL_THREADS, (KPL <= 2 ? 2 : 1))
     plain_knn_kernel(const PlainArgs a) {
     __shared__ double As[2][PL_BM][PL_BK + 1];
     __shared__ double Bs[2][PL_BN][PL_BK + 1];
+    __shared__ uint32_t s_rows[PL_BM];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const uint32_t row0 = a.row_begin + blockIdx.x * PL_BM;
     const uint32_t split = blockIdx.y;
     const uint32_t c_begin = split * a.split_cols;
     const uint32_t c_end = min(a.n, c_begin + a.split_cols);
     const uint32_t ldd = a.ldd;
+    const bool listed = a.row_list != nullptr;
+    const uint32_t n_groups =
+        listed ? (*a.row_count + PL_BM - 1) / PL_BM : (a.row_end - a.row_begin + PL_BM - 1) / PL_BM;
+    const uint32_t rows_total = a.row_end - a.row_begin;
 
-    WarpTopK<KPL> top[4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r) top[r].reset();
-
-    double rn_a[4];
-#pragma unroll
-    for (int r = 0; r < 4; ++r)
-        rn_a[r] = (METRIC == HM_METRIC_COSINE) ? a.rnorm[row0 + warp * 4 + r] : 0.0;
-
-    // loads of one stage: A 32x16 (2 per thread), B 128x16 (8 per thread)
-    auto load_stage = [&](int buf, uint32_t col0, uint32_t k0) {
-#pragma unroll
-        for (int p = 0; p < 2; ++p) {
-            const int lin = tid + p * PL_THREADS;
-            const int r = lin >> 4, c = lin & 15;
-            const double *src = a.x64 + (size_t)(row0 + r) * ldd + k0 + c;
-            const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&As[buf][r][c]);
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src));
-        }
-#pragma unroll
-        for (int p = 0; p < 8; ++p) {
-            const int lin = tid + p * PL_THREADS;
-            const int r = lin >> 4, c = lin & 15;
-            const double *src = a.x64 + (size_t)(col0 + r) * ldd + k0 + c;
-            const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&Bs[buf][r][c]);
-            asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src));
-        }
-        asm volatile("cp.async.commit_group;\n" ::);
-    };
-
-    const uint32_t nk = ldd / PL_BK;
-    for (uint32_t col0 = c_begin; col0 < c_end; col0 += PL_BN) {
-        double acc[4][4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r)
-#pragma unroll
-            for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
-
-        load_stage(0, col0, 0);
-        for (uint32_t kt = 0; kt < nk; ++kt) {
-            const int buf = kt & 1;
-            if (kt + 1 < nk) {
-                load_stage(buf ^ 1, col0, (kt + 1) * PL_BK);
-                asm volatile("cp.async.wait_group 1;\n" ::);
+    for (uint32_t grp = blockIdx.x; grp < n_groups; grp += (listed ? gridDim.x : n_groups)) {
+        // the 32 query rows of this group (0xffffffff: none)
+        if (tid < PL_BM) {
+            uint32_t r;
+            if (listed) {
+                const uint32_t at = grp * PL_BM + tid;
+                r = at < *a.row_count ? a.row_list[at] : 0xffffffffu;
             } else {
-                asm volatile("cp.async.wait_group 0;\n" ::);
+                r = a.row_begin + grp * PL_BM + tid;
+                if (r >= a.row_end) r = 0xffffffffu;
             }
-            __syncthreads();
-#pragma unroll
-            for (int kk = 0; kk < PL_BK; ++kk) {
-                double av[4], bv[4];
-#pragma unroll
-                for (int r = 0; r < 4; ++r) av[r] = As[buf][warp * 4 + r][kk];
-#pragma unroll
-                for (int c = 0; c < 4; ++c) bv[c] = Bs[buf][lane + 32 * c][kk];
-#pragma unroll
-                for (int r = 0; r < 4; ++r)
-#pragma unroll
-                    for (int c = 0; c < 4; ++c) acc[r][c] = pair_step<METRIC>(acc[r][c], av[r], bv[c]);
-            }
-            __syncthreads();
+            s_rows[tid] = r;
         }
+        __syncthreads();
 
-        // finish the 16 pairs and feed the keys to the rows' lists
-        double rn_b[4];
+        WarpTopK<KPL> top[4];
 #pragma unroll
-        for (int c = 0; c < 4; ++c)
-            rn_b[c] = (METRIC == HM_METRIC_COSINE) ? a.rnorm[col0 + lane + 32 * c] : 0.0;
+        for (int r = 0; r < 4; ++r) top[r].reset();
+        uint32_t my_rows[4];
+        double rn_a[4];
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
-            const uint32_t row = row0 + warp * 4 + r;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const uint32_t col = col0 + lane + 32 * c;
-                float dist = pair_finish<METRIC>(acc[r][c], rn_a[r], rn_b[c]);
-                if (col == row) dist = 0.0f;  // src/knn.rs:38-39
-                const uint64_t key = (col < c_end) ? make_key(dist, col) : KEY_NONE;
-                top[r].offer(key, a.k, lane);
-            }
+            my_rows[r] = s_rows[warp * 4 + r];
+            rn_a[r] = (METRIC == HM_METRIC_COSINE && my_rows[r] != 0xffffffffu)
+                          ? a.rnorm[my_rows[r]] : 0.0;
         }
-    }
 
-    // write the first k elements of each valid row
-    const uint32_t rows = a.row_end - a.row_begin;
+        // loads of one stage: A 32x16 (2 per thread), B 128x16 (8 per thread)
+        auto load_stage = [&](int buf, uint32_t col0, uint32_t k0) {
 #pragma unroll
-    for (int r = 0; r < 4; ++r) {
-        const uint32_t row = row0 + warp * 4 + r;
-        if (row >= a.row_end) continue;
-        const size_t orow = row - a.row_begin;
+            for (int p = 0; p < 2; ++p) {
+                const int lin = tid + p * PL_THREADS;
+                const int r = lin >> 4, c = lin & 15;
+                const uint32_t ar = s_rows[r] == 0xffffffffu ? 0u : s_rows[r];
+                const double *src = a.x64 + (size_t)ar * ldd + k0 + c;
+                const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&As[buf][r][c]);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src));
+            }
 #pragma unroll
-        for (int q = 0; q < KPL; ++q) {
-            const uint32_t e = q * 32 + lane;
-            if (e >= a.k) continue;
-            const uint64_t key = top[r].v[q];
-            if (a.partial) {
-                a.partial[((size_t)split * rows + orow) * a.k + e] = key;
-            } else {
-                a.idx_out[orow * a.k + e] = key_idx(key);
-                a.dist_out[orow * a.k + e] = key_dist(key);
+            for (int p = 0; p < 8; ++p) {
+                const int lin = tid + p * PL_THREADS;
+                const int r = lin >> 4, c = lin & 15;
+                const double *src = a.x64 + (size_t)(col0 + r) * ldd + k0 + c;
+                const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&Bs[buf][r][c]);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src));
+            }
+            asm volatile("cp.async.commit_group;\n" ::);
+        };
+
+        const uint32_t nk = ldd / PL_BK;
+        for (uint32_t col0 = c_begin; col0 < c_end; col0 += PL_BN) {
+            double acc[4][4];
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[r][c] = 0.0;
+
+            load_stage(0, col0, 0);
+            for (uint32_t kt = 0; kt < nk; ++kt) {
+                const int buf = kt & 1;
+                if (kt + 1 < nk) {
+                    load_stage(buf ^ 1, col0, (kt + 1) * PL_BK);
+                    asm volatile("cp.async.wait_group 1;\n" ::);
+                } else {
+                    asm volatile("cp.async.wait_group 0;\n" ::);
+                }
+                __syncthreads();
+#pragma unroll
+                for (int kk = 0; kk < PL_BK; ++kk) {
+                    double av[4], bv[4];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r) av[r] = As[buf][warp * 4 + r][kk];
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) bv[c] = Bs[buf][lane + 32 * c][kk];
+#pragma unroll
+                    for (int r = 0; r < 4; ++r)
+#pragma unroll
+                        for (int c = 0; c < 4; ++c)
+                            acc[r][c] = pair_step<METRIC>(acc[r][c], av[r], bv[c]);
+                }
+                __syncthreads();
+            }
+
+            // finish the 16 pairs and feed the keys to the rows' lists
+            double rn_b[4];
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+                rn_b[c] = (METRIC == HM_METRIC_COSINE) ? a.rnorm[col0 + lane + 32 * c] : 0.0;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const uint32_t col = col0 + lane + 32 * c;
+                    float dist = pair_finish<METRIC>(acc[r][c], rn_a[r], rn_b[c]);
+                    if (col == my_rows[r]) dist = 0.0f;  // src/knn.rs:38-39
+                    const uint64_t key = (col < c_end) ? make_key(dist, col) : KEY_NONE;
+                    top[r].offer(key, a.k, lane);
+                }
             }
         }
+
+        // write the first k elements of each valid row
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const uint32_t row = my_rows[r];
+            if (row == 0xffffffffu) continue;
+            const size_t orow = listed ? row : row - a.row_begin;
+#pragma unroll
+            for (int q = 0; q < KPL; ++q) {
+                const uint32_t e = q * 32 + lane;
+                if (e >= a.k) continue;
+                const uint64_t key = top[r].v[q];
+                if (a.partial) {
+                    a.partial[((size_t)split * rows_total + orow) * a.k + e] = key;
+                } else {
+                    a.idx_out[orow * a.k + e] = key_idx(key);
+                    a.dist_out[orow * a.k + e] = key_dist(key);
+                }
+            }
+        }
+        __syncthreads();  // s_rows is rewritten by the next group
     }
 }
 
 template <int METRIC>
-static int launch_plain_metric(const PlainArgs &a, uint32_t splits, cudaStream_t s) {
+static int launch_plain_metric(const PlainArgs &a, uint32_t splits, cudaStream_t s,
+                               uint32_t grid_x = 0) {
     const uint32_t rows = a.row_end - a.row_begin;
-    dim3 grid((rows + PL_BM - 1) / PL_BM, splits);
+    dim3 grid(grid_x ? grid_x : (rows + PL_BM - 1) / PL_BM, splits);
     ScopedKernelTimer timer(HM_KCLASS_BULK, s);
     switch (kpl_for_k(a.k)) {
     case 1: plain_knn_kernel<METRIC, 1><<<grid, PL_THREADS, 0, s>>>(a); break;
@@ -243,6 +268,23 @@ static int launch_plain_metric(const PlainArgs &a, uint32_t splits, cudaStream_t
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();
     return HM_OK;
+}
+
+int launch_plain_knn_rows(const PlainArgs &a, int metric, cudaStream_t s) {
+    PlainArgs b = a;
+    b.partial = nullptr;
+    b.split_cols = (uint32_t)round_up(a.n, PL_BN);
+    b.row_begin = 0;
+    b.row_end = a.n;
+    // persistent grid: groups of listed rows are strided over 2 CTAs per SM
+    const uint32_t groups = (a.n + PL_BM - 1) / PL_BM;
+    const uint32_t ctas = groups < 296 ? groups : 296;
+    switch (metric) {
+    case HM_METRIC_EUCLIDEAN: return launch_plain_metric<HM_METRIC_EUCLIDEAN>(b, 1, s, ctas);
+    case HM_METRIC_COSINE: return launch_plain_metric<HM_METRIC_COSINE>(b, 1, s, ctas);
+    case HM_METRIC_MANHATTAN: return launch_plain_metric<HM_METRIC_MANHATTAN>(b, 1, s, ctas);
+    default: return set_error(HM_ERR_INVALID, "unknown metric %d", metric);
+    }
 }
 
 int launch_plain_knn(const PlainArgs &a, int metric, uint32_t splits, cudaStream_t s) {

@@ -1,0 +1,163 @@
+// rerank.cu -- exact rerank of the screen's candidates.
+//
+// One warp per query row.  The row's final screen threshold is the smallest
+// of its parts' k-th screened values (each is an upper bound of the row's
+// k-th); candidates with c^ <= tau + band are compacted into shared memory,
+// and each lane then evaluates one candidate's distance exactly as the
+// reference does (src/metric.rs:42-53 euclidean, :58-70 cosine: binary64,
+// dimension order, no contraction, self forced to 0 as in src/knn.rs:38-39),
+// feeding the (distance bits, index) keys to a warp top-k list.  Rows whose
+// candidate list overflowed, or that the screen cannot bound (zero vectors
+// under cosine), are appended to the overflow list for the exact plain path.
+#include <cuda_runtime.h>
+
+#include "hm_internal.cuh"
+#include "screen.cuh"
+
+namespace hm {
+
+constexpr int RR_WARPS = 8;
+constexpr int RR_LIST = 256;  // compacted candidates per warp between flushes
+
+template <int METRIC>
+__device__ __forceinline__ float exact_distance(const double *__restrict__ xi,
+                                                const float *__restrict__ xj, uint32_t d,
+                                                double rn_i, double rn_j) {
+    double acc = 0.0;
+    if (METRIC == HM_METRIC_EUCLIDEAN) {
+        for (uint32_t t = 0; t < d; ++t) {
+            const double diff = __dsub_rn(xi[t], (double)__ldg(xj + t));
+            acc = __dadd_rn(acc, __dmul_rn(diff, diff));
+        }
+        return __double2float_rn(__dsqrt_rn(acc));
+    } else {
+        for (uint32_t t = 0; t < d; ++t) acc = __dadd_rn(acc, __dmul_rn(xi[t], (double)__ldg(xj + t)));
+        const double q = __ddiv_rn(acc, __dmul_rn(rn_i, rn_j));
+        const double r = __dsub_rn(1.0, q);
+        return (r > 0.0) ? __double2float_rn(r) : 0.0f;
+    }
+}
+
+template <int METRIC, int KPL>
+__global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs a, uint32_t dstride) {
+    extern __shared__ double rr_smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t row = blockIdx.x * RR_WARPS + warp;
+    if (row >= a.n) return;
+    double *xi = rr_smem + (size_t)warp * dstride;
+    uint32_t *list = reinterpret_cast<uint32_t *>(rr_smem + (size_t)RR_WARPS * dstride) + warp * RR_LIST;
+
+    // overflow / unbounded rows go to the exact plain path
+    bool ovf = a.force_exact[row] != 0;
+    float tau = __int_as_float(0x7f800000);
+    for (uint32_t p = 0; p < a.parts; ++p) {
+        const size_t slot = (size_t)row * a.parts + p;
+        ovf |= a.cand_cnt[slot] > a.cap;
+        tau = fminf(tau, a.part_tau[slot]);
+    }
+    if (ovf) {
+        if (lane == 0) {
+            const uint32_t at = atomicAdd(a.ovf_cnt, 1u);
+            a.ovf_list[at] = row;
+            atomicAdd(&a.counters->overflow_rows, 1u);
+        }
+        return;
+    }
+    const float thr = __fadd_ru(tau, a.band[row]);
+
+    for (uint32_t t = lane; t < a.d; t += 32) xi[t] = (double)a.x[(size_t)row * a.d + t];
+    __syncwarp();
+    const double rn_i = (METRIC == HM_METRIC_COSINE) ? a.rnorm[row] : 0.0;
+
+    WarpTopK<KPL> top;
+    top.reset();
+    uint32_t fill = 0, kept = 0;
+    const unsigned lt_mask = (1u << lane) - 1u;
+
+    auto flush = [&](uint32_t m) {
+        for (uint32_t b = 0; b < m; b += 32) {
+            uint64_t key = KEY_NONE;
+            if (b + lane < m) {
+                const uint32_t j = list[b + lane];
+                const float dist =
+                    (j == row) ? 0.0f
+                               : exact_distance<METRIC>(xi, a.x + (size_t)j * a.d, a.d, rn_i,
+                                                        METRIC == HM_METRIC_COSINE ? a.rnorm[j] : 0.0);
+                key = make_key(dist, j);
+            }
+            top.offer(key, a.k, lane);
+        }
+        __syncwarp();
+    };
+
+    for (uint32_t p = 0; p < a.parts; ++p) {
+        const size_t slot = (size_t)row * a.parts + p;
+        const uint32_t cnt = a.cand_cnt[slot];
+        const unsigned long long *cand = a.cand + slot * a.cap;
+        for (uint32_t e0 = 0; e0 < cnt; e0 += 32) {
+            bool pass = false;
+            uint32_t j = 0;
+            if (e0 + lane < cnt) {
+                const unsigned long long c = cand[e0 + lane];
+                const float cv = __uint_as_float((uint32_t)(c >> 32));
+                j = (uint32_t)c;
+                pass = !(cv > thr);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, pass);
+            if (pass) list[fill + __popc(m & lt_mask)] = j;
+            fill += __popc(m);
+            kept += __popc(m);
+            __syncwarp();
+            if (fill > RR_LIST - 32) {
+                flush(fill);
+                fill = 0;
+            }
+        }
+    }
+    flush(fill);
+
+#pragma unroll
+    for (int q = 0; q < KPL; ++q) {
+        const uint32_t e = q * 32 + lane;
+        if (e < a.k) {
+            a.idx_out[(size_t)row * a.k + e] = key_idx(top.v[q]);
+            a.dist_out[(size_t)row * a.k + e] = key_dist(top.v[q]);
+        }
+    }
+    if (lane == 0) {
+        atomicAdd(&a.counters->candidates, (unsigned long long)kept);
+        atomicMax(&a.counters->max_row, kept);
+    }
+}
+
+template <int METRIC>
+static int launch_metric(const RerankArgs &a, uint32_t kpl, cudaStream_t s) {
+    const uint32_t dstride = (uint32_t)round_up(a.d, 2);
+    const size_t smem = (size_t)RR_WARPS * dstride * sizeof(double) + RR_WARPS * RR_LIST * sizeof(uint32_t);
+    const int blocks = (int)((a.n + RR_WARPS - 1) / RR_WARPS);
+#define HM_RR_CASE(K)                                                                       \
+    case K: {                                                                               \
+        HM_CUDA_TRY(cudaFuncSetAttribute(rerank_kernel<METRIC, K>,                          \
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+        rerank_kernel<METRIC, K><<<blocks, RR_WARPS * 32, smem, s>>>(a, dstride);           \
+        break;                                                                              \
+    }
+    switch (kpl) {
+        HM_RR_CASE(1)
+        HM_RR_CASE(2)
+    default: return set_error(HM_ERR_UNSUPPORTED, "rerank width %u", kpl);
+    }
+#undef HM_RR_CASE
+    HM_CUDA_TRY(cudaGetLastError());
+    count_launch();
+    return HM_OK;
+}
+
+int launch_rerank(const RerankArgs &a, int metric, uint32_t kpl, cudaStream_t s) {
+    ScopedKernelTimer timer(HM_KCLASS_SELECT, s);
+    if (metric == HM_METRIC_EUCLIDEAN) return launch_metric<HM_METRIC_EUCLIDEAN>(a, kpl, s);
+    if (metric == HM_METRIC_COSINE) return launch_metric<HM_METRIC_COSINE>(a, kpl, s);
+    return set_error(HM_ERR_UNSUPPORTED, "metric %d has no screened path", metric);
+}
+
+}  // namespace hm

@@ -1,0 +1,412 @@
+// screen_gemm.cu -- the tensor-core screen: U U^T on tcgen05 with TMEM
+// accumulators, fused with a per-row running top-k threshold and candidate
+// emission, so the N x N similarity matrix never leaves the SM.
+//
+// One CTA per SM (persistent), 6 warps:
+//   warp 0     TMA producer: 128-row A slice + 256-row B slice per stage
+//              (128-byte K slices, 128B swizzle, 4-stage mbarrier ring; no
+//              cluster multicast),
+//   warp 1     allocates 512 TMEM columns (two 128 x 256 fp32 accumulators)
+//              and issues tcgen05.mma (one thread) + tcgen05.commit,
+//   warps 2-5  epilogue: each thread owns one query row (its TMEM lane),
+//              reads its 256 accumulator columns with tcgen05.ld, forms the
+//              screened value c^ in binary32, keeps a sorted register array of
+//              its k smallest c^ (threshold tau) and emits every column with
+//              c^ <= tau + band_i into the row's candidate list.
+// Work units are (row block of 128, column part); the columns of a unit are
+// walked in 256-wide tiles with the two accumulators double buffered, so the
+// epilogue of one tile overlaps the MMAs of the next.
+//
+// Every wait on an mbarrier is bounded (wall clock via %globaltimer and an
+// iteration cap): on expiry the CTA records an error code, stops issuing,
+// waits (bounded) for its own copies and MMAs, frees TMEM and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "hm_internal.cuh"
+#include "screen.cuh"
+
+namespace hm {
+
+constexpr uint32_t SC_A_BYTES = SC_BM * SC_SLICE_BYTES;  // 16 KB
+constexpr uint32_t SC_B_BYTES = SC_BN * SC_SLICE_BYTES;  // 32 KB
+constexpr uint32_t SC_SMEM_BYTES = 1024 + SC_STAGES * (SC_A_BYTES + SC_B_BYTES) + 256;
+constexpr uint32_t SC_TMEM_COLS = 512;
+constexpr uint64_t SC_WAIT_LIMIT_NS = 4000000000ull;  // 4 s
+constexpr uint64_t SC_DRAIN_LIMIT_NS = 200000000ull;  // 0.2 s for copies already in flight
+constexpr uint32_t SC_WAIT_SPIN_CAP = 1u << 30;
+
+enum : uint32_t {
+    SC_ERR_PRODUCER = 1,
+    SC_ERR_MMA_FULL = 2,
+    SC_ERR_MMA_ACC = 3,
+    SC_ERR_EPILOGUE = 4,
+    SC_ERR_DRAIN = 5,
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase of parity `parity` to complete.  Gives up when
+// another role has raised the abort flag (unless draining) or after the
+// time / iteration limits.
+__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile uint32_t *abort_flag,
+                                       bool draining = false) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer_ns();
+    const uint64_t limit = draining ? SC_DRAIN_LIMIT_NS : SC_WAIT_LIMIT_NS;
+    for (uint32_t spin = 1; spin < SC_WAIT_SPIN_CAP; ++spin) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if ((spin & 31) == 0) {
+            if (!draining && *abort_flag) return false;
+            if (globaltimer_ns() - t0 > limit) return false;
+        }
+    }
+    return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, uint32_t bar,
+                                            int32_t x, int32_t y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_before_sync() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_after_sync() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// Shared-memory matrix descriptor: K-major operand, 128-byte swizzle, rows
+// of 128 bytes stored back to back (8-row groups 1024 bytes apart).
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+    return (uint64_t)((addr >> 4) & 0x3fffu)  // start address
+           | ((uint64_t)1 << 16)              // leading byte offset (unused for SW128 K-major)
+           | ((uint64_t)(1024 >> 4) << 32)    // stride byte offset: 8 rows x 128 B
+           | ((uint64_t)1 << 46)              // descriptor version (sm_100)
+           | ((uint64_t)2 << 61);             // swizzle mode: 128B
+}
+
+template <int KIND>
+__device__ __forceinline__ void mma_issue(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accum) {
+    if (KIND == SCREEN_KIND_BF16) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
+            : "memory");
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+            "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
+            : "memory");
+    }
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32"
+        " {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15,"
+        " %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31},"
+        " [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+          "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
+          "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
+          "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void raise_error(volatile uint32_t *abort_flag, uint32_t *error_code,
+                                            uint32_t code) {
+    *abort_flag = 1;
+    atomicCAS(error_code, 0u, code);
+}
+
+struct UnitTiles {
+    uint32_t rb, part, ct_begin, ct_end;
+};
+
+__device__ __forceinline__ UnitTiles unit_tiles(const ScreenGemmArgs &g, uint32_t u) {
+    UnitTiles t;
+    t.rb = u / g.parts;
+    t.part = u % g.parts;
+    t.ct_begin = t.part * g.part_tiles;
+    t.ct_end = min(g.col_tiles, t.ct_begin + g.part_tiles);
+    return t;
+}
+
+template <int KIND, int KP>
+__global__ void __launch_bounds__(SC_THREADS, 1)
+    screen_gemm_kernel(const __grid_constant__ CUtensorMap tma, const __grid_constant__ CUtensorMap tmb,
+                       const ScreenGemmArgs g) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
+                                                ~(uintptr_t)1023);
+    uint8_t *sA = smem;
+    uint8_t *sB = smem + SC_STAGES * SC_A_BYTES;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(sB + SC_STAGES * SC_B_BYTES);
+    uint64_t *full = bars;                  // [SC_STAGES]
+    uint64_t *empty = bars + SC_STAGES;     // [SC_STAGES]
+    uint64_t *accf = bars + 2 * SC_STAGES;  // [2]
+    uint64_t *acce = accf + 2;              // [2]
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acce + 2);
+    volatile uint32_t *abort_flag = tmem_slot + 1;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < SC_STAGES; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&accf[b]), 1);
+            mbar_init(smem_u32(&acce[b]), 4);
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(tmem_slot)),
+                     "r"(SC_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0) {
+        // ------------------------------------------------------ TMA producer
+        if (lane == 0) {
+            uint32_t it = 0;
+            bool ok = true;
+            for (uint32_t u = blockIdx.x; ok && u < g.units; u += gridDim.x) {
+                const UnitTiles ut = unit_tiles(g, u);
+                for (uint32_t ct = ut.ct_begin; ok && ct < ut.ct_end; ++ct) {
+                    for (uint32_t ks = 0; ks < g.k_stages; ++ks, ++it) {
+                        const uint32_t s = it % SC_STAGES, r = it / SC_STAGES;
+                        if (!mbar_wait(smem_u32(&empty[s]), (r & 1) ^ 1, abort_flag)) {
+                            raise_error(abort_flag, g.error_code, SC_ERR_PRODUCER);
+                            ok = false;
+                            break;
+                        }
+                        const uint32_t fb = smem_u32(&full[s]);
+                        mbar_arrive_expect_tx(fb, SC_A_BYTES + SC_B_BYTES);
+                        const int32_t kx = (int32_t)(ks * (SC_SLICE_BYTES / (KIND == SCREEN_KIND_BF16 ? 2 : 4)));
+                        tma_load_2d(smem_u32(sA + s * SC_A_BYTES), &tma, fb, kx, (int32_t)(ut.rb * SC_BM));
+                        tma_load_2d(smem_u32(sB + s * SC_B_BYTES), &tmb, fb, kx, (int32_t)(ct * SC_BN));
+                    }
+                }
+            }
+            // drain: every issued stage must have landed before the CTA exits
+            const uint32_t issued = it;
+            for (uint32_t t = issued > SC_STAGES ? issued - SC_STAGES : 0; t < issued; ++t) {
+                const uint32_t s = t % SC_STAGES, r = t / SC_STAGES;
+                if (!mbar_wait(smem_u32(&full[s]), r & 1, abort_flag, true)) {
+                    raise_error(abort_flag, g.error_code, SC_ERR_DRAIN);
+                    break;
+                }
+            }
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ------------------------------------------------------- MMA issuer
+        if (lane == 0) {
+            uint32_t it = 0, tile = 0;
+            bool ok = true;
+            constexpr uint32_t kM = SC_BM, kN = SC_BN;
+            for (uint32_t u = blockIdx.x; ok && u < g.units; u += gridDim.x) {
+                const UnitTiles ut = unit_tiles(g, u);
+                for (uint32_t ct = ut.ct_begin; ok && ct < ut.ct_end; ++ct, ++tile) {
+                    const uint32_t buf = tile & 1, use = tile >> 1;
+                    if (!mbar_wait(smem_u32(&acce[buf]), (use & 1) ^ 1, abort_flag)) {
+                        raise_error(abort_flag, g.error_code, SC_ERR_MMA_ACC);
+                        ok = false;
+                        break;
+                    }
+                    fence_after_sync();
+                    const uint32_t d_tmem = tmem_base + buf * kN;
+                    for (uint32_t ks = 0; ks < g.k_stages; ++ks, ++it) {
+                        const uint32_t s = it % SC_STAGES, r = it / SC_STAGES;
+                        if (!mbar_wait(smem_u32(&full[s]), r & 1, abort_flag)) {
+                            raise_error(abort_flag, g.error_code, SC_ERR_MMA_FULL);
+                            ok = false;
+                            break;
+                        }
+                        fence_after_sync();
+                        const uint32_t a0 = smem_u32(sA + s * SC_A_BYTES);
+                        const uint32_t b0 = smem_u32(sB + s * SC_B_BYTES);
+#pragma unroll
+                        for (uint32_t kk = 0; kk < SC_SLICE_BYTES / 32; ++kk)
+                            mma_issue<KIND>(d_tmem, smem_desc(a0 + kk * 32), smem_desc(b0 + kk * 32),
+                                            g.idesc, (ks | kk) != 0);
+                        mma_commit(smem_u32(&empty[s]));
+                    }
+                    if (!ok) break;
+                    mma_commit(smem_u32(&accf[buf]));
+                    (void)kM;
+                }
+            }
+            // drain: the last commit must have landed before TMEM is freed
+            if (it > 0) {
+                const uint32_t s = (it - 1) % SC_STAGES, r = (it - 1) / SC_STAGES;
+                if (!mbar_wait(smem_u32(&empty[s]), r & 1, abort_flag, true))
+                    raise_error(abort_flag, g.error_code, SC_ERR_DRAIN);
+            }
+        }
+        __syncwarp();
+    } else {
+        // --------------------------------------------------------- epilogue
+        const uint32_t quad = (uint32_t)(warp & 3);  // TMEM lane quadrant of this warp
+        const uint32_t row_in_tile = quad * 32 + lane;
+        const float INF = __int_as_float(0x7f800000);
+        uint32_t tile = 0;
+        bool ok = true;
+        for (uint32_t u = blockIdx.x; ok && u < g.units; u += gridDim.x) {
+            const UnitTiles ut = unit_tiles(g, u);
+            const uint32_t row = ut.rb * SC_BM + row_in_tile;
+            const bool valid = row < g.n;
+            float arr[KP];
+#pragma unroll
+            for (int q = 0; q < KP; ++q) arr[q] = (q < KP - (int)g.k) ? -INF : INF;
+            const float band = valid ? g.band[row] : 0.0f;
+            const float rowterm = (valid && g.rowterm) ? g.rowterm[row] : 0.0f;
+            float thr = INF;
+            uint32_t cnt = 0;
+            const size_t slot = ((size_t)row * g.parts + ut.part);
+            unsigned long long *cand = g.cand + slot * g.cap;
+
+            for (uint32_t ct = ut.ct_begin; ct < ut.ct_end; ++ct, ++tile) {
+                const uint32_t buf = tile & 1, use = tile >> 1;
+                if (!mbar_wait(smem_u32(&accf[buf]), use & 1, abort_flag)) {
+                    raise_error(abort_flag, g.error_code, SC_ERR_EPILOGUE);
+                    ok = false;
+                    break;
+                }
+                fence_after_sync();
+                for (uint32_t ch = 0; ch < SC_BN / 32; ++ch) {
+                    const uint32_t col0 = ct * SC_BN + ch * 32;
+                    if (col0 >= g.n) break;  // uniform over the CTA
+                    uint32_t v[32];
+                    tmem_ld32(tmem_base + ((quad * 32) << 16) + buf * SC_BN + ch * 32, v);
+                    const uint32_t my_col = col0 + lane;
+                    const float ct_mine = my_col < g.n ? g.colterm[my_col] : 0.0f;
+#pragma unroll
+                    for (int t = 0; t < 32; ++t) {
+                        const uint32_t j = col0 + t;
+                        const float cj = __shfl_sync(0xffffffffu, ct_mine, t);
+                        if (j >= g.n) continue;
+                        float c = __fsub_rn(__fadd_rn(rowterm, cj), __fmul_rn(g.scale, __uint_as_float(v[t])));
+                        if (j == row) c = 0.0f;
+                        if (g.dump && valid) g.dump[(size_t)row * g.n + j] = c;
+                        if (valid && !(c > thr)) {
+                            if (cnt < g.cap)
+                                cand[cnt] = ((unsigned long long)__float_as_uint(c) << 32) | j;
+                            ++cnt;
+                            if (c < arr[KP - 1]) {
+#pragma unroll
+                                for (int q = KP - 1; q > 0; --q) arr[q] = fminf(arr[q], fmaxf(arr[q - 1], c));
+                                arr[0] = fminf(arr[0], c);
+                                thr = __fadd_ru(arr[KP - 1], band);
+                            }
+                        }
+                    }
+                }
+                fence_before_sync();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(smem_u32(&acce[buf]));
+            }
+            if (valid) {
+                g.cand_cnt[slot] = cnt;
+                g.part_tau[slot] = arr[KP - 1];
+            }
+        }
+    }
+
+    fence_before_sync();
+    __syncthreads();
+    if (warp == 1) {
+        fence_after_sync();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                     "r"(SC_TMEM_COLS));
+    }
+}
+
+template <int KIND, int KP>
+static int launch_kind(const ScreenGemmArgs &g, const CUtensorMap &ta, const CUtensorMap &tb,
+                       cudaStream_t s) {
+    HM_CUDA_TRY(cudaFuncSetAttribute(screen_gemm_kernel<KIND, KP>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)SC_SMEM_BYTES));
+    int dev = 0, sms = 148;
+    HM_CUDA_TRY(cudaGetDevice(&dev));
+    HM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const uint32_t grid = g.units < (uint32_t)sms ? g.units : (uint32_t)sms;
+    screen_gemm_kernel<KIND, KP><<<grid, SC_THREADS, SC_SMEM_BYTES, s>>>(ta, tb, g);
+    HM_CUDA_TRY(cudaGetLastError());
+    count_launch();
+    return HM_OK;
+}
+
+int launch_screen_gemm(const ScreenGemmArgs &g, int kind, uint32_t kp, const CUtensorMap &ta,
+                       const CUtensorMap &tb, cudaStream_t s) {
+    ScopedKernelTimer timer(HM_KCLASS_BULK, s);
+    if (kind == SCREEN_KIND_BF16) {
+        if (kp == 32) return launch_kind<SCREEN_KIND_BF16, 32>(g, ta, tb, s);
+        if (kp == 64) return launch_kind<SCREEN_KIND_BF16, 64>(g, ta, tb, s);
+    } else {
+        if (kp == 32) return launch_kind<SCREEN_KIND_TF32, 32>(g, ta, tb, s);
+        if (kp == 64) return launch_kind<SCREEN_KIND_TF32, 64>(g, ta, tb, s);
+    }
+    return set_error(HM_ERR_UNSUPPORTED, "screen top-k width %u", kp);
+}
+
+}  // namespace hm

@@ -184,6 +184,10 @@ HM_API int hm_timing_read(int kernel_class, double *total_ms, uint64_t *launches
 /* Kernels this library has launched since it was loaded (all classes). */
 HM_API uint64_t hm_launch_count(void);
 
+/* Test hook: while set (non-NULL), screened runs on this thread also write
+ * every screened value c^_ij into d_out[i * n + j] (n x n floats). */
+HM_API int hm_debug_set_screen_dump(float *d_out);
+
 #ifdef __cplusplus
 }
 #endif

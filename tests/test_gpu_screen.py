@@ -1,0 +1,105 @@
+"""GPU parity of the screened paths (tcgen05 BF16 / TF32 / split-BF16 screen +
+exact rerank): every path must return the oracle's bytes; the screen itself
+must stay inside its proven band."""
+import numpy as np
+import pytest
+
+import holomap_b200 as hm
+from parity import assert_same_bytes, edge_case, rows_sorted_by_key
+
+pytestmark = pytest.mark.gpu
+PATHS = ["screen_bf16", "screen_tf32", "screen_bf16x3"]
+
+
+def screened_values(x, metric, path):
+    """Run one screened call with the dump hook set; return c^ (n x n)."""
+    import torch
+    n, d = x.shape
+    buf = torch.full((n * n,), float("nan"), dtype=torch.float32, device="cuda")
+    hm.lib().hm_debug_set_screen_dump(buf.data_ptr())
+    try:
+        hm.exact_knn(x, d, 5, metric, path)
+    finally:
+        hm.lib().hm_debug_set_screen_dump(None)
+    return buf.cpu().numpy().reshape(n, n)
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("metric", ["cosine", "euclidean"])
+def test_screen_values_track_exact_inner_products(path, metric):
+    g = np.random.default_rng(1)
+    n, d = 700, 72
+    x = g.normal(size=(n, d)).astype(np.float32)
+    c = screened_values(x, metric, path)
+    xd = x.astype(np.float64)
+    if metric == "cosine":
+        u = xd / np.linalg.norm(xd, axis=1, keepdims=True)
+        exact = 1.0 - u @ u.T
+        tol = {"screen_bf16": 2e-2, "screen_tf32": 3e-3, "screen_bf16x3": 1e-4}[path]
+    else:
+        u = xd - xd.mean(0)
+        m = np.sqrt((u * u).sum(1).max())
+        u = u * 2.0 ** -np.frexp(m)[1]
+        sq = (u * u).sum(1)
+        exact = sq[:, None] + sq[None, :] - 2 * u @ u.T
+        tol = {"screen_bf16": 2e-2, "screen_tf32": 3e-3, "screen_bf16x3": 1e-4}[path] * 4
+    np.fill_diagonal(exact, 0.0)
+    assert np.isfinite(c).all(), "screen left entries unwritten"
+    err = np.abs(c - exact).max()
+    assert err < tol, f"max |c^ - c| = {err}"
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("metric", ["euclidean", "cosine"])
+@pytest.mark.parametrize("n,d,k", [(300, 5, 15), (1000, 50, 15), (4500, 130, 30), (2100, 384, 64),
+                                   (5000, 16, 2), (1300, 7, 33)])
+def test_screened_matches_oracle(oracle, path, metric, n, d, k):
+    x = edge_case("gauss", n, d, seed=n + d)
+    st = hm.HmStats()
+    knn, sm = hm.knn_smooth(x, d, k, metric, path, stats=st)
+    oi, od = oracle.exact_knn(x, k, metric)
+    assert_same_bytes(knn.indices, oi, "indices")
+    assert_same_bytes(knn.dists, od, "dists")
+    osig, orho = oracle.smooth_knn(od, k)
+    assert_same_bytes(sm.sigmas, osig, "sigma")
+    assert_same_bytes(sm.rhos, orho, "rho")
+    assert st.path_used == hm.KnnPath.parse(path)
+    assert st.candidates_total >= n * k
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("kind", ["duplicates", "ulp", "zeros", "huge", "tiny", "grid",
+                                  "sorted_line"])
+@pytest.mark.parametrize("metric", ["euclidean", "cosine"])
+def test_screened_edge_cases(oracle, path, kind, metric):
+    x = edge_case(kind, 1111, 6, seed=13)
+    knn = hm.exact_knn(x, 6, 15, metric, path)
+    oi, od = oracle.exact_knn(x, 15, metric)
+    assert_same_bytes(knn.indices, oi, "indices")
+    assert_same_bytes(knn.dists, od, "dists")
+
+
+@pytest.mark.parametrize("name", ["blobs_euclidean", "cosine", "duplicates_euclidean"])
+@pytest.mark.parametrize("path", PATHS)
+def test_screened_golden_fixtures(oracle, name, path):
+    import json
+    from pathlib import Path
+    fx = json.loads((Path(__file__).parent / "golden" / f"stage2_{name}.json").read_text())
+    x = np.asarray(fx["data"], dtype=np.float32)
+    k = fx["n_neighbors"]
+    knn = hm.exact_knn(x, x.shape[1], k, fx["metric"], path)
+    assert knn.indices.reshape(-1, k).tolist() == fx["knn_indices"]
+    oi, od = oracle.exact_knn(x, k, fx["metric"])
+    assert_same_bytes(knn.dists, od, "dists")
+
+
+def test_screened_equals_plain_on_clustered_duplicates():
+    from holomap_b200.synth import dups_20k
+    wl = dups_20k(n=12000, d=64)
+    a = hm.exact_knn(wl.data, wl.d, wl.k, wl.metric, "plain")
+    for path in PATHS:
+        st = hm.HmStats()
+        b = hm.exact_knn(wl.data, wl.d, wl.k, wl.metric, path, stats=st)
+        assert_same_bytes(b.indices, a.indices, f"{path} indices")
+        assert_same_bytes(b.dists, a.dists, f"{path} dists")
+        assert rows_sorted_by_key(b.indices.reshape(-1, wl.k), b.dists.reshape(-1, wl.k))
