@@ -48,6 +48,9 @@ def parse_args():
     ap.add_argument("--workload", default="embed_50k",
                     choices=["embed_50k", "dups_20k", "blobs_1k"])
     ap.add_argument("--path", default="auto")
+    ap.add_argument("--rows", type=int, default=None,
+                    help="use only the first ROWS points of the workload (a smaller case "
+                         "of the same kernels, e.g. for profiling)")
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the oracle baseline sample")
@@ -55,9 +58,12 @@ def parse_args():
     return ap.parse_args()
 
 
-def workload(name):
-    from holomap_b200.synth import WORKLOADS
-    return WORKLOADS[name]()
+def workload(name, rows=None):
+    from holomap_b200.synth import WORKLOADS, Workload
+    wl = WORKLOADS[name]()
+    if rows:
+        wl = Workload(f"{wl.name}[:{rows}]", np.ascontiguousarray(wl.data[:rows]), wl.k, wl.metric)
+    return wl
 
 
 # ------------------------------------------------------------------ clocks
@@ -141,7 +147,7 @@ def reference_arm(args):
         return 0
     import holomap_oracle
     holomap_oracle.build()
-    wl = workload(args.workload)
+    wl = workload(args.workload, args.rows)
     threads = os.cpu_count() or 1
     # one step = a bounded sample of rows, sized for about 4 s of host work
     probe_rows = max(threads, 4)
@@ -200,7 +206,7 @@ def main():
         if world > 1:
             dist.barrier()
 
-    wl = workload(args.workload)
+    wl = workload(args.workload, args.rows)
     path = hm.KnnPath.parse(args.path)
     resolved = hm.autotune_path(wl.n, wl.d, wl.k, wl.metric) if path == hm.KnnPath.AUTO else path
     prob = DeviceKnnProblem(wl.n, wl.d, wl.k, wl.metric, resolved, device=dev)
@@ -293,6 +299,7 @@ def main():
                         "max": max(step_ms)},
             "stats": {"path_used": int(st.path_used), "col_splits": int(st.col_splits),
                       "candidates_per_row": st.candidates_total / wl.n,
+                      "emitted_per_row": st.candidates_emitted / wl.n,
                       "candidates_max_row": int(st.candidates_max_row),
                       "candidate_cap": int(st.candidate_cap),
                       "overflow_rows": int(st.overflow_rows),

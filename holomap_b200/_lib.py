@@ -104,6 +104,7 @@ class HmStats(ctypes.Structure):
         ("zero_rho_rows", ctypes.c_uint64),
         ("screen_band", ctypes.c_double),
         ("device_ms", ctypes.c_double),
+        ("candidates_emitted", ctypes.c_uint64),
     ]
 
     def as_dict(self) -> dict:

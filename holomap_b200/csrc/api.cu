@@ -261,6 +261,7 @@ static void fill_stats(hm_stats *st, const Layout &L, const Flags &f, uint64_t n
     st->candidates_total = f.screen.candidates;
     st->candidates_max_row = f.screen.max_row;
     st->overflow_rows = f.screen.overflow_rows;
+    st->candidates_emitted = f.screen.emitted;
     float band = 0.f;
     memcpy(&band, &f.screen.band_max_bits, sizeof band);
     st->screen_band = L.path == HM_PATH_PLAIN ? 0.0 : (double)band;

@@ -18,26 +18,13 @@ namespace hm {
 
 constexpr int RR_WARPS = 8;
 constexpr int RR_LIST = 256;  // compacted candidates per warp between flushes
+constexpr int RR_CH = 32;     // dimensions staged per round
 
-template <int METRIC>
-__device__ __forceinline__ float exact_distance(const double *__restrict__ xi,
-                                                const float *__restrict__ xj, uint32_t d,
-                                                double rn_i, double rn_j) {
-    double acc = 0.0;
-    if (METRIC == HM_METRIC_EUCLIDEAN) {
-        for (uint32_t t = 0; t < d; ++t) {
-            const double diff = __dsub_rn(xi[t], (double)__ldg(xj + t));
-            acc = __dadd_rn(acc, __dmul_rn(diff, diff));
-        }
-        return __double2float_rn(__dsqrt_rn(acc));
-    } else {
-        for (uint32_t t = 0; t < d; ++t) acc = __dadd_rn(acc, __dmul_rn(xi[t], (double)__ldg(xj + t)));
-        const double q = __ddiv_rn(acc, __dmul_rn(rn_i, rn_j));
-        const double r = __dsub_rn(1.0, q);
-        return (r > 0.0) ? __double2float_rn(r) : 0.0f;
-    }
-}
-
+// One warp per query row.  Candidates are evaluated 32 at a time, one per
+// lane; their rows are staged through shared memory 32 dimensions at a time
+// with coalesced loads (one 128-byte row segment per load instruction), so
+// the per-lane binary64 chains read shared memory instead of scattered
+// global addresses.
 template <int METRIC, int KPL>
 __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs a, uint32_t dstride) {
     extern __shared__ double rr_smem[];
@@ -45,16 +32,16 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs 
     const uint32_t row = blockIdx.x * RR_WARPS + warp;
     if (row >= a.n) return;
     double *xi = rr_smem + (size_t)warp * dstride;
-    uint32_t *list = reinterpret_cast<uint32_t *>(rr_smem + (size_t)RR_WARPS * dstride) + warp * RR_LIST;
+    float *tiles = reinterpret_cast<float *>(rr_smem + (size_t)RR_WARPS * dstride);
+    float *tile = tiles + (size_t)warp * RR_CH * 33;  // [t][candidate], padded
+    uint32_t *list = reinterpret_cast<uint32_t *>(tiles + (size_t)RR_WARPS * RR_CH * 33) + warp * RR_LIST;
+    unsigned long long *offs = reinterpret_cast<unsigned long long *>(
+                                   reinterpret_cast<uint32_t *>(tiles + (size_t)RR_WARPS * RR_CH * 33) +
+                                   RR_WARPS * RR_LIST) + warp * 32;
 
     // overflow / unbounded rows go to the exact plain path
     bool ovf = a.force_exact[row] != 0;
-    float tau = __int_as_float(0x7f800000);
-    for (uint32_t p = 0; p < a.parts; ++p) {
-        const size_t slot = (size_t)row * a.parts + p;
-        ovf |= a.cand_cnt[slot] > a.cap;
-        tau = fminf(tau, a.part_tau[slot]);
-    }
+    for (uint32_t p = 0; p < a.parts; ++p) ovf |= a.cand_cnt[(size_t)row * a.parts + p] > a.cap;
     if (ovf) {
         if (lane == 0) {
             const uint32_t at = atomicAdd(a.ovf_cnt, 1u);
@@ -63,6 +50,30 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs 
         }
         return;
     }
+    // Threshold: the exact k-th smallest screened value of the row, taken
+    // over the union of its candidate lists (every column at or below any
+    // list's running threshold was emitted, so the union holds the row's k
+    // smallest screened values).
+    WarpTopK<KPL> sel;
+    sel.reset();
+    for (uint32_t p = 0; p < a.parts; ++p) {
+        const size_t slot = (size_t)row * a.parts + p;
+        const uint32_t cnt = a.cand_cnt[slot];
+        const unsigned long long *cand = a.cand + slot * a.cap;
+        for (uint32_t e0 = 0; e0 < cnt; e0 += 32) {
+            uint64_t key = KEY_NONE;
+            if (e0 + lane < cnt) {
+                const unsigned long long c = cand[e0 + lane];
+                const uint32_t b = (uint32_t)(c >> 32);
+                const uint32_t ord = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+                key = ((uint64_t)ord << 32) | (uint32_t)c;
+            }
+            sel.offer(key, a.k, lane);
+        }
+    }
+    const uint32_t tord = (uint32_t)(sel.tau >> 32);
+    const float tau = sel.tau == KEY_NONE ? __int_as_float(0x7f800000)
+                                          : __uint_as_float((tord & 0x80000000u) ? (tord & 0x7fffffffu) : ~tord);
     const float thr = __fadd_ru(tau, a.band[row]);
 
     for (uint32_t t = lane; t < a.d; t += 32) xi[t] = (double)a.x[(size_t)row * a.d + t];
@@ -76,13 +87,49 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs 
 
     auto flush = [&](uint32_t m) {
         for (uint32_t b = 0; b < m; b += 32) {
+            const bool mine = b + lane < m;
+            const uint32_t j = mine ? list[b + lane] : row;
+            offs[lane] = (unsigned long long)j * a.d;
+            __syncwarp();
+            // candidate rows are staged 32 dimensions at a time; the next
+            // slice is loaded into registers while this one is consumed
+            float pre[32];
+            auto load = [&](uint32_t c0) {
+                const uint32_t c = c0 + lane;
+#pragma unroll
+                for (int r = 0; r < 32; ++r) pre[r] = (c < a.d) ? __ldg(a.x + offs[r] + c) : 0.0f;
+            };
+            load(0);
+            double acc = 0.0;
+            for (uint32_t c0 = 0; c0 < a.d; c0 += RR_CH) {
+#pragma unroll
+                for (int r = 0; r < 32; ++r) tile[lane * 33 + r] = pre[r];
+                __syncwarp();
+                if (c0 + RR_CH < a.d) load(c0 + RR_CH);
+                const uint32_t tn = min((uint32_t)RR_CH, a.d - c0);
+                for (uint32_t t = 0; t < tn; ++t) {
+                    const double y = (double)tile[t * 33 + lane];
+                    if (METRIC == HM_METRIC_EUCLIDEAN) {
+                        const double diff = __dsub_rn(xi[c0 + t], y);
+                        acc = __dadd_rn(acc, __dmul_rn(diff, diff));
+                    } else {
+                        acc = __dadd_rn(acc, __dmul_rn(xi[c0 + t], y));
+                    }
+                }
+                __syncwarp();
+            }
             uint64_t key = KEY_NONE;
-            if (b + lane < m) {
-                const uint32_t j = list[b + lane];
-                const float dist =
-                    (j == row) ? 0.0f
-                               : exact_distance<METRIC>(xi, a.x + (size_t)j * a.d, a.d, rn_i,
-                                                        METRIC == HM_METRIC_COSINE ? a.rnorm[j] : 0.0);
+            if (mine) {
+                float dist;
+                if (j == row) {
+                    dist = 0.0f;  // src/knn.rs:38-39
+                } else if (METRIC == HM_METRIC_EUCLIDEAN) {
+                    dist = __double2float_rn(__dsqrt_rn(acc));
+                } else {
+                    const double q = __ddiv_rn(acc, __dmul_rn(rn_i, a.rnorm[j]));
+                    const double r = __dsub_rn(1.0, q);
+                    dist = (r > 0.0) ? __double2float_rn(r) : 0.0f;
+                }
                 key = make_key(dist, j);
             }
             top.offer(key, a.k, lane);
@@ -133,7 +180,9 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs 
 template <int METRIC>
 static int launch_metric(const RerankArgs &a, uint32_t kpl, cudaStream_t s) {
     const uint32_t dstride = (uint32_t)round_up(a.d, 2);
-    const size_t smem = (size_t)RR_WARPS * dstride * sizeof(double) + RR_WARPS * RR_LIST * sizeof(uint32_t);
+    const size_t smem = (size_t)RR_WARPS * dstride * sizeof(double) +
+                        (size_t)RR_WARPS * RR_CH * 33 * sizeof(float) + RR_WARPS * RR_LIST * sizeof(uint32_t) +
+                        RR_WARPS * 32 * sizeof(unsigned long long);
     const int blocks = (int)((a.n + RR_WARPS - 1) / RR_WARPS);
 #define HM_RR_CASE(K)                                                                       \
     case K: {                                                                               \

@@ -72,8 +72,9 @@ int screen_plan(uint64_t n, uint32_t d, uint32_t k, int metric, int path, Screen
         }
     }
     L.units = L.row_blocks * L.parts;
-    const double per_part = (double)n / L.parts;
-    const double expect = 2.0 * k * (2.0 + std::log(std::fmax(1.0, per_part / k)));
+    // each (row, part) has two candidate lists, one per epilogue half tile
+    const double per_slot = (double)n / (2.0 * L.parts);
+    const double expect = 1.5 * k * (2.0 + std::log(std::fmax(1.0, per_slot / k)));
     L.cap = pow2ceil((uint32_t)expect);
     if (L.cap < 128) L.cap = 128;
     if (L.cap > 4096) L.cap = 4096;
@@ -98,22 +99,24 @@ int screen_plan(uint64_t n, uint32_t d, uint32_t k, int metric, int path, Screen
     off = a256(off + (size_t)n * sizeof(RowStat));
     L.off_rowterm = off;
     off = a256(off + (size_t)n * sizeof(float));
-    L.off_colterm = off;
-    off = a256(off + (size_t)n * sizeof(float));
+    L.off_colterm = off;  // padded to whole tiles, zero past n
+    off = a256(off + round_up(n, SC_BN) * sizeof(float));
     L.off_band = off;
     off = a256(off + (size_t)n * sizeof(float));
     L.off_force = off;
     off = a256(off + (size_t)n);
     L.off_cand = off;
-    off = a256(off + (size_t)n * L.parts * L.cap * sizeof(unsigned long long));
+    off = a256(off + (size_t)n * L.parts * 2 * L.cap * sizeof(unsigned long long));
     L.off_cnt = off;
-    off = a256(off + (size_t)n * L.parts * sizeof(uint32_t));
+    off = a256(off + (size_t)n * L.parts * 2 * sizeof(uint32_t));
     L.off_tau = off;
-    off = a256(off + (size_t)n * L.parts * sizeof(float));
+    off = a256(off + (size_t)n * L.parts * 2 * sizeof(float));
     L.off_ovf = off;
     off = a256(off + (size_t)n * sizeof(uint32_t));
     L.off_ovf_cnt = off;
     off = a256(off + sizeof(uint32_t));
+    L.off_rowthr = off;
+    off = a256(off + (size_t)n * sizeof(uint32_t));
     L.total = off;
     return HM_OK;
 }
@@ -197,6 +200,9 @@ int screen_run(const ScreenRun &r, const ScreenLayout &L, char *ws, cudaStream_t
     g.cand_cnt = reinterpret_cast<uint32_t *>(ws + L.off_cnt);
     g.part_tau = reinterpret_cast<float *>(ws + L.off_tau);
     g.error_code = &r.counters->error_code;
+    g.emitted = &r.counters->emitted;
+    g.zero_rows = reinterpret_cast<unsigned long long *>(ws + L.off_max) + 7;
+    g.rowthr = reinterpret_cast<uint32_t *>(ws + L.off_rowthr);
     g.dump = r.debug_dump ? r.debug_dump : g_debug_dump;
     g.idesc = make_idesc(L.kind);
     HM_TRY(launch_screen_gemm(g, L.kind, r.k <= 32 ? 32u : 64u, ta, tb, s));
@@ -209,7 +215,7 @@ int screen_run(const ScreenRun &r, const ScreenLayout &L, char *ws, cudaStream_t
     ra.n = r.n;
     ra.d = r.d;
     ra.k = r.k;
-    ra.parts = L.parts;
+    ra.parts = L.parts * 2;  // candidate lists per row
     ra.cap = L.cap;
     ra.cand = g.cand;
     ra.cand_cnt = g.cand_cnt;

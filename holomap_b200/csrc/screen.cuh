@@ -36,6 +36,8 @@ struct ScreenCounters {
     uint32_t overflow_rows;         // rows sent to the exact fallback
     uint32_t band_max_bits;         // widest keep band 2E_i (binary32 bits)
     uint32_t error_code;            // nonzero if a bounded wait gave up
+    uint32_t pad;
+    unsigned long long emitted;     // candidates the screen wrote, all rows
 };
 
 // Screen GEMM tile: 128 query rows (UMMA M) x 256 columns (UMMA N), 128-byte
@@ -44,7 +46,8 @@ constexpr int SC_BM = 128;
 constexpr int SC_BN = 256;
 constexpr int SC_SLICE_BYTES = 128;
 constexpr int SC_STAGES = 4;
-constexpr int SC_THREADS = 192;  // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue
+constexpr int SC_EPI_WARPS = 8;  // two per TMEM lane quadrant, one per half tile
+constexpr int SC_THREADS = 64 + 32 * SC_EPI_WARPS;  // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
 
 enum ScreenKind { SCREEN_KIND_BF16 = 0, SCREEN_KIND_TF32 = 1 };
 
@@ -62,7 +65,7 @@ struct ScreenLayout {
     uint32_t csum_blocks = 0; // euclidean column-mean partial blocks
     size_t off_a = 0, off_b = 0, off_csum = 0, off_mu = 0, off_max = 0, off_rowstat = 0;
     size_t off_rowterm = 0, off_colterm = 0, off_band = 0, off_force = 0;
-    size_t off_cand = 0, off_cnt = 0, off_tau = 0, off_ovf = 0, off_ovf_cnt = 0;
+    size_t off_cand = 0, off_cnt = 0, off_tau = 0, off_ovf = 0, off_ovf_cnt = 0, off_rowthr = 0;
     size_t total = 0;
 };
 
@@ -111,10 +114,13 @@ struct ScreenGemmArgs {
     const float *rowterm;     // euclidean ||u_i||^2 (binary32); null for cosine
     const float *colterm;     // per column additive term
     const float *band;        // per row keep band 2E_i
-    unsigned long long *cand; // [(row*parts + part)*cap] = (c^ bits << 32) | j
-    uint32_t *cand_cnt;       // [row*parts + part]
-    float *part_tau;          // [row*parts + part]
+    unsigned long long *cand; // [slot*cap] = (c^ bits << 32) | j, slot = (row*parts + part)*2 + half
+    uint32_t *cand_cnt;       // [slot]
+    float *part_tau;          // [slot]
     uint32_t *error_code;
+    unsigned long long *emitted;
+    const unsigned long long *zero_rows;  // cosine: rows with ||x|| = 0
+    uint32_t *rowthr;         // per row: smallest list threshold so far (order-preserving key)
     float *dump;
     uint32_t idesc;
 };

@@ -2,17 +2,20 @@
 // accumulators, fused with a per-row running top-k threshold and candidate
 // emission, so the N x N similarity matrix never leaves the SM.
 //
-// One CTA per SM (persistent), 6 warps:
+// One CTA per SM (persistent), 10 warps:
 //   warp 0     TMA producer: 128-row A slice + 256-row B slice per stage
 //              (128-byte K slices, 128B swizzle, 4-stage mbarrier ring; no
 //              cluster multicast),
 //   warp 1     allocates 512 TMEM columns (two 128 x 256 fp32 accumulators)
 //              and issues tcgen05.mma (one thread) + tcgen05.commit,
-//   warps 2-5  epilogue: each thread owns one query row (its TMEM lane),
-//              reads its 256 accumulator columns with tcgen05.ld, forms the
-//              screened value c^ in binary32, keeps a sorted register array of
-//              its k smallest c^ (threshold tau) and emits every column with
-//              c^ <= tau + band_i into the row's candidate list.
+//   warps 2-9  epilogue: each thread owns one query row (its TMEM lane) and
+//              one half of every tile's 256 columns.  Per 32-column chunk it
+//              forms the screened values c^ in binary32 and their minimum
+//              (branch-free); only when that minimum passes the row's
+//              threshold does it emit the chunk's columns with
+//              c^ <= tau + band into the row's candidate list and insert
+//              them into a sorted register array of the k smallest c^ seen,
+//              whose largest entry is tau.
 // Work units are (row block of 128, column part); the columns of a unit are
 // walked in 256-wide tiles with the two accumulators double buffered, so the
 // epilogue of one tile overlaps the MMAs of the next.
@@ -147,7 +150,10 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
                  : "memory");
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+// tcgen05.ld of 32 consecutive accumulator columns of this warp's 32 lanes;
+// the registers are valid only after tmem_ld_wait on the same array (the
+// wait names them as in/out operands so no use can be scheduled before it).
+__device__ __forceinline__ void tmem_ld32_issue(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32"
         " {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15,"
@@ -159,7 +165,27 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
           "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
           "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
         : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_ld_wait(uint32_t (&v)[32]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]),
+                   "+r"(v[6]), "+r"(v[7]), "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]),
+                   "+r"(v[12]), "+r"(v[13]), "+r"(v[14]), "+r"(v[15]), "+r"(v[16]), "+r"(v[17]),
+                   "+r"(v[18]), "+r"(v[19]), "+r"(v[20]), "+r"(v[21]), "+r"(v[22]), "+r"(v[23]),
+                   "+r"(v[24]), "+r"(v[25]), "+r"(v[26]), "+r"(v[27]), "+r"(v[28]), "+r"(v[29]),
+                   "+r"(v[30]), "+r"(v[31])
+                 :
+                 : "memory");
+}
+
+// binary32 <-> unsigned key with the same order (for atomicMin)
+__device__ __forceinline__ uint32_t ord32(float f) {
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float unord32(uint32_t o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
 }
 
 __device__ __forceinline__ void raise_error(volatile uint32_t *abort_flag, uint32_t *error_code,
@@ -207,7 +233,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(smem_u32(&accf[b]), 1);
-            mbar_init(smem_u32(&acce[b]), 4);
+            mbar_init(smem_u32(&acce[b]), SC_EPI_WARPS);
         }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -305,23 +331,31 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         __syncwarp();
     } else {
         // --------------------------------------------------------- epilogue
-        const uint32_t quad = (uint32_t)(warp & 3);  // TMEM lane quadrant of this warp
+        // warps 2..9: quadrant (warp & 3) of the TMEM lanes = 32 query rows,
+        // half (warp - 2) / 4 of the tile's 256 columns
+        const uint32_t quad = (uint32_t)(warp & 3);
+        const uint32_t half = (uint32_t)(warp - 2) >> 2;
         const uint32_t row_in_tile = quad * 32 + lane;
         const float INF = __int_as_float(0x7f800000);
+        // cosine fast test needs every column term to be 1 (no zero rows)
+        const bool fast_cos = g.rowterm == nullptr && *g.zero_rows == 0;
         uint32_t tile = 0;
         bool ok = true;
         for (uint32_t u = blockIdx.x; ok && u < g.units; u += gridDim.x) {
             const UnitTiles ut = unit_tiles(g, u);
             const uint32_t row = ut.rb * SC_BM + row_in_tile;
             const bool valid = row < g.n;
+            // sorted k smallest chunk minima; arr[KP-1] is the running tau
             float arr[KP];
 #pragma unroll
             for (int q = 0; q < KP; ++q) arr[q] = (q < KP - (int)g.k) ? -INF : INF;
             const float band = valid ? g.band[row] : 0.0f;
             const float rowterm = (valid && g.rowterm) ? g.rowterm[row] : 0.0f;
-            float thr = INF;
+            float thr = valid ? INF : -INF;  // invalid rows never emit
+            float tglob = INF;      // the row's shared threshold, last seen
+            float published = INF;  // this list's tau, last shared
             uint32_t cnt = 0;
-            const size_t slot = ((size_t)row * g.parts + ut.part);
+            const size_t slot = ((size_t)row * g.parts + ut.part) * 2 + half;
             unsigned long long *cand = g.cand + slot * g.cap;
 
             for (uint32_t ct = ut.ct_begin; ct < ut.ct_end; ++ct, ++tile) {
@@ -332,33 +366,111 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                     break;
                 }
                 fence_after_sync();
-                for (uint32_t ch = 0; ch < SC_BN / 32; ++ch) {
-                    const uint32_t col0 = ct * SC_BN + ch * 32;
-                    if (col0 >= g.n) break;  // uniform over the CTA
-                    uint32_t v[32];
-                    tmem_ld32(tmem_base + ((quad * 32) << 16) + buf * SC_BN + ch * 32, v);
-                    const uint32_t my_col = col0 + lane;
-                    const float ct_mine = my_col < g.n ? g.colterm[my_col] : 0.0f;
+                if (valid) {  // the row's other lists may have tightened its threshold
+                    const float tg = unord32(*(volatile const uint32_t *)(g.rowthr + row));
+                    if (tg < tglob) {
+                        tglob = tg;
+                        thr = __fadd_ru(fminf(arr[KP - 1], tglob), band);
+                    }
+                }
+                const uint32_t c_base = ct * SC_BN + half * (SC_BN / 2);
+                const bool diag = (ct * SC_BN < ut.rb * SC_BM + SC_BM) && (ut.rb * SC_BM < ct * SC_BN + SC_BN);
+                const uint32_t t_base = tmem_base + ((quad * 32) << 16) + buf * SC_BN + half * (SC_BN / 2);
+                // chunks of 32 columns, two accumulator register sets: the
+                // tcgen05.ld of the next chunk is in flight while this one is
+                // processed
+                auto process = [&](uint32_t (&v)[32], uint32_t ch) {
+                    // c overwrites the accumulator registers in place
+                    float (&c)[32] = reinterpret_cast<float (&)[32]>(v);
+                    const uint32_t j0 = c_base + ch * 32;
+                    // columns past n: never emitted, never the chunk minimum
+                    const uint32_t vmask = (j0 + 32 <= g.n) ? 0xffffffffu
+                                           : (j0 >= g.n ? 0u : (0xffffffffu >> (32 - (g.n - j0))));
+                    if (fast_cos) {
 #pragma unroll
-                    for (int t = 0; t < 32; ++t) {
-                        const uint32_t j = col0 + t;
-                        const float cj = __shfl_sync(0xffffffffu, ct_mine, t);
-                        if (j >= g.n) continue;
-                        float c = __fsub_rn(__fadd_rn(rowterm, cj), __fmul_rn(g.scale, __uint_as_float(v[t])));
-                        if (j == row) c = 0.0f;
-                        if (g.dump && valid) g.dump[(size_t)row * g.n + j] = c;
-                        if (valid && !(c > thr)) {
-                            if (cnt < g.cap)
-                                cand[cnt] = ((unsigned long long)__float_as_uint(c) << 32) | j;
-                            ++cnt;
-                            if (c < arr[KP - 1]) {
+                        for (int t = 0; t < 32; ++t) c[t] = __fsub_rn(1.0f, c[t]);
+                    } else {
+                        const float4 *ctp = reinterpret_cast<const float4 *>(g.colterm + j0);
 #pragma unroll
-                                for (int q = KP - 1; q > 0; --q) arr[q] = fminf(arr[q], fmaxf(arr[q - 1], c));
-                                arr[0] = fminf(arr[0], c);
-                                thr = __fadd_ru(arr[KP - 1], band);
-                            }
+                        for (int q = 0; q < 8; ++q) {
+                            const float4 cq = __ldg(ctp + q);
+                            const float cs[4] = {cq.x, cq.y, cq.z, cq.w};
+#pragma unroll
+                            for (int e = 0; e < 4; ++e)
+                                c[4 * q + e] = __fsub_rn(__fadd_rn(rowterm, cs[e]), __fmul_rn(g.scale, c[4 * q + e]));
                         }
                     }
+                    if (diag) {
+#pragma unroll
+                        for (int t = 0; t < 32; ++t)
+                            if (j0 + t == row) c[t] = 0.0f;
+                    }
+                    if (vmask != 0xffffffffu) {
+#pragma unroll
+                        for (int t = 0; t < 32; ++t)
+                            if (!((vmask >> t) & 1u)) c[t] = INF;
+                    }
+                    if (g.dump && valid) {
+                        for (int t = 0; t < 32; ++t)
+                            if (j0 + t < g.n) g.dump[(size_t)row * g.n + j0 + t] = c[t];
+                    }
+                    // columns within the threshold: one predicate word per
+                    // column (set.leu keeps a NaN), OR-reduced as a tree
+                    uint32_t pw[32];
+#pragma unroll
+                    for (int t = 0; t < 32; ++t) {
+                        uint32_t m;
+                        asm("set.leu.u32.f32 %0, %1, %2;" : "=r"(m) : "f"(c[t]), "f"(thr));
+                        pw[t] = m & (1u << t);
+                    }
+#pragma unroll
+                    for (int w = 16; w > 0; w >>= 1)
+#pragma unroll
+                        for (int t = 0; t < w; ++t) pw[t] |= pw[t + w];
+                    uint32_t pm = pw[0] & vmask;
+                    if (pm) {
+                        // emit each passing column and insert it into the
+                        // running k smallest when it improves them
+                        float cl[32];
+#pragma unroll
+                        for (int t = 0; t < 32; ++t) cl[t] = c[t];
+                        bool improved = false;
+                        while (pm) {
+                            const int t = __ffs(pm) - 1;
+                            pm &= pm - 1;
+                            const float x = cl[t];
+                            if (cnt < g.cap) cand[cnt] = ((unsigned long long)__float_as_uint(x) << 32) | (j0 + t);
+                            ++cnt;
+                            if (x < arr[KP - 1]) {
+#pragma unroll
+                                for (int q = KP - 1; q > 0; --q) arr[q] = fminf(arr[q], fmaxf(arr[q - 1], x));
+                                arr[0] = fminf(arr[0], x);
+                                improved = true;
+                            }
+                        }
+                        if (improved) {
+                            const float tl = arr[KP - 1];
+                            if (tl < published) {  // share with the row's other lists
+                                const uint32_t o = ord32(tl);
+                                const uint32_t prev = atomicMin(g.rowthr + row, o);
+                                tglob = fminf(tglob, unord32(prev < o ? prev : o));
+                                published = tl;
+                            }
+                            thr = __fadd_ru(fminf(tl, tglob), band);
+                        }
+                    }
+                };
+                uint32_t va[32], vb[32];
+                tmem_ld32_issue(t_base, va);
+                tmem_ld_wait(va);
+#pragma unroll 1
+                for (uint32_t ch = 0; ch < SC_BN / 64; ch += 2) {
+                    tmem_ld32_issue(t_base + (ch + 1) * 32, vb);
+                    process(va, ch);
+                    tmem_ld_wait(vb);
+                    if (ch + 2 < SC_BN / 64) tmem_ld32_issue(t_base + (ch + 2) * 32, va);
+                    process(vb, ch + 1);
+                    if (ch + 2 < SC_BN / 64) tmem_ld_wait(va);
                 }
                 fence_before_sync();
                 __syncwarp();
@@ -367,6 +479,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
             if (valid) {
                 g.cand_cnt[slot] = cnt;
                 g.part_tau[slot] = arr[KP - 1];
+                atomicAdd(g.emitted, (unsigned long long)cnt);
             }
         }
     }

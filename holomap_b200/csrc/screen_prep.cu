@@ -191,6 +191,9 @@ __global__ void __launch_bounds__(256) operand_kernel(const float *__restrict__ 
             colterm[row] = zero_row ? 0.0f : 1.0f;
         }
         force[row] = zero_row ? 1 : 0;
+        // shared screen threshold of the row starts at +inf (order-preserving key)
+        reinterpret_cast<uint32_t *>(ws + L.off_rowthr)[row] = 0xff800000u;
+        if (zero_row) atomicAdd(&maxb[7], 1ull);
     }
 }
 
@@ -231,6 +234,7 @@ int launch_screen_prep(const ScreenPrepArgs &a, cudaStream_t s) {
     ScopedKernelTimer timer(HM_KCLASS_PREP, s);
     const ScreenLayout &L = a.L;
     HM_CUDA_TRY(cudaMemsetAsync(a.ws + L.off_max, 0, 8 * sizeof(unsigned long long), s));
+    HM_CUDA_TRY(cudaMemsetAsync(a.ws + L.off_colterm, 0, round_up(a.n, SC_BN) * sizeof(float), s));
     if (a.metric == HM_METRIC_EUCLIDEAN) {
         const uint32_t rows_per = (a.n + L.csum_blocks - 1) / L.csum_blocks;
         colsum_partial_kernel<<<L.csum_blocks, 128, 0, s>>>(

@@ -78,6 +78,8 @@ typedef struct hm_stats {
     uint64_t zero_rho_rows;      /* rows whose sigma floor used the global mean */
     double screen_band;          /* screened paths: largest keep band (distance units) */
     double device_ms;            /* device time of the call's kernels */
+    uint64_t candidates_emitted; /* screened paths: candidates the screen wrote (before the
+                                    final threshold) */
 } hm_stats;
 
 /* ----------------------------------------------------------------------------
