@@ -155,7 +155,9 @@ static int run_knn(const float *d_data, uint64_t n, uint32_t d, uint32_t k, int 
     }
     double *x64 = reinterpret_cast<double *>(ws + L.off_x64);
     double *rnorm = reinterpret_cast<double *>(ws + L.off_rnorm);
-    HM_TRY(launch_prep_plain(d_data, (uint32_t)n, d, L.ldd, L.n_pad, metric, x64, rnorm, s));
+    // the screened path builds the binary64 copy only if its fallback needs it
+    HM_TRY(launch_prep_plain(d_data, (uint32_t)n, d, L.ldd, L.n_pad, metric,
+                             L.path == HM_PATH_PLAIN ? x64 : nullptr, rnorm, s));
 
     if (L.path == HM_PATH_PLAIN) {
         PlainArgs a{};
@@ -184,6 +186,7 @@ static int run_knn(const float *d_data, uint64_t n, uint32_t d, uint32_t k, int 
     r.n = (uint32_t)n;
     r.d = d;
     r.ldd = L.ldd;
+    r.n_pad = L.n_pad;
     r.k = k;
     r.metric = metric;
     r.path = L.path;

@@ -164,9 +164,14 @@ struct PlainArgs {
 
 int kpl_for_k(uint32_t k);  // 1, 2, 4, 8 or 0 if k > 256
 
-// X (n x d f32) -> zero-padded binary64 copy (+ row norms for cosine).
+// X (n x d f32) -> zero-padded binary64 copy (skipped when x64 is null) and,
+// for cosine, the row norms.
 int launch_prep_plain(const float *x, uint32_t n, uint32_t d, uint32_t ldd, uint32_t n_pad,
                       int metric, double *x64, double *rnorm, cudaStream_t s);
+// The binary64 copy alone; when `gate` is set it is built only if *gate != 0
+// (the screened path's fallback rows).
+int launch_prep_x64(const float *x, uint32_t n, uint32_t d, uint32_t ldd, uint32_t n_pad,
+                    double *x64, const uint32_t *gate, cudaStream_t s);
 int launch_plain_knn(const PlainArgs &a, int metric, uint32_t splits, cudaStream_t s);
 // Row-list mode with a persistent grid (the list length lives on the device).
 int launch_plain_knn_rows(const PlainArgs &a, int metric, cudaStream_t s);

@@ -35,7 +35,9 @@ int kpl_for_k(uint32_t k) {
 
 // ------------------------------------------------------------------ prep
 __global__ void prep_plain_kernel(const float *__restrict__ x, uint32_t n, uint32_t d,
-                                  uint32_t ldd, uint32_t n_pad, double *__restrict__ x64) {
+                                  uint32_t ldd, uint32_t n_pad, double *__restrict__ x64,
+                                  const uint32_t *__restrict__ gate) {
+    if (gate && *gate == 0) return;  // nothing needs the binary64 copy
     const size_t total = (size_t)n_pad * ldd;
     for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
          t += (size_t)gridDim.x * blockDim.x) {
@@ -63,16 +65,23 @@ __global__ void row_norm_kernel(const float *__restrict__ x, uint32_t n, uint32_
     rnorm[r] = __dsqrt_rn(s);
 }
 
-int launch_prep_plain(const float *x, uint32_t n, uint32_t d, uint32_t ldd, uint32_t n_pad,
-                      int metric, double *x64, double *rnorm, cudaStream_t s) {
+int launch_prep_x64(const float *x, uint32_t n, uint32_t d, uint32_t ldd, uint32_t n_pad,
+                    double *x64, const uint32_t *gate, cudaStream_t s) {
     ScopedKernelTimer timer(HM_KCLASS_PREP, s);
     const size_t total = (size_t)n_pad * ldd;
     const int threads = 256;
     int blocks = (int)((total + threads - 1) / threads);
     if (blocks > 148 * 16) blocks = 148 * 16;
-    prep_plain_kernel<<<blocks, threads, 0, s>>>(x, n, d, ldd, n_pad, x64);
+    prep_plain_kernel<<<blocks, threads, 0, s>>>(x, n, d, ldd, n_pad, x64, gate);
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();
+    return HM_OK;
+}
+
+int launch_prep_plain(const float *x, uint32_t n, uint32_t d, uint32_t ldd, uint32_t n_pad,
+                      int metric, double *x64, double *rnorm, cudaStream_t s) {
+    if (x64) HM_TRY(launch_prep_x64(x, n, d, ldd, n_pad, x64, nullptr, s));
+    ScopedKernelTimer timer(HM_KCLASS_PREP, s);
     if (metric == HM_METRIC_COSINE) {
         row_norm_kernel<<<(n_pad + 127) / 128, 128, 0, s>>>(x, n, d, n_pad, rnorm);
         HM_CUDA_TRY(cudaGetLastError());

@@ -16,15 +16,21 @@
 
 namespace hm {
 
+// One dimension of the reference's accumulation: euclidean (x - y)^2,
+// cosine x * y, each operation rounded to nearest in binary64.
+template <int METRIC>
+__device__ __forceinline__ double step(double acc, double x, double y) {
+    if (METRIC == HM_METRIC_EUCLIDEAN) {
+        const double diff = __dsub_rn(x, y);
+        return __dadd_rn(acc, __dmul_rn(diff, diff));
+    }
+    return __dadd_rn(acc, __dmul_rn(x, y));
+}
+
 constexpr int RR_WARPS = 8;
 constexpr int RR_LIST = 256;  // compacted candidates per warp between flushes
-constexpr int RR_CH = 32;     // dimensions staged per round
 
-// One warp per query row.  Candidates are evaluated 32 at a time, one per
-// lane; their rows are staged through shared memory 32 dimensions at a time
-// with coalesced loads (one 128-byte row segment per load instruction), so
-// the per-lane binary64 chains read shared memory instead of scattered
-// global addresses.
+// One warp per query row; candidates are evaluated 32 at a time, one per lane.
 template <int METRIC, int KPL>
 __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs a, uint32_t dstride) {
     extern __shared__ double rr_smem[];
@@ -32,12 +38,7 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs 
     const uint32_t row = blockIdx.x * RR_WARPS + warp;
     if (row >= a.n) return;
     double *xi = rr_smem + (size_t)warp * dstride;
-    float *tiles = reinterpret_cast<float *>(rr_smem + (size_t)RR_WARPS * dstride);
-    float *tile = tiles + (size_t)warp * RR_CH * 33;  // [t][candidate], padded
-    uint32_t *list = reinterpret_cast<uint32_t *>(tiles + (size_t)RR_WARPS * RR_CH * 33) + warp * RR_LIST;
-    unsigned long long *offs = reinterpret_cast<unsigned long long *>(
-                                   reinterpret_cast<uint32_t *>(tiles + (size_t)RR_WARPS * RR_CH * 33) +
-                                   RR_WARPS * RR_LIST) + warp * 32;
+    uint32_t *list = reinterpret_cast<uint32_t *>(rr_smem + (size_t)RR_WARPS * dstride) + warp * RR_LIST;
 
     // overflow / unbounded rows go to the exact plain path
     bool ovf = a.force_exact[row] != 0;
@@ -50,24 +51,22 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs 
         }
         return;
     }
-    // Threshold: the exact k-th smallest screened value of the row, taken
-    // over the union of its candidate lists (every column at or below any
-    // list's running threshold was emitted, so the union holds the row's k
-    // smallest screened values).
+    // Threshold: the exact k-th smallest screened value of the row.  Every
+    // one of the row's k smallest screened values stays in the k-array of the
+    // list that saw it, so the k-th smallest of the union of the lists'
+    // arrays is exactly that value.
     WarpTopK<KPL> sel;
     sel.reset();
     for (uint32_t p = 0; p < a.parts; ++p) {
-        const size_t slot = (size_t)row * a.parts + p;
-        const uint32_t cnt = a.cand_cnt[slot];
-        const unsigned long long *cand = a.cand + slot * a.cap;
-        for (uint32_t e0 = 0; e0 < cnt; e0 += 32) {
+        const float *kk = a.part_topk + ((size_t)row * a.parts + p) * a.k;
+        for (uint32_t e0 = 0; e0 < a.k; e0 += 32) {
             uint64_t key = KEY_NONE;
-            if (e0 + lane < cnt) {
-                const unsigned long long c = cand[e0 + lane];
-                const uint32_t b = (uint32_t)(c >> 32);
+            if (e0 + lane < a.k) {
+                const uint32_t b = __float_as_uint(kk[e0 + lane]);
                 const uint32_t ord = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-                key = ((uint64_t)ord << 32) | (uint32_t)c;
+                key = ((uint64_t)ord << 32) | (p * a.k + e0 + lane);
             }
+            if (!__any_sync(0xffffffffu, key < sel.tau)) break;  // arrays are ascending
             sel.offer(key, a.k, lane);
         }
     }
@@ -85,39 +84,31 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs 
     uint32_t fill = 0, kept = 0;
     const unsigned lt_mask = (1u << lane) - 1u;
 
+    // Each lane evaluates one candidate, reading that candidate's row with
+    // 16-byte loads (4 dimensions, consumed in order) and the query row as
+    // broadcast pairs from shared memory.
     auto flush = [&](uint32_t m) {
         for (uint32_t b = 0; b < m; b += 32) {
             const bool mine = b + lane < m;
             const uint32_t j = mine ? list[b + lane] : row;
-            offs[lane] = (unsigned long long)j * a.d;
-            __syncwarp();
-            // candidate rows are staged 32 dimensions at a time; the next
-            // slice is loaded into registers while this one is consumed
-            float pre[32];
-            auto load = [&](uint32_t c0) {
-                const uint32_t c = c0 + lane;
-#pragma unroll
-                for (int r = 0; r < 32; ++r) pre[r] = (c < a.d) ? __ldg(a.x + offs[r] + c) : 0.0f;
-            };
-            load(0);
+            const float *xj = a.x + (size_t)j * a.d;
             double acc = 0.0;
-            for (uint32_t c0 = 0; c0 < a.d; c0 += RR_CH) {
-#pragma unroll
-                for (int r = 0; r < 32; ++r) tile[lane * 33 + r] = pre[r];
-                __syncwarp();
-                if (c0 + RR_CH < a.d) load(c0 + RR_CH);
-                const uint32_t tn = min((uint32_t)RR_CH, a.d - c0);
-                for (uint32_t t = 0; t < tn; ++t) {
-                    const double y = (double)tile[t * 33 + lane];
-                    if (METRIC == HM_METRIC_EUCLIDEAN) {
-                        const double diff = __dsub_rn(xi[c0 + t], y);
-                        acc = __dadd_rn(acc, __dmul_rn(diff, diff));
-                    } else {
-                        acc = __dadd_rn(acc, __dmul_rn(xi[c0 + t], y));
-                    }
+            uint32_t t = 0;
+            if ((a.d & 3u) == 0) {
+                const float4 *xj4 = reinterpret_cast<const float4 *>(xj);
+                const double2 *xi2 = reinterpret_cast<const double2 *>(xi);
+#pragma unroll 4
+                for (uint32_t q = 0; q < a.d / 4; ++q) {
+                    const float4 y = __ldg(xj4 + q);
+                    const double2 p0 = xi2[2 * q], p1 = xi2[2 * q + 1];
+                    acc = step<METRIC>(acc, p0.x, (double)y.x);
+                    acc = step<METRIC>(acc, p0.y, (double)y.y);
+                    acc = step<METRIC>(acc, p1.x, (double)y.z);
+                    acc = step<METRIC>(acc, p1.y, (double)y.w);
                 }
-                __syncwarp();
+                t = a.d;
             }
+            for (; t < a.d; ++t) acc = step<METRIC>(acc, xi[t], (double)__ldg(xj + t));
             uint64_t key = KEY_NONE;
             if (mine) {
                 float dist;
@@ -179,10 +170,8 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs 
 
 template <int METRIC>
 static int launch_metric(const RerankArgs &a, uint32_t kpl, cudaStream_t s) {
-    const uint32_t dstride = (uint32_t)round_up(a.d, 2);
-    const size_t smem = (size_t)RR_WARPS * dstride * sizeof(double) +
-                        (size_t)RR_WARPS * RR_CH * 33 * sizeof(float) + RR_WARPS * RR_LIST * sizeof(uint32_t) +
-                        RR_WARPS * 32 * sizeof(unsigned long long);
+    const uint32_t dstride = (uint32_t)round_up(a.d, 4);
+    const size_t smem = (size_t)RR_WARPS * dstride * sizeof(double) + RR_WARPS * RR_LIST * sizeof(uint32_t);
     const int blocks = (int)((a.n + RR_WARPS - 1) / RR_WARPS);
 #define HM_RR_CASE(K)                                                                       \
     case K: {                                                                               \

@@ -110,7 +110,7 @@ int screen_plan(uint64_t n, uint32_t d, uint32_t k, int metric, int path, Screen
     L.off_cnt = off;
     off = a256(off + (size_t)n * L.parts * 2 * sizeof(uint32_t));
     L.off_tau = off;
-    off = a256(off + (size_t)n * L.parts * 2 * sizeof(float));
+    off = a256(off + (size_t)n * L.parts * 2 * k * sizeof(float));
     L.off_ovf = off;
     off = a256(off + (size_t)n * sizeof(uint32_t));
     L.off_ovf_cnt = off;
@@ -198,7 +198,7 @@ int screen_run(const ScreenRun &r, const ScreenLayout &L, char *ws, cudaStream_t
     g.band = reinterpret_cast<float *>(ws + L.off_band);
     g.cand = reinterpret_cast<unsigned long long *>(ws + L.off_cand);
     g.cand_cnt = reinterpret_cast<uint32_t *>(ws + L.off_cnt);
-    g.part_tau = reinterpret_cast<float *>(ws + L.off_tau);
+    g.part_topk = reinterpret_cast<float *>(ws + L.off_tau);
     g.error_code = &r.counters->error_code;
     g.emitted = &r.counters->emitted;
     g.zero_rows = reinterpret_cast<unsigned long long *>(ws + L.off_max) + 7;
@@ -219,7 +219,7 @@ int screen_run(const ScreenRun &r, const ScreenLayout &L, char *ws, cudaStream_t
     ra.cap = L.cap;
     ra.cand = g.cand;
     ra.cand_cnt = g.cand_cnt;
-    ra.part_tau = g.part_tau;
+    ra.part_topk = g.part_topk;
     ra.band = g.band;
     ra.force_exact = reinterpret_cast<uint8_t *>(ws + L.off_force);
     ra.ovf_list = reinterpret_cast<uint32_t *>(ws + L.off_ovf);
@@ -229,7 +229,9 @@ int screen_run(const ScreenRun &r, const ScreenLayout &L, char *ws, cudaStream_t
     ra.counters = r.counters;
     HM_TRY(launch_rerank(ra, r.metric, L.kpl, s));
 
-    // exact plain path for the rows the screen could not settle
+    // exact plain path for the rows the screen could not settle (its binary64
+    // copy of the points is built only when such rows exist)
+    HM_TRY(launch_prep_x64(r.data, r.n, r.d, r.ldd, r.n_pad, const_cast<double *>(r.x64), ovf_cnt, s));
     PlainArgs pl{};
     pl.x64 = r.x64;
     pl.rnorm = r.rnorm;

@@ -73,7 +73,7 @@ struct ScreenRun {
     const float *data;
     const double *x64;
     const double *rnorm;
-    uint32_t n, d, ldd, k;
+    uint32_t n, d, ldd, n_pad, k;
     int metric, path;
     uint32_t *idx_out;
     float *dist_out;
@@ -116,7 +116,7 @@ struct ScreenGemmArgs {
     const float *band;        // per row keep band 2E_i
     unsigned long long *cand; // [slot*cap] = (c^ bits << 32) | j, slot = (row*parts + part)*2 + half
     uint32_t *cand_cnt;       // [slot]
-    float *part_tau;          // [slot]
+    float *part_topk;         // [slot * k]: each list's k smallest c^, ascending
     uint32_t *error_code;
     unsigned long long *emitted;
     const unsigned long long *zero_rows;  // cosine: rows with ||x|| = 0
@@ -133,7 +133,7 @@ struct RerankArgs {
     uint32_t n, d, k, parts, cap;
     const unsigned long long *cand;
     const uint32_t *cand_cnt;
-    const float *part_tau;
+    const float *part_topk;
     const float *band;
     const uint8_t *force_exact;
     uint32_t *ovf_list;

@@ -477,8 +477,13 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                 if (lane == 0) mbar_arrive(smem_u32(&acce[buf]));
             }
             if (valid) {
+                // the list's k smallest screened values (sorted; the global k
+                // smallest of the row are all among the union of these)
                 g.cand_cnt[slot] = cnt;
-                g.part_tau[slot] = arr[KP - 1];
+                float *kk = g.part_topk + slot * g.k;
+#pragma unroll
+                for (int q = 0; q < KP; ++q)
+                    if (q >= KP - (int)g.k) kk[q - (KP - (int)g.k)] = arr[q];
                 atomicAdd(g.emitted, (unsigned long long)cnt);
             }
         }
