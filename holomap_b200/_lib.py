@@ -111,6 +111,23 @@ class HmStats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class HmJob(ctypes.Structure):
+    """``hm_job`` of include/holomap_cuda.h (device pointers)."""
+
+    _fields_ = [
+        ("data", ctypes.c_void_p),
+        ("n", ctypes.c_uint64),
+        ("d", ctypes.c_uint32),
+        ("k", ctypes.c_uint32),
+        ("metric", ctypes.c_int32),
+        ("path", ctypes.c_int32),
+        ("idx_out", ctypes.c_void_p),
+        ("dist_out", ctypes.c_void_p),
+        ("sigma_out", ctypes.c_void_p),
+        ("rho_out", ctypes.c_void_p),
+    ]
+
+
 # (name, restype, argtypes) for every symbol of include/holomap_cuda.h
 _u64, _u32, _i32, _vp, _sz = (ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p,
                               ctypes.c_size_t)
@@ -133,6 +150,14 @@ SIGNATURES = {
     "hm_knn_smooth_noalloc": (_i32, [_vp, _u64, _u32, _u32, _i32, _vp, _vp, _vp, _vp, _vp]),
     "hm_noalloc_scratch_bytes": (_sz, []),
     "hm_debug_set_screen_dump": (_i32, [_vp]),
+    "hm_batch_create": (_i32, [_vp, _u32, _vp]),
+    "hm_batch_destroy": (None, [_vp]),
+    "hm_batch_workspace_bytes": (_sz, [_vp]),
+    "hm_batch_bind": (_i32, [_vp, _vp, _sz, _vp]),
+    "hm_batch_run": (_i32, [_vp, _vp]),
+    "hm_batch_graph_launch": (_i32, [_vp, _vp]),
+    "hm_batch_job_stats": (_i32, [_vp, _u32, _vp]),
+    "hm_batch_job_path": (_i32, [_vp, _u32]),
 }
 
 KCLASS = {"bulk": 0, "select": 1, "smooth": 2, "prep": 3}

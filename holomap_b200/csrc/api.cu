@@ -1,19 +1,29 @@
-// api.cu -- the extern "C" entry points of libholomap_cuda.so.
+// api.cu -- the extern "C" entry points of libholomap_cuda.so and the batch
+// planner / executor behind them.
 //
 // Host side of the drop-in for src/api.rs:147-148 (exact_knn + smooth_knn).
-// Validation mirrors src/api.rs:114-145; the device pipeline is
-//   prep -> distance bulk (plain or screened) -> [split merge] -> smooth-kNN
-//   -> global-mean floor for rows without a positive distance,
-// all stream-ordered, with one host<->device round trip for the host-pointer
-// entry points.
+// Every call is a batch of jobs (a single call is a batch of one).  The plan
+// resolves each job's path (exact plain path, or a tensor-core screen whose
+// operand format groups the jobs), lays out every buffer in one workspace
+// and writes the job tables; the run enqueues, on one stream:
+//   init counters + input check + cosine norms        (all jobs)
+//   binary64 copies + exact plain kernel              (exact-path jobs)
+//   screen prep -> band -> screen -> rerank           (per screen group)
+//   binary64 copies + plain kernel on fallback rows   (screened jobs)
+//   split merge                                       (exact jobs with splits)
+//   smooth-kNN + global-mean floors                   (all jobs with outputs)
+// Validation mirrors src/api.rs:114-145 on exact_knn's own domain.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
+#include <new>
 #include <string>
+#include <vector>
 
 #include "hm_internal.cuh"
 #include "screen.cuh"
@@ -34,9 +44,30 @@ int set_error(int code, const char *fmt, ...) {
 
 void clear_error() { g_last_error.clear(); }
 
+// tensor maps and the test hook live in screen.cu
+int make_operand_map(CUtensorMap *m, void *base, uint64_t rows, uint32_t kpmax, uint32_t elem_bytes,
+                     uint32_t kslice, uint32_t box_rows);
+float *debug_dump_pointer();
+
+static size_t align256(size_t x) { return round_up(x, 256); }
+
+static uint32_t pow2ceil(uint32_t v) {
+    uint32_t p = 1;
+    while (p < v) p <<= 1;
+    return p;
+}
+
+static int sm_count() {
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
+        return sms;
+    cudaGetLastError();  // no device here: plan for a B200
+    return 148;
+}
+
 // ------------------------------------------------------------ validation
-static int validate_knn(const void *data, uint64_t n, uint32_t d, uint32_t k, int metric) {
-    if (!data) return set_error(HM_ERR_INVALID, "data is NULL");
+static int validate_shape(uint64_t n, uint32_t d, uint32_t k, int metric) {
     if (d == 0 || n == 0)
         return set_error(HM_ERR_INVALID, "bad shape: n=%llu rows of n_features=%u",
                          (unsigned long long)n, d);
@@ -49,159 +80,519 @@ static int validate_knn(const void *data, uint64_t n, uint32_t d, uint32_t k, in
                          (unsigned long long)n);
     if (metric < HM_METRIC_EUCLIDEAN || metric > HM_METRIC_MANHATTAN)
         return set_error(HM_ERR_INVALID, "unknown metric %d", metric);
-    if (n > 0xffffffffull)
-        return set_error(HM_ERR_UNSUPPORTED, "n=%llu exceeds the u32 index range",
+    if (n > 0x7fffffffull)
+        return set_error(HM_ERR_UNSUPPORTED, "n=%llu exceeds the supported index range",
                          (unsigned long long)n);
     if (kpl_for_k(k) == 0)
         return set_error(HM_ERR_UNSUPPORTED, "k=%u exceeds the largest supported k (256)", k);
     return HM_OK;
 }
 
-// ------------------------------------------------------------- workspace
-static size_t align256(size_t x) { return round_up(x, 256); }
-
-struct Layout {
-    int path = HM_PATH_PLAIN;
-    uint32_t ldd = 0, n_pad = 0, splits = 1, split_cols = 0;
-    size_t off_flags = 0;    // Flags
-    size_t off_x64 = 0, off_rnorm = 0, off_partial = 0, off_zero_rows = 0;
-    size_t off_screen = 0;   // screened path workspace
-    ScreenLayout screen;
-    size_t total = 0;
-};
-
-// Device-side counters left in the workspace for hm_stats_from_workspace.
-struct Flags {
-    uint32_t zero_count;
-    uint32_t nonfinite_min;   // smallest flat index of a non-finite input, or ~0
-    uint32_t pad[2];
-    ScreenCounters screen;
-};
-
-static int resolve_path(uint64_t n, uint32_t d, uint32_t k, int metric, int path) {
-    if (path == HM_PATH_AUTO) return hm_autotune_path(n, d, k, metric);
-    return path;
+static bool screen_capable(uint32_t d, uint32_t k, int metric) {
+    return metric != HM_METRIC_MANHATTAN && k <= 64 && d <= 2048;
 }
 
-static int plan(uint64_t n, uint32_t d, uint32_t k, int metric, int path, Layout &L) {
-    L.path = resolve_path(n, d, k, metric, path);
-    if (L.path < HM_PATH_PLAIN || L.path > HM_PATH_SCREEN_BF16X3)
-        return set_error(HM_ERR_INVALID, "unknown path %d", path);
-    if (L.path != HM_PATH_PLAIN && metric == HM_METRIC_MANHATTAN)
-        return set_error(HM_ERR_UNSUPPORTED,
-                         "manhattan has no inner-product form; use the plain path");
-    L.ldd = (uint32_t)round_up(d, PL_BK);
-    L.n_pad = (uint32_t)(round_up(n, PL_ROW_PAD) + PL_ROW_PAD);
-    const uint32_t row_blocks = (uint32_t)((n + PL_BM - 1) / PL_BM);
-    const uint32_t col_tiles = (uint32_t)((n + PL_BN - 1) / PL_BN);
-    uint32_t splits = (1184 + row_blocks - 1) / row_blocks;  // ~4 CTAs per SM slot
-    uint32_t max_splits = col_tiles / 2 ? col_tiles / 2 : 1;
-    if (splits > max_splits) splits = max_splits;
-    if (splits > 32) splits = 32;
-    if (splits < 1) splits = 1;
-    L.split_cols = (uint32_t)round_up((n + splits - 1) / splits, PL_BN);
-    L.splits = (uint32_t)((n + L.split_cols - 1) / L.split_cols);
+// ------------------------------------------------------------------ plan
+struct JobPlan {
+    hm_job spec{};
+    int path = HM_PATH_PLAIN;
+    uint32_t ldd = 0, n_pad = 0, splits = 1, split_cols = 0, arow0 = 0;
+    size_t off_x64 = 0, off_rnorm = 0, off_partial = 0, off_zero_rows = 0, off_ovf = 0;
+    size_t off_mu = 0, off_csum = 0;
+    int group = -1;
+    uint32_t row0 = 0, unit0 = 0, kp1 = 0, k_stages = 0, row_blocks = 0, col_tiles = 0;
+    uint32_t parts = 1, part_tiles = 0, cap = 0;
+    uint64_t slot0 = 0, cand0 = 0, topk0 = 0;
+};
 
-    size_t off = 0;
-    L.off_flags = off;
-    off = align256(off + sizeof(Flags));
-    L.off_zero_rows = off;
-    off = align256(off + n * sizeof(uint32_t));
-    L.off_x64 = off;
-    off = align256(off + (size_t)L.n_pad * L.ldd * sizeof(double));
-    L.off_rnorm = off;
-    off = align256(off + (size_t)L.n_pad * sizeof(double));
-    L.off_partial = off;
-    if (L.splits > 1) off = align256(off + (size_t)L.splits * n * k * sizeof(uint64_t));
-    L.off_screen = off;
-    if (L.path != HM_PATH_PLAIN) {
-        HM_TRY(screen_plan(n, d, k, metric, L.path, L.screen));
-        off = align256(off + L.screen.total);
+struct GroupPlan {
+    int kind = SCREEN_KIND_BF16;
+    bool split = false;
+    uint32_t elem_bytes = 2, kslice = 64, kpmax = 0, rows = 0, units = 0;
+    uint32_t kp = 32, kpl = 1, dmax = 0;
+    int metric_mask = 0;
+    std::vector<uint32_t> jobs;
+    uint64_t lists = 0, cand = 0, topk = 0;
+    size_t off_opa = 0, off_opb = 0, off_rowstat = 0, off_rowterm = 0, off_colterm = 0;
+    size_t off_band = 0, off_force = 0, off_rowthr = 0, off_cand = 0, off_cnt = 0, off_topk = 0;
+    // tables
+    size_t off_gdev = 0, off_job_ids = 0, off_row_starts = 0, off_unit_starts = 0;
+    GroupDev host{};
+    CUtensorMap ta{}, tb{};
+};
+
+}  // namespace hm
+
+struct hm_batch {
+    std::vector<hm::JobPlan> jobs;
+    hm::GroupPlan groups[3];  // bf16, tf32, split bf16
+    uint32_t all_rows = 0, kpl_all = 1, kpl_plain[3] = {1, 1, 1}, kpl_fb[3] = {1, 1, 1};
+    std::vector<uint2> items[3];       // exact-path work per metric
+    std::vector<uint32_t> fb_jobs[3];  // screened jobs per metric (fallback rows)
+    uint32_t fb_per_job[3] = {1, 1, 1};
+    std::vector<uint32_t> job_blocks;  // prep block offsets
+    bool any_plain = false, any_screen = false, any_smooth = false, any_split = false;
+    size_t off_tables = 0, off_jobs = 0, off_counters = 0, off_row_starts = 0, off_job_blocks = 0;
+    size_t off_items[3] = {}, off_fb[3] = {};
+    size_t tables_bytes = 0, total = 0;
+    // bound state
+    char *ws = nullptr;
+    std::vector<char> table;           // host image of the tables
+    void *pinned = nullptr;            // pinned staging for large tables
+    cudaGraphExec_t graph = nullptr;
+    cudaStream_t capture = nullptr;    // private stream the graph is captured on
+    ~hm_batch() {
+        if (graph) cudaGraphExecDestroy(graph);
+        if (capture) cudaStreamDestroy(capture);
+        if (pinned) cudaFreeHost(pinned);
     }
-    L.total = off;
+};
+
+namespace hm {
+
+static int group_of_path(int path) {
+    switch (path) {
+    case HM_PATH_SCREEN_BF16: return 0;
+    case HM_PATH_SCREEN_TF32: return 1;
+    case HM_PATH_SCREEN_BF16X3: return 2;
+    default: return -1;
+    }
+}
+
+static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B) {
+    if (njobs == 0) return set_error(HM_ERR_INVALID, "empty batch");
+    if (njobs > (1u << 16)) return set_error(HM_ERR_UNSUPPORTED, "more than 65536 jobs");
+    const uint32_t G = (uint32_t)sm_count();
+    B.jobs.assign(njobs, JobPlan{});
+    for (int g = 0; g < 3; ++g) B.groups[g] = GroupPlan{};
+    B.groups[0].kind = SCREEN_KIND_BF16;
+    B.groups[1].kind = SCREEN_KIND_TF32;
+    B.groups[1].elem_bytes = 4;
+    B.groups[2].split = true;
+    for (int g = 0; g < 3; ++g) B.groups[g].kslice = SC_SLICE_BYTES / B.groups[g].elem_bytes;
+
+    // paths and exact-path geometry
+    uint64_t plain_groups = 0;
+    for (uint32_t j = 0; j < njobs; ++j) {
+        JobPlan &P = B.jobs[j];
+        P.spec = specs[j];
+        const hm_job &s = P.spec;
+        HM_TRY(validate_shape(s.n, s.d, s.k, s.metric));
+        int path = s.path;
+        if (path == HM_PATH_AUTO) path = hm_autotune_path(s.n, s.d, s.k, s.metric);
+        if (path < HM_PATH_PLAIN || path > HM_PATH_SCREEN_BF16X3)
+            return set_error(HM_ERR_INVALID, "unknown path %d", s.path);
+        if (path != HM_PATH_PLAIN && !screen_capable(s.d, s.k, s.metric))
+            return set_error(HM_ERR_UNSUPPORTED,
+                             "the screened paths need euclidean or cosine, k <= 64 and d <= 2048");
+        P.path = path;
+        P.ldd = (uint32_t)round_up(s.d, PL_BK);
+        P.n_pad = (uint32_t)(round_up(s.n, PL_ROW_PAD) + PL_ROW_PAD);
+        P.arow0 = B.all_rows;
+        B.all_rows += (uint32_t)s.n;
+        B.kpl_all = std::max<uint32_t>(B.kpl_all, (uint32_t)kpl_for_k(s.k));
+        if (s.sigma_out && s.rho_out) B.any_smooth = true;
+        if (path == HM_PATH_PLAIN) plain_groups += (s.n + PL_BM - 1) / PL_BM;
+    }
+    // column splits of the exact path: about 4 CTAs per SM slot over the batch
+    uint32_t S = plain_groups ? (uint32_t)((1184 + plain_groups - 1) / plain_groups) : 1;
+    S = std::min<uint32_t>(std::max<uint32_t>(S, 1), 32);
+    for (uint32_t j = 0; j < njobs; ++j) {
+        JobPlan &P = B.jobs[j];
+        const uint64_t n = P.spec.n;
+        const uint32_t col_tiles = (uint32_t)((n + PL_BN - 1) / PL_BN);
+        uint32_t splits = 1;
+        if (P.path == HM_PATH_PLAIN) {
+            splits = std::min<uint32_t>(S, std::max<uint32_t>(1, col_tiles / 2));
+            B.any_plain = true;
+        }
+        P.split_cols = (uint32_t)round_up((n + splits - 1) / splits, PL_BN);
+        P.splits = (uint32_t)((n + P.split_cols - 1) / P.split_cols);
+        if (P.splits > 1) B.any_split = true;
+    }
+
+    // screen groups
+    for (uint32_t j = 0; j < njobs; ++j) {
+        JobPlan &P = B.jobs[j];
+        const int g = group_of_path(P.path);
+        if (g < 0) continue;
+        GroupPlan &Gp = B.groups[g];
+        P.group = g;
+        Gp.jobs.push_back(j);
+        B.any_screen = true;
+        P.kp1 = (uint32_t)round_up(P.spec.d, Gp.kslice);
+        const uint32_t kp = Gp.split ? 3 * P.kp1 : P.kp1;
+        P.k_stages = kp / Gp.kslice;
+        Gp.kpmax = std::max(Gp.kpmax, kp);
+        Gp.dmax = std::max(Gp.dmax, P.spec.d);
+        if (P.spec.k > 32) {
+            Gp.kp = 64;
+            Gp.kpl = 2;
+        }
+        Gp.metric_mask |= 1 << P.spec.metric;
+        P.row_blocks = (uint32_t)((P.spec.n + SC_BM - 1) / SC_BM);
+        P.col_tiles = (uint32_t)((P.spec.n + SC_BN - 1) / SC_BN);
+    }
+    for (int g = 0; g < 3; ++g) {
+        GroupPlan &Gp = B.groups[g];
+        if (Gp.jobs.empty()) continue;
+        uint64_t units1 = 0;
+        for (uint32_t j : Gp.jobs) units1 += B.jobs[j].row_blocks;
+        for (uint32_t j : Gp.jobs) {
+            JobPlan &P = B.jobs[j];
+            if (Gp.jobs.size() == 1) {
+                // one job: balance the persistent grid (makespan in tiles)
+                // against the extra lists each column part costs
+                double best = 1e300;
+                for (uint32_t sp = 1; sp <= 8 && sp <= P.col_tiles; ++sp) {
+                    const uint32_t pt = (P.col_tiles + sp - 1) / sp;
+                    const uint32_t parts = (P.col_tiles + pt - 1) / pt;
+                    const uint64_t units = (uint64_t)P.row_blocks * parts;
+                    const double cost = (double)((units + G - 1) / G) * pt * (1.0 + 0.03 * parts);
+                    if (cost < best - 1e-9) {
+                        best = cost;
+                        P.part_tiles = pt;
+                        P.parts = parts;
+                    }
+                }
+            } else {
+                uint32_t parts = units1 >= G ? 1u : (uint32_t)((G + units1 - 1) / units1);
+                parts = std::min<uint32_t>(std::min<uint32_t>(parts, 8), P.col_tiles);
+                P.part_tiles = (P.col_tiles + parts - 1) / parts;
+                P.parts = (P.col_tiles + P.part_tiles - 1) / P.part_tiles;
+            }
+            const double per_list = (double)P.spec.n / (2.0 * P.parts);
+            const double expect = 1.5 * P.spec.k * (2.0 + std::log(std::fmax(1.0, per_list / P.spec.k)));
+            P.cap = std::min<uint32_t>(std::max<uint32_t>(pow2ceil((uint32_t)expect), 128), 4096);
+            P.row0 = Gp.rows;
+            Gp.rows += (uint32_t)round_up(P.spec.n, 32);  // rows of each job start 32-aligned
+            P.unit0 = Gp.units;
+            Gp.units += P.row_blocks * P.parts;
+            P.slot0 = Gp.lists;
+            const uint64_t lists = P.spec.n * 2ull * P.parts;
+            Gp.lists += lists;
+            P.cand0 = Gp.cand;
+            Gp.cand += lists * P.cap;
+            P.topk0 = Gp.topk;
+            Gp.topk += lists * P.spec.k;
+        }
+    }
+
+    // work tables of the exact path and of the screened fallback
+    for (uint32_t j = 0; j < njobs; ++j) {
+        const JobPlan &P = B.jobs[j];
+        const int m = P.spec.metric;
+        if (P.path == HM_PATH_PLAIN) {
+            const uint32_t groups = (uint32_t)((P.spec.n + PL_BM - 1) / PL_BM);
+            for (uint32_t gi = 0; gi < groups; ++gi)
+                for (uint32_t sp = 0; sp < P.splits; ++sp) B.items[m].push_back(make_uint2(j, gi << 6 | sp));
+            B.kpl_plain[m] = std::max<uint32_t>(B.kpl_plain[m], (uint32_t)kpl_for_k(P.spec.k));
+        } else {
+            B.fb_jobs[m].push_back(j);
+            B.kpl_fb[m] = std::max<uint32_t>(B.kpl_fb[m], (uint32_t)kpl_for_k(P.spec.k));
+        }
+    }
+    for (int m = 0; m < 3; ++m)
+        if (!B.fb_jobs[m].empty())
+            B.fb_per_job[m] = std::max<uint32_t>(
+                1, std::min<uint32_t>(64, (uint32_t)((2 * G + B.fb_jobs[m].size() - 1) / B.fb_jobs[m].size())));
+    // prep blocks: about one block per 2048 elements of a job, at most 2048
+    B.job_blocks.assign(njobs + 1, 0);
+    for (uint32_t j = 0; j < njobs; ++j) {
+        const JobPlan &P = B.jobs[j];
+        const uint64_t work = std::max<uint64_t>(P.spec.n * P.spec.d, (uint64_t)P.n_pad * P.ldd);
+        const uint32_t b = (uint32_t)std::min<uint64_t>(2048, std::max<uint64_t>(1, (work + 2047) / 2048));
+        B.job_blocks[j + 1] = B.job_blocks[j] + b;
+    }
+
+    // ---------------------------------------------------------- layout
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        const size_t where = off;
+        off = align256(off + std::max<size_t>(bytes, 1));
+        return where;
+    };
+    // tables (written by bind, contiguous)
+    B.off_tables = off;
+    B.off_jobs = take(sizeof(JobDev) * njobs);
+    B.off_row_starts = take(sizeof(uint32_t) * (njobs + 1));
+    B.off_job_blocks = take(sizeof(uint32_t) * (njobs + 1));
+    for (int m = 0; m < 3; ++m) {
+        B.off_items[m] = take(sizeof(uint2) * B.items[m].size());
+        B.off_fb[m] = take(sizeof(uint32_t) * B.fb_jobs[m].size());
+    }
+    for (int g = 0; g < 3; ++g) {
+        GroupPlan &Gp = B.groups[g];
+        if (Gp.jobs.empty()) continue;
+        Gp.off_gdev = take(sizeof(GroupDev));
+        Gp.off_job_ids = take(sizeof(uint32_t) * Gp.jobs.size());
+        Gp.off_row_starts = take(sizeof(uint32_t) * (Gp.jobs.size() + 1));
+        Gp.off_unit_starts = take(sizeof(uint32_t) * (Gp.jobs.size() + 1));
+    }
+    B.tables_bytes = off - B.off_tables;
+    // device-written
+    B.off_counters = take(sizeof(JobCounters) * njobs);
+    for (uint32_t j = 0; j < njobs; ++j) {
+        JobPlan &P = B.jobs[j];
+        const uint64_t n = P.spec.n;
+        P.off_x64 = take((size_t)P.n_pad * P.ldd * sizeof(double));  // exact path or fallback rows
+        P.off_rnorm = take((size_t)P.n_pad * sizeof(double));
+        P.off_zero_rows = take(n * sizeof(uint32_t));
+        if (P.splits > 1) P.off_partial = take((size_t)P.splits * n * P.spec.k * sizeof(uint64_t));
+        if (P.group >= 0) {
+            P.off_ovf = take(n * sizeof(uint32_t));
+            P.off_mu = take((size_t)P.spec.d * sizeof(double));
+            P.off_csum = take((size_t)64 * P.spec.d * sizeof(double));
+        }
+    }
+    for (int g = 0; g < 3; ++g) {
+        GroupPlan &Gp = B.groups[g];
+        if (Gp.jobs.empty()) continue;
+        const size_t rows = Gp.rows;
+        Gp.off_opa = take(rows * Gp.kpmax * Gp.elem_bytes);
+        Gp.off_opb = Gp.split ? take(rows * Gp.kpmax * Gp.elem_bytes) : Gp.off_opa;
+        Gp.off_rowstat = take(rows * sizeof(RowStat));
+        Gp.off_rowterm = take(rows * sizeof(float));
+        Gp.off_colterm = take((round_up(rows, SC_BN) + SC_BN) * sizeof(float));
+        Gp.off_band = take(rows * sizeof(float));
+        Gp.off_force = take(rows);
+        Gp.off_rowthr = take(rows * sizeof(uint32_t));
+        Gp.off_cand = take(Gp.cand * sizeof(unsigned long long));
+        Gp.off_cnt = take(Gp.lists * sizeof(uint32_t));
+        Gp.off_topk = take(Gp.topk * sizeof(float));
+    }
+    B.total = off;
     return HM_OK;
 }
 
-// ------------------------------------------------------- device pipeline
-__global__ void check_finite_kernel(const float *__restrict__ x, uint64_t total,
-                                    uint32_t *__restrict__ first_bad) {
-    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < total;
-         t += (uint64_t)gridDim.x * blockDim.x) {
-        if (!isfinite(x[t])) atomicMin(first_bad, (uint32_t)(t < 0xfffffffeull ? t : 0xfffffffeull));
-    }
+// --------------------------------------------------------------- binding
+// Small tables are written by a kernel from its parameters (no host memory
+// stays referenced); larger ones by one copy from pinned staging.
+constexpr uint32_t kParamTable = 3072;
+struct ParamTable {
+    uint32_t bytes;
+    unsigned char data[kParamTable];
+};
+
+__global__ void write_table_kernel(char *dst, const ParamTable t) {
+    for (uint32_t i = threadIdx.x; i < t.bytes; i += blockDim.x) dst[i] = (char)t.data[i];
 }
 
-__global__ void init_flags_kernel(Flags *f) {
-    if (threadIdx.x == 0) {
-        f->zero_count = 0;
-        f->nonfinite_min = 0xffffffffu;
-        f->screen = ScreenCounters{};
-    }
+template <typename T>
+static T *at(char *base, size_t off) {
+    return reinterpret_cast<T *>(base + off);
 }
 
-static int run_knn(const float *d_data, uint64_t n, uint32_t d, uint32_t k, int metric,
-                   const Layout &L, char *ws, uint32_t *d_idx, float *d_dist, cudaStream_t s) {
-    Flags *flags = reinterpret_cast<Flags *>(ws + L.off_flags);
-    {
-        ScopedKernelTimer timer(HM_KCLASS_PREP, s);
-        init_flags_kernel<<<1, 32, 0, s>>>(flags);
+static int bind_batch(hm_batch &B, void *d_ws, size_t bytes, cudaStream_t s) {
+    if (!d_ws) return set_error(HM_ERR_INVALID, "workspace is NULL");
+    if (bytes < B.total)
+        return set_error(HM_ERR_INVALID, "workspace of %zu bytes is below the %zu needed", bytes, B.total);
+    if (reinterpret_cast<uintptr_t>(d_ws) % 256)
+        return set_error(HM_ERR_INVALID, "workspace must be 256-byte aligned");
+    char *ws = static_cast<char *>(d_ws);
+    B.ws = ws;
+    if (B.graph) {
+        cudaGraphExecDestroy(B.graph);
+        B.graph = nullptr;
+    }
+    const uint32_t njobs = (uint32_t)B.jobs.size();
+    B.table.assign(B.tables_bytes, 0);
+    char *host = B.table.data() - B.off_tables;  // host image addressed like the workspace
+
+    std::vector<uint32_t> row_starts(njobs + 1, 0);
+    for (uint32_t j = 0; j < njobs; ++j) {
+        const JobPlan &P = B.jobs[j];
+        const hm_job &s = P.spec;
+        JobDev J{};
+        J.n = (uint32_t)s.n;
+        J.d = s.d;
+        J.k = s.k;
+        J.metric = (uint32_t)s.metric;
+        J.path = (uint32_t)P.path;
+        J.arow0 = P.arow0;
+        J.x = s.data;
+        J.idx = s.idx_out;
+        J.dist = s.dist_out;
+        J.sigma = (s.sigma_out && s.rho_out) ? s.sigma_out : nullptr;
+        J.rho = (s.sigma_out && s.rho_out) ? s.rho_out : nullptr;
+        J.x64 = at<double>(ws, P.off_x64);
+        J.rnorm = at<double>(ws, P.off_rnorm);
+        J.ldd = P.ldd;
+        J.n_pad = P.n_pad;
+        J.splits = P.splits;
+        J.split_cols = P.split_cols;
+        J.partial = P.splits > 1 ? at<uint64_t>(ws, P.off_partial) : nullptr;
+        J.target = std::log2((double)s.k);  // src/smooth_knn.rs:25 (platform log2)
+        J.zero_rows = at<uint32_t>(ws, P.off_zero_rows);
+        J.group = P.group < 0 ? 0u : (uint32_t)P.group;
+        J.row0 = P.row0;
+        J.unit0 = P.unit0;
+        J.kp1 = P.kp1;
+        J.k_stages = P.k_stages;
+        J.row_blocks = P.row_blocks;
+        J.col_tiles = P.col_tiles;
+        J.parts = P.parts;
+        J.part_tiles = P.part_tiles;
+        J.cap = P.cap;
+        J.slot0 = P.slot0;
+        J.cand0 = P.cand0;
+        J.topk0 = P.topk0;
+        J.scale = s.metric == HM_METRIC_EUCLIDEAN ? 2.0f : 1.0f;
+        J.mu = P.group >= 0 ? at<double>(ws, P.off_mu) : nullptr;
+        J.csum = P.group >= 0 ? at<double>(ws, P.off_csum) : nullptr;
+        J.ovf_list = P.group >= 0 ? at<uint32_t>(ws, P.off_ovf) : nullptr;
+        J.cnt = at<JobCounters>(ws, B.off_counters) + j;
+        at<JobDev>(host, B.off_jobs)[j] = J;
+        row_starts[j + 1] = row_starts[j] + J.n;
+    }
+    memcpy(host + B.off_row_starts, row_starts.data(), sizeof(uint32_t) * (njobs + 1));
+    memcpy(host + B.off_job_blocks, B.job_blocks.data(), sizeof(uint32_t) * (njobs + 1));
+    for (int m = 0; m < 3; ++m) {
+        if (!B.items[m].empty())
+            memcpy(host + B.off_items[m], B.items[m].data(), sizeof(uint2) * B.items[m].size());
+        if (!B.fb_jobs[m].empty())
+            memcpy(host + B.off_fb[m], B.fb_jobs[m].data(), sizeof(uint32_t) * B.fb_jobs[m].size());
+    }
+    for (int g = 0; g < 3; ++g) {
+        GroupPlan &Gp = B.groups[g];
+        if (Gp.jobs.empty()) continue;
+        const uint32_t gj = (uint32_t)Gp.jobs.size();
+        std::vector<uint32_t> rs(gj + 1), us(gj + 1);
+        for (uint32_t i = 0; i < gj; ++i) {
+            const JobPlan &P = B.jobs[Gp.jobs[i]];
+            rs[i] = P.row0;
+            us[i] = P.unit0;
+        }
+        rs[gj] = Gp.rows;
+        us[gj] = Gp.units;
+        memcpy(host + Gp.off_job_ids, Gp.jobs.data(), sizeof(uint32_t) * gj);
+        memcpy(host + Gp.off_row_starts, rs.data(), sizeof(uint32_t) * (gj + 1));
+        memcpy(host + Gp.off_unit_starts, us.data(), sizeof(uint32_t) * (gj + 1));
+        GroupDev D{};
+        D.rows = Gp.rows;
+        D.njobs = gj;
+        D.units = Gp.units;
+        D.kind = (uint32_t)Gp.kind;
+        D.split = Gp.split ? 1u : 0u;
+        D.elem_bytes = Gp.elem_bytes;
+        D.kslice = Gp.kslice;
+        D.kpmax = Gp.kpmax;
+        D.job_ids = at<uint32_t>(ws, Gp.off_job_ids);
+        D.row_starts = at<uint32_t>(ws, Gp.off_row_starts);
+        D.unit_starts = at<uint32_t>(ws, Gp.off_unit_starts);
+        D.opa = ws + Gp.off_opa;
+        D.opb = ws + Gp.off_opb;
+        D.rowstat = at<RowStat>(ws, Gp.off_rowstat);
+        D.rowterm = at<float>(ws, Gp.off_rowterm);
+        D.colterm = at<float>(ws, Gp.off_colterm);
+        D.band = at<float>(ws, Gp.off_band);
+        D.force = at<uint8_t>(ws, Gp.off_force);
+        D.rowthr = at<uint32_t>(ws, Gp.off_rowthr);
+        D.cand = at<unsigned long long>(ws, Gp.off_cand);
+        D.cand_cnt = at<uint32_t>(ws, Gp.off_cnt);
+        D.topk = at<float>(ws, Gp.off_topk);
+        Gp.host = D;
+        memcpy(host + Gp.off_gdev, &D, sizeof D);
+        HM_TRY(make_operand_map(&Gp.ta, D.opa, Gp.rows, Gp.kpmax, Gp.elem_bytes, Gp.kslice, SC_BM));
+        HM_TRY(make_operand_map(&Gp.tb, D.opb, Gp.rows, Gp.kpmax, Gp.elem_bytes, Gp.kslice, SC_BN));
+    }
+
+    char *dst = ws + B.off_tables;
+    if (B.tables_bytes <= kParamTable) {
+        ParamTable t;
+        t.bytes = (uint32_t)B.tables_bytes;
+        memcpy(t.data, B.table.data(), B.tables_bytes);
+        write_table_kernel<<<1, 256, 0, s>>>(dst, t);
         HM_CUDA_TRY(cudaGetLastError());
-        const uint64_t total = n * (uint64_t)d;
-        int blocks = (int)((total + 255) / 256);
-        if (blocks > 148 * 8) blocks = 148 * 8;
-        check_finite_kernel<<<blocks, 256, 0, s>>>(d_data, total, &flags->nonfinite_min);
-        HM_CUDA_TRY(cudaGetLastError());
-        count_launch(2);
+        count_launch();
+    } else {
+        if (!B.pinned) HM_CUDA_TRY(cudaMallocHost(&B.pinned, B.tables_bytes));
+        memcpy(B.pinned, B.table.data(), B.tables_bytes);
+        HM_CUDA_TRY(cudaMemcpyAsync(dst, B.pinned, B.tables_bytes, cudaMemcpyHostToDevice, s));
     }
-    double *x64 = reinterpret_cast<double *>(ws + L.off_x64);
-    double *rnorm = reinterpret_cast<double *>(ws + L.off_rnorm);
-    // the screened path builds the binary64 copy only if its fallback needs it
-    HM_TRY(launch_prep_plain(d_data, (uint32_t)n, d, L.ldd, L.n_pad, metric,
-                             L.path == HM_PATH_PLAIN ? x64 : nullptr, rnorm, s));
-
-    if (L.path == HM_PATH_PLAIN) {
-        PlainArgs a{};
-        a.x64 = x64;
-        a.rnorm = rnorm;
-        a.n = (uint32_t)n;
-        a.ldd = L.ldd;
-        a.k = k;
-        a.split_cols = L.split_cols;
-        a.row_begin = 0;
-        a.row_end = (uint32_t)n;
-        a.partial = L.splits > 1 ? reinterpret_cast<uint64_t *>(ws + L.off_partial) : nullptr;
-        a.idx_out = d_idx;
-        a.dist_out = d_dist;
-        a.row_list = nullptr;
-        a.row_count = nullptr;
-        HM_TRY(launch_plain_knn(a, metric, L.splits, s));
-        if (L.splits > 1)
-            HM_TRY(launch_merge_splits(a.partial, (uint32_t)n, k, L.splits, d_idx, d_dist, s));
-        return HM_OK;
-    }
-    ScreenRun r{};
-    r.data = d_data;
-    r.x64 = x64;
-    r.rnorm = rnorm;
-    r.n = (uint32_t)n;
-    r.d = d;
-    r.ldd = L.ldd;
-    r.n_pad = L.n_pad;
-    r.k = k;
-    r.metric = metric;
-    r.path = L.path;
-    r.idx_out = d_idx;
-    r.dist_out = d_dist;
-    r.counters = &flags->screen;
-    return screen_run(r, L.screen, ws + L.off_screen, s);
+    return HM_OK;
 }
 
-static int run_smooth(const float *d_dist, uint64_t n, uint32_t k, float *d_sigma, float *d_rho,
-                      uint32_t *zero_count, uint32_t *zero_rows, cudaStream_t s) {
-    const double target = std::log2((double)k);  // src/smooth_knn.rs:25 (platform log2)
-    HM_TRY(launch_smooth_knn(d_dist, (uint32_t)n, k, target, d_sigma, d_rho, zero_count,
-                             zero_rows, s));
-    HM_TRY(launch_mean_all_floor(d_dist, n * (uint64_t)k, zero_count, zero_rows, d_sigma, s));
+// ------------------------------------------------------------------- run
+static int run_batch(hm_batch &B, cudaStream_t s) {
+    if (!B.ws) return set_error(HM_ERR_INVALID, "batch has no workspace bound");
+    char *ws = B.ws;
+    const uint32_t njobs = (uint32_t)B.jobs.size();
+    const JobDev *jobs = at<JobDev>(ws, B.off_jobs);
+    const uint32_t *row_starts = at<uint32_t>(ws, B.off_row_starts);
+    const uint32_t *job_blocks = at<uint32_t>(ws, B.off_job_blocks);
+    const uint32_t blocks = B.job_blocks.back();
+
+    HM_TRY(launch_prep_jobs(jobs, njobs, job_blocks, blocks, PREP_CHECK_AND_NORMS, s));
+    if (B.any_plain) HM_TRY(launch_prep_jobs(jobs, njobs, job_blocks, blocks, PREP_X64_EXACT, s));
+    for (int m = 0; m < 3; ++m) {
+        if (B.items[m].empty()) continue;
+        PlainWork w{};
+        w.jobs = jobs;
+        w.njobs = njobs;
+        w.items = at<uint2>(ws, B.off_items[m]);
+        w.nitems = (uint32_t)B.items[m].size();
+        w.kpl = B.kpl_plain[m];
+        HM_TRY(launch_plain(w, m, s));
+    }
+    for (int g = 0; g < 3; ++g) {
+        GroupPlan &Gp = B.groups[g];
+        if (Gp.jobs.empty()) continue;
+        const GroupDev *Gd = at<GroupDev>(ws, Gp.off_gdev);
+        HM_TRY(launch_screen_prep(jobs, Gp.host, Gd, s));
+        HM_TRY(launch_screen_band(jobs, Gp.host, Gd, s));
+        HM_TRY(launch_screen_gemm(jobs, Gp.host, Gd, Gp.kp, Gp.ta, Gp.tb, debug_dump_pointer(), s));
+        HM_TRY(launch_rerank(jobs, Gp.host, Gd, Gp.kpl, Gp.dmax, Gp.metric_mask, s));
+    }
+    if (B.any_screen) {
+        // exact plain path for the rows the screen could not settle (binary64
+        // copies are built only for jobs that have such rows)
+        HM_TRY(launch_prep_jobs(jobs, njobs, job_blocks, blocks, PREP_X64_FALLBACK, s));
+        for (int m = 0; m < 3; ++m) {
+            if (B.fb_jobs[m].empty()) continue;
+            PlainWork w{};
+            w.jobs = jobs;
+            w.njobs = njobs;
+            w.kpl = B.kpl_fb[m];
+            w.fallback = 1;
+            w.per_job = B.fb_per_job[m];
+            w.fb_jobs = at<uint32_t>(ws, B.off_fb[m]);
+            w.fb_njobs = (uint32_t)B.fb_jobs[m].size();
+            HM_TRY(launch_plain(w, m, s));
+        }
+    }
+    if (B.any_split)
+        HM_TRY(launch_merge(jobs, njobs, njobs > 1 ? row_starts : nullptr, B.all_rows, B.kpl_all, s));
+    if (B.any_smooth) {
+        HM_TRY(launch_smooth(jobs, njobs, njobs > 1 ? row_starts : nullptr, B.all_rows, s));
+        HM_TRY(launch_mean_all_floor(jobs, njobs, s));
+    }
+    return HM_OK;
+}
+
+static void stats_from_counters(const hm_batch &B, uint32_t j, const JobCounters &c, hm_stats *st) {
+    memset(st, 0, sizeof *st);
+    const JobPlan &P = B.jobs[j];
+    st->path_used = P.path;
+    st->col_splits = P.splits;
+    st->zero_rho_rows = c.zero_count;
+    if (P.path != HM_PATH_PLAIN) {
+        st->candidate_cap = P.cap;
+        st->candidates_total = c.candidates;
+        st->candidates_max_row = c.max_row;
+        st->overflow_rows = c.ovf_count;
+        st->candidates_emitted = c.emitted;
+        float band;
+        memcpy(&band, &c.band_max_bits, sizeof band);
+        st->screen_band = band;
+    }
+}
+
+static int check_counters(const JobCounters &c) {
+    if (c.nonfinite_min != 0xffffffffu)
+        return set_error(HM_ERR_INVALID, "data contains a non-finite value at index %u", c.nonfinite_min);
+    if (c.error_code)
+        return set_error(HM_ERR_TIMEOUT, "screen kernel gave up waiting (code %u)", c.error_code);
     return HM_OK;
 }
 
@@ -210,9 +601,6 @@ struct ThreadCtx {
     int device = -1;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    ~ThreadCtx() {
-        // streams/events die with the context at process exit; nothing to do
-    }
 };
 static thread_local ThreadCtx g_ctx;
 
@@ -255,35 +643,37 @@ struct Allocs {
     }
 };
 
-static void fill_stats(hm_stats *st, const Layout &L, const Flags &f, uint64_t n) {
-    if (!st) return;
-    st->path_used = L.path;
-    st->col_splits = L.splits;
-    st->zero_rho_rows = f.zero_count;
-    st->candidate_cap = L.path == HM_PATH_PLAIN ? 0 : L.screen.cap;
-    st->candidates_total = f.screen.candidates;
-    st->candidates_max_row = f.screen.max_row;
-    st->overflow_rows = f.screen.overflow_rows;
-    st->candidates_emitted = f.screen.emitted;
-    float band = 0.f;
-    memcpy(&band, &f.screen.band_max_bits, sizeof band);
-    st->screen_band = L.path == HM_PATH_PLAIN ? 0.0 : (double)band;
-    (void)n;
+static hm_job one_job(const float *data, uint64_t n, uint32_t d, uint32_t k, int metric, int path,
+                      uint32_t *idx, float *dist, float *sigma, float *rho) {
+    hm_job j{};
+    j.data = data;
+    j.n = n;
+    j.d = d;
+    j.k = k;
+    j.metric = metric;
+    j.path = path;
+    j.idx_out = idx;
+    j.dist_out = dist;
+    j.sigma_out = sigma;
+    j.rho_out = rho;
+    return j;
 }
 
 static int host_pipeline(const float *data, uint64_t n, uint32_t d, uint32_t k, int metric,
                          int path, uint32_t *idx_out, float *dist_out, float *sigma_out,
                          float *rho_out, hm_stats *stats) {
-    HM_TRY(validate_knn(data, n, d, k, metric));
+    if (!data) return set_error(HM_ERR_INVALID, "data is NULL");
+    hm_batch B;
+    // planned with the host outputs standing in for the device buffers (only
+    // their presence matters to the plan)
+    hm_job spec = one_job(data, n, d, k, metric, path, idx_out, dist_out, sigma_out, rho_out);
+    HM_TRY(plan_batch(&spec, 1, B));
     if (!idx_out || !dist_out) return set_error(HM_ERR_INVALID, "output pointer is NULL");
-    Layout L;
-    HM_TRY(plan(n, d, k, metric, path, L));
     ThreadCtx *ctx;
     HM_TRY(thread_ctx(ctx));
     cudaStream_t s = ctx->stream;
     const bool smooth = sigma_out && rho_out;
-    int rc = HM_OK;
-    Flags flags{};
+    JobCounters cnt{};
     {
         Allocs A(s);
         void *d_data, *d_idx, *d_dist, *d_sigma = nullptr, *d_rho = nullptr, *ws;
@@ -294,19 +684,14 @@ static int host_pipeline(const float *data, uint64_t n, uint32_t d, uint32_t k, 
             HM_TRY(A.get(&d_sigma, n * sizeof(float)));
             HM_TRY(A.get(&d_rho, n * sizeof(float)));
         }
-        HM_TRY(A.get(&ws, L.total));
+        HM_TRY(A.get(&ws, B.total));
+        B.jobs[0].spec = one_job(static_cast<float *>(d_data), n, d, k, metric, path,
+                                 static_cast<uint32_t *>(d_idx), static_cast<float *>(d_dist),
+                                 static_cast<float *>(d_sigma), static_cast<float *>(d_rho));
         HM_CUDA_TRY(cudaMemcpyAsync(d_data, data, n * d * sizeof(float), cudaMemcpyHostToDevice, s));
         HM_CUDA_TRY(cudaEventRecord(ctx->ev0, s));
-        char *w = static_cast<char *>(ws);
-        rc = run_knn(static_cast<float *>(d_data), n, d, k, metric, L, w,
-                     static_cast<uint32_t *>(d_idx), static_cast<float *>(d_dist), s);
-        if (rc == HM_OK && smooth) {
-            Flags *f = reinterpret_cast<Flags *>(w + L.off_flags);
-            rc = run_smooth(static_cast<float *>(d_dist), n, k, static_cast<float *>(d_sigma),
-                            static_cast<float *>(d_rho), &f->zero_count,
-                            reinterpret_cast<uint32_t *>(w + L.off_zero_rows), s);
-        }
-        if (rc != HM_OK) return rc;
+        HM_TRY(bind_batch(B, ws, B.total, s));
+        HM_TRY(run_batch(B, s));
         HM_CUDA_TRY(cudaEventRecord(ctx->ev1, s));
         HM_CUDA_TRY(cudaMemcpyAsync(idx_out, d_idx, n * k * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
         HM_CUDA_TRY(cudaMemcpyAsync(dist_out, d_dist, n * k * sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -314,22 +699,17 @@ static int host_pipeline(const float *data, uint64_t n, uint32_t d, uint32_t k, 
             HM_CUDA_TRY(cudaMemcpyAsync(sigma_out, d_sigma, n * sizeof(float), cudaMemcpyDeviceToHost, s));
             HM_CUDA_TRY(cudaMemcpyAsync(rho_out, d_rho, n * sizeof(float), cudaMemcpyDeviceToHost, s));
         }
-        HM_CUDA_TRY(cudaMemcpyAsync(&flags, w + L.off_flags, sizeof(Flags), cudaMemcpyDeviceToHost, s));
+        HM_CUDA_TRY(cudaMemcpyAsync(&cnt, static_cast<char *>(ws) + B.off_counters, sizeof cnt,
+                                    cudaMemcpyDeviceToHost, s));
         HM_CUDA_TRY(cudaStreamSynchronize(s));
         if (stats) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, ctx->ev0, ctx->ev1);
+            stats_from_counters(B, 0, cnt, stats);
             stats->device_ms = ms;
         }
     }
-    if (flags.nonfinite_min != 0xffffffffu)
-        return set_error(HM_ERR_INVALID, "data contains a non-finite value at index %u",
-                         flags.nonfinite_min);
-    if (flags.screen.error_code)
-        return set_error(HM_ERR_TIMEOUT, "screen kernel gave up waiting (code %u)",
-                         flags.screen.error_code);
-    fill_stats(stats, L, flags, n);
-    return HM_OK;
+    return check_counters(cnt);
 }
 
 }  // namespace hm
@@ -345,8 +725,7 @@ const char *hm_last_error(void) { return g_last_error.c_str(); }
 int hm_knn(const float *data, uint64_t n, uint32_t d, uint32_t k, int metric, int path,
            uint32_t *idx_out, float *dist_out, hm_stats *stats) {
     clear_error();
-    return host_pipeline(data, n, d, k, metric, path, idx_out, dist_out, nullptr, nullptr,
-                         stats);
+    return host_pipeline(data, n, d, k, metric, path, idx_out, dist_out, nullptr, nullptr, stats);
 }
 
 int hm_knn_smooth(const float *data, uint64_t n, uint32_t d, uint32_t k, int metric, int path,
@@ -354,12 +733,65 @@ int hm_knn_smooth(const float *data, uint64_t n, uint32_t d, uint32_t k, int met
                   hm_stats *stats) {
     clear_error();
     if (!sigma_out || !rho_out) return set_error(HM_ERR_INVALID, "sigma/rho output is NULL");
-    return host_pipeline(data, n, d, k, metric, path, idx_out, dist_out, sigma_out, rho_out,
-                         stats);
+    return host_pipeline(data, n, d, k, metric, path, idx_out, dist_out, sigma_out, rho_out, stats);
 }
 
+size_t hm_workspace_bytes(uint64_t n, uint32_t d, uint32_t k, int metric, int path) {
+    clear_error();
+    hm_batch B;
+    hm_job spec = one_job(nullptr, n, d, k, metric, path, nullptr, nullptr, nullptr, nullptr);
+    if (plan_batch(&spec, 1, B) != HM_OK) return 0;
+    return B.total;
+}
+
+int hm_knn_smooth_device(const float *d_data, uint64_t n, uint32_t d, uint32_t k, int metric,
+                         int path, uint32_t *d_idx, float *d_dist, float *d_sigma, float *d_rho,
+                         void *d_workspace, size_t workspace_bytes, void *stream,
+                         hm_stats *stats) {
+    clear_error();
+    if (!d_data) return set_error(HM_ERR_INVALID, "data is NULL");
+    hm_batch B;
+    hm_job spec = one_job(d_data, n, d, k, metric, path, d_idx, d_dist, d_sigma, d_rho);
+    HM_TRY(plan_batch(&spec, 1, B));
+    if (!d_idx || !d_dist || !d_workspace) return set_error(HM_ERR_INVALID, "NULL pointer argument");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    HM_TRY(bind_batch(B, d_workspace, workspace_bytes, s));
+    HM_TRY(run_batch(B, s));
+    if (stats) {
+        memset(stats, 0, sizeof *stats);
+        stats->path_used = B.jobs[0].path;
+        stats->col_splits = B.jobs[0].splits;
+        stats->candidate_cap = B.jobs[0].path == HM_PATH_PLAIN ? 0 : B.jobs[0].cap;
+    }
+    return HM_OK;
+}
+
+int hm_stats_from_workspace(const void *d_workspace, uint64_t n, uint32_t d, uint32_t k,
+                            int metric, int path, hm_stats *stats) {
+    clear_error();
+    if (!d_workspace || !stats) return set_error(HM_ERR_INVALID, "NULL pointer argument");
+    hm_batch B;
+    hm_job spec = one_job(nullptr, n, d, k, metric, path, nullptr, nullptr, nullptr, nullptr);
+    HM_TRY(plan_batch(&spec, 1, B));
+    JobCounters c{};
+    HM_CUDA_TRY(cudaMemcpy(&c, static_cast<const char *>(d_workspace) + B.off_counters, sizeof c,
+                           cudaMemcpyDeviceToHost));
+    stats_from_counters(B, 0, c, stats);
+    return check_counters(c);
+}
+
+// smooth-kNN alone: a job whose distances are given (no kNN stage)
 size_t hm_smooth_workspace_bytes(uint64_t n) {
-    return align256(sizeof(uint32_t) * 4) + align256(n * sizeof(uint32_t));
+    return align256(sizeof(JobDev)) + align256(sizeof(JobCounters)) + align256(n * sizeof(uint32_t));
+}
+
+__global__ void write_smooth_job_kernel(JobDev *dst, const JobDev j) {
+    if (threadIdx.x == 0) {
+        *dst = j;
+        JobCounters c{};
+        c.nonfinite_min = 0xffffffffu;
+        *j.cnt = c;
+    }
 }
 
 int hm_smooth_knn_device(const float *d_dists, uint64_t n, uint32_t k, float *d_sigma,
@@ -368,11 +800,25 @@ int hm_smooth_knn_device(const float *d_dists, uint64_t n, uint32_t k, float *d_
     if (!d_dists || !d_sigma || !d_rho || !d_workspace)
         return set_error(HM_ERR_INVALID, "NULL pointer argument");
     if (n == 0 || k == 0) return set_error(HM_ERR_INVALID, "empty distance matrix");
-    if (n > 0xffffffffull) return set_error(HM_ERR_UNSUPPORTED, "n exceeds the u32 range");
+    if (n > 0x7fffffffull) return set_error(HM_ERR_UNSUPPORTED, "n exceeds the supported range");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
     char *w = static_cast<char *>(d_workspace);
-    return run_smooth(d_dists, n, k, d_sigma, d_rho, reinterpret_cast<uint32_t *>(w),
-                      reinterpret_cast<uint32_t *>(w + align256(sizeof(uint32_t) * 4)),
-                      static_cast<cudaStream_t>(stream));
+    JobDev J{};
+    J.n = (uint32_t)n;
+    J.k = k;
+    J.dist = const_cast<float *>(d_dists);
+    J.sigma = d_sigma;
+    J.rho = d_rho;
+    J.target = std::log2((double)k);  // src/smooth_knn.rs:25 (platform log2)
+    J.cnt = reinterpret_cast<JobCounters *>(w + align256(sizeof(JobDev)));
+    J.zero_rows = reinterpret_cast<uint32_t *>(w + align256(sizeof(JobDev)) + align256(sizeof(JobCounters)));
+    JobDev *jd = reinterpret_cast<JobDev *>(w);
+    write_smooth_job_kernel<<<1, 32, 0, s>>>(jd, J);
+    HM_CUDA_TRY(cudaGetLastError());
+    count_launch();
+    HM_TRY(launch_smooth(jd, 1, nullptr, (uint32_t)n, s));
+    HM_TRY(launch_mean_all_floor(jd, 1, s));
+    return HM_OK;
 }
 
 int hm_smooth_knn(const float *dists, uint64_t n, uint32_t k, float *sigma_out, float *rho_out) {
@@ -397,62 +843,84 @@ int hm_smooth_knn(const float *dists, uint64_t n, uint32_t k, float *sigma_out, 
     return HM_OK;
 }
 
-size_t hm_workspace_bytes(uint64_t n, uint32_t d, uint32_t k, int metric, int path) {
+// ----------------------------------------------------------------- batches
+int hm_batch_create(const hm_job *jobs, uint32_t njobs, hm_batch **out) {
     clear_error();
-    if (validate_knn((const void *)1, n, d, k, metric) != HM_OK) return 0;
-    Layout L;
-    if (plan(n, d, k, metric, path, L) != HM_OK) return 0;
-    return L.total;
+    if (!jobs || !out) return set_error(HM_ERR_INVALID, "NULL pointer argument");
+    *out = nullptr;
+    for (uint32_t j = 0; j < njobs; ++j) {
+        if (!jobs[j].data || !jobs[j].idx_out || !jobs[j].dist_out)
+            return set_error(HM_ERR_INVALID, "job %u has a NULL data/output pointer", j);
+    }
+    hm_batch *B = new (std::nothrow) hm_batch();
+    if (!B) return set_error(HM_ERR_OOM, "host allocation failed");
+    const int rc = plan_batch(jobs, njobs, *B);
+    if (rc != HM_OK) {
+        delete B;
+        return rc;
+    }
+    *out = B;
+    return HM_OK;
 }
 
-int hm_knn_smooth_device(const float *d_data, uint64_t n, uint32_t d, uint32_t k, int metric,
-                         int path, uint32_t *d_idx, float *d_dist, float *d_sigma, float *d_rho,
-                         void *d_workspace, size_t workspace_bytes, void *stream,
-                         hm_stats *stats) {
+void hm_batch_destroy(hm_batch *batch) { delete batch; }
+
+size_t hm_batch_workspace_bytes(const hm_batch *batch) { return batch ? batch->total : 0; }
+
+int hm_batch_bind(hm_batch *batch, void *d_workspace, size_t workspace_bytes, void *stream) {
     clear_error();
-    HM_TRY(validate_knn(d_data, n, d, k, metric));
-    if (!d_idx || !d_dist || !d_workspace)
-        return set_error(HM_ERR_INVALID, "NULL pointer argument");
-    Layout L;
-    HM_TRY(plan(n, d, k, metric, path, L));
-    if (workspace_bytes < L.total)
-        return set_error(HM_ERR_INVALID, "workspace of %zu bytes is below the %zu needed",
-                         workspace_bytes, L.total);
-    if (reinterpret_cast<uintptr_t>(d_workspace) % 256)
-        return set_error(HM_ERR_INVALID, "workspace must be 256-byte aligned");
+    if (!batch) return set_error(HM_ERR_INVALID, "batch is NULL");
+    return bind_batch(*batch, d_workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+int hm_batch_run(hm_batch *batch, void *stream) {
+    clear_error();
+    if (!batch) return set_error(HM_ERR_INVALID, "batch is NULL");
+    return run_batch(*batch, static_cast<cudaStream_t>(stream));
+}
+
+int hm_batch_graph_launch(hm_batch *batch, void *stream) {
+    clear_error();
+    if (!batch) return set_error(HM_ERR_INVALID, "batch is NULL");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    char *w = static_cast<char *>(d_workspace);
-    HM_TRY(run_knn(d_data, n, d, k, metric, L, w, d_idx, d_dist, s));
-    if (d_sigma && d_rho) {
-        Flags *f = reinterpret_cast<Flags *>(w + L.off_flags);
-        HM_TRY(run_smooth(d_dist, n, k, d_sigma, d_rho, &f->zero_count,
-                          reinterpret_cast<uint32_t *>(w + L.off_zero_rows), s));
+    if (!batch->graph) {
+        // captured on a private stream (the caller's may be the legacy
+        // default stream, which cannot be captured); launched on the caller's
+        if (!batch->capture) HM_CUDA_TRY(cudaStreamCreateWithFlags(&batch->capture, cudaStreamNonBlocking));
+        const bool timing = timing_enabled();
+        hm_timing_enable(0);  // no event records inside the graph
+        cudaGraph_t g = nullptr;
+        HM_CUDA_TRY(cudaStreamBeginCapture(batch->capture, cudaStreamCaptureModeThreadLocal));
+        const int rc = run_batch(*batch, batch->capture);
+        const cudaError_t e = cudaStreamEndCapture(batch->capture, &g);
+        hm_timing_enable(timing ? 1 : 0);
+        if (rc != HM_OK) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        HM_CUDA_TRY(e);
+        const cudaError_t ei = cudaGraphInstantiate(&batch->graph, g, 0);
+        cudaGraphDestroy(g);
+        HM_CUDA_TRY(ei);
     }
-    if (stats) {
-        memset(stats, 0, sizeof *stats);
-        stats->path_used = L.path;
-        stats->col_splits = L.splits;
-        stats->candidate_cap = L.path == HM_PATH_PLAIN ? 0 : L.screen.cap;
-    }
+    HM_CUDA_TRY(cudaGraphLaunch(batch->graph, s));
     return HM_OK;
 }
 
-int hm_stats_from_workspace(const void *d_workspace, uint64_t n, uint32_t d, uint32_t k,
-                            int metric, int path, hm_stats *stats) {
+int hm_batch_job_stats(const hm_batch *batch, uint32_t job, hm_stats *stats) {
     clear_error();
-    if (!d_workspace || !stats) return set_error(HM_ERR_INVALID, "NULL pointer argument");
-    HM_TRY(validate_knn((const void *)1, n, d, k, metric));
-    Layout L;
-    HM_TRY(plan(n, d, k, metric, path, L));
-    Flags f{};
-    HM_CUDA_TRY(cudaMemcpy(&f, static_cast<const char *>(d_workspace) + L.off_flags, sizeof f,
+    if (!batch || !stats || !batch->ws) return set_error(HM_ERR_INVALID, "unbound batch or NULL stats");
+    if (job >= batch->jobs.size()) return set_error(HM_ERR_INVALID, "job %u out of range", job);
+    JobCounters c{};
+    HM_CUDA_TRY(cudaMemcpy(&c, batch->ws + batch->off_counters + job * sizeof(JobCounters), sizeof c,
                            cudaMemcpyDeviceToHost));
-    memset(stats, 0, sizeof *stats);
-    fill_stats(stats, L, f, n);
-    if (f.nonfinite_min != 0xffffffffu)
-        return set_error(HM_ERR_INVALID, "data contains a non-finite value at index %u",
-                         f.nonfinite_min);
-    return HM_OK;
+    stats_from_counters(*batch, job, c, stats);
+    return check_counters(c);
+}
+
+int hm_batch_job_path(const hm_batch *batch, uint32_t job) {
+    if (!batch || job >= batch->jobs.size()) return set_error(HM_ERR_INVALID, "job out of range");
+    return batch->jobs[job].path;
 }
 
 }  // extern "C"

@@ -137,6 +137,67 @@ struct WarpTopK {
     }
 };
 
+// ------------------------------------------------------------- jobs
+// Every kernel works on a table of jobs (independent kNN problems): a single
+// call is a batch of one.  Rows of all jobs form one "all-rows" space (job j
+// owns rows [arow0, arow0 + n)); screened jobs of one operand format also
+// share a "group" row space (job j owns group rows [row0, row0 + n)).
+
+// Device-written counters of one job.
+struct JobCounters {
+    uint32_t nonfinite_min;  // smallest flat index of a non-finite input, or ~0
+    uint32_t zero_count;     // rows whose rho is 0 (global-mean sigma floor)
+    uint32_t ovf_count;      // screened rows sent to the exact fallback
+    uint32_t max_row;        // most candidates reranked in one row
+    unsigned long long candidates;  // candidates reranked exactly
+    unsigned long long emitted;     // candidates the screen wrote
+    uint32_t band_max_bits;  // widest keep band (binary32 bits)
+    uint32_t error_code;     // nonzero if a bounded wait gave up
+    // screen prep maxima (non-negative doubles as bits): |u|, |e|, |r|,
+    // |A row|, |B row|, |u|^2, largest centred |x - mu|^2; then zero rows
+    unsigned long long maxb[8];
+};
+
+struct JobDev {
+    // problem and caller buffers (device pointers)
+    uint32_t n, d, k, metric, path;
+    uint32_t arow0;  // first row in the all-rows space
+    const float *x;
+    uint32_t *idx;
+    float *dist, *sigma, *rho;  // sigma / rho null: no smooth-kNN
+    // exact path (and the screened path's fallback)
+    double *x64;                 // n_pad x ldd binary64 copy
+    double *rnorm;               // sqrt of the sequential sum of squares (cosine)
+    uint32_t ldd, n_pad, splits, split_cols;
+    uint64_t *partial;           // splits x n x k keys (splits > 1)
+    // smooth-kNN
+    double target;               // log2(k), host platform log2
+    uint32_t *zero_rows;         // n
+    // screened path
+    uint32_t group, row0, unit0, kp1, k_stages, row_blocks, col_tiles, parts, part_tiles, cap;
+    unsigned long long slot0;    // first candidate list (2 * parts lists per row)
+    unsigned long long cand0;    // first candidate slot: list l holds [cand0 + (l - slot0) * cap, +cap)
+    unsigned long long topk0;    // first k-array entry: list l's is [topk0 + (l - slot0) * k, +k)
+    float scale;                 // 1 (cosine) or 2 (euclidean)
+    double *mu, *csum;           // euclidean column mean and its partial sums
+    uint32_t csum_blocks, csum_rows;
+    uint32_t *ovf_list;          // n (job-local rows)
+    JobCounters *cnt;
+};
+
+// Host-side decomposition of an all-rows / item / group index into its job:
+// `starts` holds njobs + 1 ascending offsets.
+__device__ __forceinline__ uint32_t find_job(const uint32_t *starts, uint32_t njobs, uint32_t idx) {
+    uint32_t lo = 0, hi = njobs;  // starts[lo] <= idx < starts[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (starts[mid] <= idx) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+int kpl_for_k(uint32_t k);  // 1, 2, 4, 8 or 0 if k > 256
+
 // ------------------------------------------------------------- plain path
 constexpr int PL_BM = 32;     // rows per CTA (8 warps x 4 rows)
 constexpr int PL_BN = 128;    // columns per tile (32 lanes x 4)
@@ -144,49 +205,41 @@ constexpr int PL_BK = 16;     // dimensions per shared-memory stage
 constexpr int PL_THREADS = 256;
 constexpr int PL_ROW_PAD = 128;  // binary64 copy is padded to this many rows
 
-struct PlainArgs {
-    const double *x64;    // n_pad x ldd binary64 copy, zero padded
-    const double *rnorm;  // cosine: sqrt(sequential sum x^2) per row
-    uint32_t n, ldd, k;
-    uint32_t split_cols;  // columns per split, multiple of PL_BN
-    uint32_t row_begin;   // first query row handled by this launch
-    uint32_t row_end;     // one past the last query row
-    uint64_t *partial;    // [splits][rows][k] keys when splits > 1
-    uint32_t *idx_out;    // [rows][k] (rows counted from row_begin)
-    float *dist_out;
-    // Row-list mode (exact fallback of the screened path): when row_list is
-    // set, the query rows are row_list[0 .. *row_count) instead of
-    // [row_begin, row_end), outputs are indexed by the row itself, splits
-    // must be 1 and the grid strides over groups of PL_BM listed rows.
-    const uint32_t *row_list;
-    const uint32_t *row_count;
+// Work table of the exact path: item i = (job, group of PL_BM rows, column
+// split); or, in fallback mode, each job's overflow list strided over
+// `per_job` CTAs.
+struct PlainWork {
+    const JobDev *jobs;
+    uint32_t njobs;
+    const uint2 *items;     // x = job, y = group << 6 | split
+    uint32_t nitems;
+    uint32_t kpl;           // WarpTopK width for the largest k
+    uint32_t fallback;      // 1: rows come from the jobs' overflow lists
+    uint32_t per_job;       // fallback: CTAs per job
+    const uint32_t *fb_jobs;  // fallback: the jobs that may have overflow rows
+    uint32_t fb_njobs;
 };
 
-int kpl_for_k(uint32_t k);  // 1, 2, 4, 8 or 0 if k > 256
+// Input check + binary64 copy + cosine row norms for every job.  x64_gate:
+// build the binary64 copy only for exact-path jobs, or (fallback mode) only
+// for screened jobs whose overflow count is nonzero.
+int launch_prep_jobs(const JobDev *jobs, uint32_t njobs, const uint32_t *job_blocks,
+                     uint32_t total_blocks, int mode, cudaStream_t s);
+enum { PREP_CHECK_AND_NORMS = 0, PREP_X64_EXACT = 1, PREP_X64_FALLBACK = 2 };
 
-// X (n x d f32) -> zero-padded binary64 copy (skipped when x64 is null) and,
-// for cosine, the row norms.
-int launch_prep_plain(const float *x, uint32_t n, uint32_t d, uint32_t ldd, uint32_t n_pad,
-                      int metric, double *x64, double *rnorm, cudaStream_t s);
-// The binary64 copy alone; when `gate` is set it is built only if *gate != 0
-// (the screened path's fallback rows).
-int launch_prep_x64(const float *x, uint32_t n, uint32_t d, uint32_t ldd, uint32_t n_pad,
-                    double *x64, const uint32_t *gate, cudaStream_t s);
-int launch_plain_knn(const PlainArgs &a, int metric, uint32_t splits, cudaStream_t s);
-// Row-list mode with a persistent grid (the list length lives on the device).
-int launch_plain_knn_rows(const PlainArgs &a, int metric, cudaStream_t s);
-int launch_merge_splits(const uint64_t *partial, uint32_t rows, uint32_t k, uint32_t splits,
-                        uint32_t *idx_out, float *dist_out, cudaStream_t s);
+int launch_plain(const PlainWork &w, int metric, cudaStream_t s);
+// merges split lists of every exact-path job with splits > 1
+int launch_merge(const JobDev *jobs, uint32_t njobs, const uint32_t *row_starts, uint32_t rows,
+                 uint32_t kpl, cudaStream_t s);
 
 // ------------------------------------------------------------- smooth kNN
-// Per-row calibration; rows whose rho is 0 get their unfloored sigma and are
-// listed in zero_rows[0..*zero_count) for the global-mean floor.
-int launch_smooth_knn(const float *dists, uint32_t n, uint32_t k, double target,
-                      float *sigma, float *rho, uint32_t *zero_count, uint32_t *zero_rows,
-                      cudaStream_t s);
-// Sequential binary64 mean over all n*k distances, applied as the floor of
-// the listed rows; exits at once when the list is empty.
-int launch_mean_all_floor(const float *dists, uint64_t total, const uint32_t *zero_count,
-                          const uint32_t *zero_rows, float *sigma, cudaStream_t s);
+// Per row of every job with smooth-kNN outputs (row_starts: all-rows space);
+// rows whose rho is 0 get their unfloored sigma and are listed for the
+// job's global-mean floor.
+int launch_smooth(const JobDev *jobs, uint32_t njobs, const uint32_t *row_starts, uint32_t rows,
+                  cudaStream_t s);
+// Sequential binary64 mean of each job's n*k distances, applied as the floor
+// of its listed rows; one block per job, idle when its list is empty.
+int launch_mean_all_floor(const JobDev *jobs, uint32_t njobs, cudaStream_t s);
 
 }  // namespace hm

@@ -13,8 +13,8 @@
 // zero in the padded copy and add an exact +0.0, which leaves a sum that is
 // never -0.0 unchanged.
 //
-// Layout: a CTA owns 32 query rows (8 warps x 4 rows) and walks the columns of
-// its split 128 at a time; every lane computes a 4x4 block of pairs (rows of
+// Layout: a CTA owns 32 query rows of one job (8 warps x 4 rows) and walks the
+// columns of its split 128 at a time; every lane computes a 4x4 block of pairs (rows of
 // its warp x columns lane + 32c).  A warp therefore holds all 128 candidate
 // keys of its 4 rows for the tile and feeds them to a warp-distributed sorted
 // top-k list (WarpTopK).  Column splits (grid.y) write partial lists that
@@ -34,59 +34,67 @@ int kpl_for_k(uint32_t k) {
 }
 
 // ------------------------------------------------------------------ prep
-__global__ void prep_plain_kernel(const float *__restrict__ x, uint32_t n, uint32_t d,
-                                  uint32_t ldd, uint32_t n_pad, double *__restrict__ x64,
-                                  const uint32_t *__restrict__ gate) {
-    if (gate && *gate == 0) return;  // nothing needs the binary64 copy
-    const size_t total = (size_t)n_pad * ldd;
-    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total;
-         t += (size_t)gridDim.x * blockDim.x) {
-        const size_t r = t / ldd, c = t % ldd;
-        x64[t] = (r < n && c < d) ? (double)x[r * d + c] : 0.0;
-    }
+__global__ void init_counters_kernel(JobDev *jobs, uint32_t njobs) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= njobs) return;
+    JobCounters c{};
+    c.nonfinite_min = 0xffffffffu;
+    *jobs[j].cnt = c;
 }
 
-// sqrt of the sequential binary64 sum of squares, as the cosine metric forms
-// na / nb (src/metric.rs:61-66, :69).
-__global__ void row_norm_kernel(const float *__restrict__ x, uint32_t n, uint32_t d,
-                                uint32_t n_pad, double *__restrict__ rnorm) {
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n_pad) return;
-    if (r >= n) {
-        rnorm[r] = 0.0;
+// Blocks are dealt to jobs by `job_blocks` (prefix offsets); each job's blocks
+// stride over that job's elements / rows.
+__global__ void __launch_bounds__(256) prep_jobs_kernel(const JobDev *__restrict__ jobs, uint32_t njobs,
+                                                        const uint32_t *__restrict__ job_blocks,
+                                                        int mode) {
+    const uint32_t jb = find_job(job_blocks, njobs, blockIdx.x);
+    const JobDev &J = jobs[jb];
+    const uint32_t lb = blockIdx.x - job_blocks[jb];
+    const uint32_t nb = job_blocks[jb + 1] - job_blocks[jb];
+    const size_t stride = (size_t)nb * blockDim.x;
+    const size_t t0 = (size_t)lb * blockDim.x + threadIdx.x;
+    if (mode == PREP_CHECK_AND_NORMS) {
+        const size_t total = (size_t)J.n * J.d;
+        for (size_t t = t0; t < total; t += stride)
+            if (!isfinite(J.x[t])) atomicMin(&J.cnt->nonfinite_min, (uint32_t)(t < 0xfffffffeull ? t : 0xfffffffeull));
+        if (J.metric == HM_METRIC_COSINE) {
+            // sqrt of the sequential binary64 sum of squares, as the cosine
+            // metric forms na / nb (src/metric.rs:61-66, :69)
+            for (size_t r = t0; r < J.n_pad; r += stride) {
+                double v = 0.0;
+                if (r < J.n) {
+                    const float *row = J.x + r * J.d;
+                    for (uint32_t c = 0; c < J.d; ++c) {
+                        const double e = (double)row[c];
+                        v = __dadd_rn(v, __dmul_rn(e, e));
+                    }
+                    v = __dsqrt_rn(v);
+                }
+                J.rnorm[r] = v;
+            }
+        }
         return;
     }
-    const float *row = x + (size_t)r * d;
-    double s = 0.0;
-    for (uint32_t c = 0; c < d; ++c) {
-        const double v = (double)row[c];
-        s = __dadd_rn(s, __dmul_rn(v, v));
+    if (mode == PREP_X64_EXACT && J.path != HM_PATH_PLAIN) return;
+    if (mode == PREP_X64_FALLBACK && (J.path == HM_PATH_PLAIN || J.cnt->ovf_count == 0)) return;
+    const size_t total = (size_t)J.n_pad * J.ldd;
+    for (size_t t = t0; t < total; t += stride) {
+        const size_t r = t / J.ldd, c = t % J.ldd;
+        J.x64[t] = (r < J.n && c < J.d) ? (double)J.x[r * J.d + c] : 0.0;
     }
-    rnorm[r] = __dsqrt_rn(s);
 }
 
-int launch_prep_x64(const float *x, uint32_t n, uint32_t d, uint32_t ldd, uint32_t n_pad,
-                    double *x64, const uint32_t *gate, cudaStream_t s) {
+int launch_prep_jobs(const JobDev *jobs, uint32_t njobs, const uint32_t *job_blocks,
+                     uint32_t total_blocks, int mode, cudaStream_t s) {
     ScopedKernelTimer timer(HM_KCLASS_PREP, s);
-    const size_t total = (size_t)n_pad * ldd;
-    const int threads = 256;
-    int blocks = (int)((total + threads - 1) / threads);
-    if (blocks > 148 * 16) blocks = 148 * 16;
-    prep_plain_kernel<<<blocks, threads, 0, s>>>(x, n, d, ldd, n_pad, x64, gate);
-    HM_CUDA_TRY(cudaGetLastError());
-    count_launch();
-    return HM_OK;
-}
-
-int launch_prep_plain(const float *x, uint32_t n, uint32_t d, uint32_t ldd, uint32_t n_pad,
-                      int metric, double *x64, double *rnorm, cudaStream_t s) {
-    if (x64) HM_TRY(launch_prep_x64(x, n, d, ldd, n_pad, x64, nullptr, s));
-    ScopedKernelTimer timer(HM_KCLASS_PREP, s);
-    if (metric == HM_METRIC_COSINE) {
-        row_norm_kernel<<<(n_pad + 127) / 128, 128, 0, s>>>(x, n, d, n_pad, rnorm);
+    if (mode == PREP_CHECK_AND_NORMS) {
+        init_counters_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(const_cast<JobDev *>(jobs), njobs);
         HM_CUDA_TRY(cudaGetLastError());
         count_launch();
     }
+    prep_jobs_kernel<<<total_blocks, 256, 0, s>>>(jobs, njobs, job_blocks, mode);
+    HM_CUDA_TRY(cudaGetLastError());
+    count_launch();
     return HM_OK;
 }
 
@@ -121,32 +129,41 @@ __device__ __forceinline__ float pair_finish(double acc, double rn_a, double rn_
 }
 
 template <int METRIC, int KPL>
-__global__ void __launch_bounds__(PL_THREADS, (KPL <= 2 ? 2 : 1))
-    plain_knn_kernel(const PlainArgs a) {
+__global__ void __launch_bounds__(PL_THREADS, (KPL <= 2 ? 2 : 1)) plain_knn_kernel(const PlainWork w) {
     __shared__ double As[2][PL_BM][PL_BK + 1];
     __shared__ double Bs[2][PL_BN][PL_BK + 1];
     __shared__ uint32_t s_rows[PL_BM];
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const uint32_t split = blockIdx.y;
-    const uint32_t c_begin = split * a.split_cols;
-    const uint32_t c_end = min(a.n, c_begin + a.split_cols);
-    const uint32_t ldd = a.ldd;
-    const bool listed = a.row_list != nullptr;
-    const uint32_t n_groups =
-        listed ? (*a.row_count + PL_BM - 1) / PL_BM : (a.row_end - a.row_begin + PL_BM - 1) / PL_BM;
-    const uint32_t rows_total = a.row_end - a.row_begin;
+    uint32_t jb, first_grp, grp_stride, n_groups, split = 0;
+    if (!w.fallback) {
+        const uint2 it = w.items[blockIdx.x];
+        jb = it.x;
+        first_grp = it.y >> 6;
+        split = it.y & 63u;
+        grp_stride = 1;
+        n_groups = first_grp + 1;
+    } else {
+        jb = w.fb_jobs[blockIdx.x / w.per_job];
+        first_grp = blockIdx.x % w.per_job;
+        grp_stride = w.per_job;
+        n_groups = (w.jobs[jb].cnt->ovf_count + PL_BM - 1) / PL_BM;
+    }
+    const JobDev &J = w.jobs[jb];
+    const uint32_t c_begin = split * J.split_cols;
+    const uint32_t c_end = min(J.n, c_begin + J.split_cols);
+    const uint32_t ldd = J.ldd;
 
-    for (uint32_t grp = blockIdx.x; grp < n_groups; grp += (listed ? gridDim.x : n_groups)) {
+    for (uint32_t grp = first_grp; grp < n_groups; grp += grp_stride) {
         // the 32 query rows of this group (0xffffffff: none)
         if (tid < PL_BM) {
             uint32_t r;
-            if (listed) {
+            if (w.fallback) {
                 const uint32_t at = grp * PL_BM + tid;
-                r = at < *a.row_count ? a.row_list[at] : 0xffffffffu;
+                r = at < J.cnt->ovf_count ? J.ovf_list[at] : 0xffffffffu;
             } else {
-                r = a.row_begin + grp * PL_BM + tid;
-                if (r >= a.row_end) r = 0xffffffffu;
+                r = grp * PL_BM + tid;
+                if (r >= J.n) r = 0xffffffffu;
             }
             s_rows[tid] = r;
         }
@@ -160,8 +177,7 @@ __global__ void __launch_bounds__(PL_THREADS, (KPL <= 2 ? 2 : 1))
 #pragma unroll
         for (int r = 0; r < 4; ++r) {
             my_rows[r] = s_rows[warp * 4 + r];
-            rn_a[r] = (METRIC == HM_METRIC_COSINE && my_rows[r] != 0xffffffffu)
-                          ? a.rnorm[my_rows[r]] : 0.0;
+            rn_a[r] = (METRIC == HM_METRIC_COSINE && my_rows[r] != 0xffffffffu) ? J.rnorm[my_rows[r]] : 0.0;
         }
 
         // loads of one stage: A 32x16 (2 per thread), B 128x16 (8 per thread)
@@ -171,7 +187,7 @@ __global__ void __launch_bounds__(PL_THREADS, (KPL <= 2 ? 2 : 1))
                 const int lin = tid + p * PL_THREADS;
                 const int r = lin >> 4, c = lin & 15;
                 const uint32_t ar = s_rows[r] == 0xffffffffu ? 0u : s_rows[r];
-                const double *src = a.x64 + (size_t)ar * ldd + k0 + c;
+                const double *src = J.x64 + (size_t)ar * ldd + k0 + c;
                 const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&As[buf][r][c]);
                 asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src));
             }
@@ -179,7 +195,7 @@ __global__ void __launch_bounds__(PL_THREADS, (KPL <= 2 ? 2 : 1))
             for (int p = 0; p < 8; ++p) {
                 const int lin = tid + p * PL_THREADS;
                 const int r = lin >> 4, c = lin & 15;
-                const double *src = a.x64 + (size_t)(col0 + r) * ldd + k0 + c;
+                const double *src = J.x64 + (size_t)(col0 + r) * ldd + k0 + c;
                 const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&Bs[buf][r][c]);
                 asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(dst), "l"(src));
             }
@@ -224,7 +240,7 @@ __global__ void __launch_bounds__(PL_THREADS, (KPL <= 2 ? 2 : 1))
             double rn_b[4];
 #pragma unroll
             for (int c = 0; c < 4; ++c)
-                rn_b[c] = (METRIC == HM_METRIC_COSINE) ? a.rnorm[col0 + lane + 32 * c] : 0.0;
+                rn_b[c] = (METRIC == HM_METRIC_COSINE) ? J.rnorm[col0 + lane + 32 * c] : 0.0;
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
 #pragma unroll
@@ -233,7 +249,7 @@ __global__ void __launch_bounds__(PL_THREADS, (KPL <= 2 ? 2 : 1))
                     float dist = pair_finish<METRIC>(acc[r][c], rn_a[r], rn_b[c]);
                     if (col == my_rows[r]) dist = 0.0f;  // src/knn.rs:38-39
                     const uint64_t key = (col < c_end) ? make_key(dist, col) : KEY_NONE;
-                    top[r].offer(key, a.k, lane);
+                    top[r].offer(key, J.k, lane);
                 }
             }
         }
@@ -243,17 +259,16 @@ __global__ void __launch_bounds__(PL_THREADS, (KPL <= 2 ? 2 : 1))
         for (int r = 0; r < 4; ++r) {
             const uint32_t row = my_rows[r];
             if (row == 0xffffffffu) continue;
-            const size_t orow = listed ? row : row - a.row_begin;
 #pragma unroll
             for (int q = 0; q < KPL; ++q) {
                 const uint32_t e = q * 32 + lane;
-                if (e >= a.k) continue;
+                if (e >= J.k) continue;
                 const uint64_t key = top[r].v[q];
-                if (a.partial) {
-                    a.partial[((size_t)split * rows_total + orow) * a.k + e] = key;
+                if (J.splits > 1 && !w.fallback) {
+                    J.partial[((size_t)split * J.n + row) * J.k + e] = key;
                 } else {
-                    a.idx_out[orow * a.k + e] = key_idx(key);
-                    a.dist_out[orow * a.k + e] = key_dist(key);
+                    J.idx[(size_t)row * J.k + e] = key_idx(key);
+                    J.dist[(size_t)row * J.k + e] = key_dist(key);
                 }
             }
         }
@@ -262,69 +277,55 @@ __global__ void __launch_bounds__(PL_THREADS, (KPL <= 2 ? 2 : 1))
 }
 
 template <int METRIC>
-static int launch_plain_metric(const PlainArgs &a, uint32_t splits, cudaStream_t s,
-                               uint32_t grid_x = 0) {
-    const uint32_t rows = a.row_end - a.row_begin;
-    dim3 grid(grid_x ? grid_x : (rows + PL_BM - 1) / PL_BM, splits);
-    ScopedKernelTimer timer(HM_KCLASS_BULK, s);
-    switch (kpl_for_k(a.k)) {
-    case 1: plain_knn_kernel<METRIC, 1><<<grid, PL_THREADS, 0, s>>>(a); break;
-    case 2: plain_knn_kernel<METRIC, 2><<<grid, PL_THREADS, 0, s>>>(a); break;
-    case 4: plain_knn_kernel<METRIC, 4><<<grid, PL_THREADS, 0, s>>>(a); break;
-    case 8: plain_knn_kernel<METRIC, 8><<<grid, PL_THREADS, 0, s>>>(a); break;
-    default: return set_error(HM_ERR_UNSUPPORTED, "k=%u exceeds 256", a.k);
+static int launch_plain_metric(const PlainWork &w, uint32_t grid, cudaStream_t s) {
+    switch (w.kpl) {
+    case 1: plain_knn_kernel<METRIC, 1><<<grid, PL_THREADS, 0, s>>>(w); break;
+    case 2: plain_knn_kernel<METRIC, 2><<<grid, PL_THREADS, 0, s>>>(w); break;
+    case 4: plain_knn_kernel<METRIC, 4><<<grid, PL_THREADS, 0, s>>>(w); break;
+    case 8: plain_knn_kernel<METRIC, 8><<<grid, PL_THREADS, 0, s>>>(w); break;
+    default: return set_error(HM_ERR_UNSUPPORTED, "select width %u", w.kpl);
     }
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();
     return HM_OK;
 }
 
-int launch_plain_knn_rows(const PlainArgs &a, int metric, cudaStream_t s) {
-    PlainArgs b = a;
-    b.partial = nullptr;
-    b.split_cols = (uint32_t)round_up(a.n, PL_BN);
-    b.row_begin = 0;
-    b.row_end = a.n;
-    // persistent grid: groups of listed rows are strided over 2 CTAs per SM
-    const uint32_t groups = (a.n + PL_BM - 1) / PL_BM;
-    const uint32_t ctas = groups < 296 ? groups : 296;
+// One launch per metric present (the arithmetic is a template parameter);
+// `w` describes that metric's items or fallback jobs.
+int launch_plain(const PlainWork &w, int metric, cudaStream_t s) {
+    const uint32_t grid = w.fallback ? w.fb_njobs * w.per_job : w.nitems;
+    if (grid == 0) return HM_OK;
+    ScopedKernelTimer timer(HM_KCLASS_BULK, s);
     switch (metric) {
-    case HM_METRIC_EUCLIDEAN: return launch_plain_metric<HM_METRIC_EUCLIDEAN>(b, 1, s, ctas);
-    case HM_METRIC_COSINE: return launch_plain_metric<HM_METRIC_COSINE>(b, 1, s, ctas);
-    case HM_METRIC_MANHATTAN: return launch_plain_metric<HM_METRIC_MANHATTAN>(b, 1, s, ctas);
-    default: return set_error(HM_ERR_INVALID, "unknown metric %d", metric);
-    }
-}
-
-int launch_plain_knn(const PlainArgs &a, int metric, uint32_t splits, cudaStream_t s) {
-    switch (metric) {
-    case HM_METRIC_EUCLIDEAN: return launch_plain_metric<HM_METRIC_EUCLIDEAN>(a, splits, s);
-    case HM_METRIC_COSINE: return launch_plain_metric<HM_METRIC_COSINE>(a, splits, s);
-    case HM_METRIC_MANHATTAN: return launch_plain_metric<HM_METRIC_MANHATTAN>(a, splits, s);
+    case HM_METRIC_EUCLIDEAN: return launch_plain_metric<HM_METRIC_EUCLIDEAN>(w, grid, s);
+    case HM_METRIC_COSINE: return launch_plain_metric<HM_METRIC_COSINE>(w, grid, s);
+    case HM_METRIC_MANHATTAN: return launch_plain_metric<HM_METRIC_MANHATTAN>(w, grid, s);
     default: return set_error(HM_ERR_INVALID, "unknown metric %d", metric);
     }
 }
 
 // ------------------------------------------------------------ split merge
-// One warp per row folds the `splits` sorted partial lists into one.
+// One warp per row of an exact-path job with splits > 1 folds its split lists.
 template <int KPL>
-__global__ void __launch_bounds__(256) merge_splits_kernel(const uint64_t *__restrict__ partial,
-                                                           uint32_t rows, uint32_t k,
-                                                           uint32_t splits,
-                                                           uint32_t *__restrict__ idx_out,
-                                                           float *__restrict__ dist_out) {
+__global__ void __launch_bounds__(256) merge_splits_kernel(const JobDev *__restrict__ jobs, uint32_t njobs,
+                                                           const uint32_t *__restrict__ row_starts,
+                                                           uint32_t rows) {
     const int lane = threadIdx.x & 31;
-    const uint32_t row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (row >= rows) return;
+    const uint32_t ar = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (ar >= rows) return;
+    const uint32_t jb = row_starts ? find_job(row_starts, njobs, ar) : 0;
+    const JobDev &J = jobs[jb];
+    if (J.path != HM_PATH_PLAIN || J.splits <= 1) return;
+    const uint32_t row = ar - J.arow0, k = J.k;
     WarpTopK<KPL> top;
 #pragma unroll
     for (int q = 0; q < KPL; ++q) {
         const uint32_t e = q * 32 + lane;
-        top.v[q] = (e < k) ? partial[(size_t)row * k + e] : KEY_NONE;
+        top.v[q] = (e < k) ? J.partial[(size_t)row * k + e] : KEY_NONE;
     }
     top.refresh_tau(k, lane);
-    for (uint32_t sp = 1; sp < splits; ++sp) {
-        const uint64_t *list = partial + ((size_t)sp * rows + row) * k;
+    for (uint32_t sp = 1; sp < J.splits; ++sp) {
+        const uint64_t *list = J.partial + ((size_t)sp * J.n + row) * k;
         for (uint32_t e0 = 0; e0 < k; e0 += 32) {
             const uint64_t key = (e0 + lane < k) ? list[e0 + lane] : KEY_NONE;
             if (!__any_sync(0xffffffffu, key < top.tau)) break;  // lists are sorted
@@ -335,22 +336,22 @@ __global__ void __launch_bounds__(256) merge_splits_kernel(const uint64_t *__res
     for (int q = 0; q < KPL; ++q) {
         const uint32_t e = q * 32 + lane;
         if (e < k) {
-            idx_out[(size_t)row * k + e] = key_idx(top.v[q]);
-            dist_out[(size_t)row * k + e] = key_dist(top.v[q]);
+            J.idx[(size_t)row * k + e] = key_idx(top.v[q]);
+            J.dist[(size_t)row * k + e] = key_dist(top.v[q]);
         }
     }
 }
 
-int launch_merge_splits(const uint64_t *partial, uint32_t rows, uint32_t k, uint32_t splits,
-                        uint32_t *idx_out, float *dist_out, cudaStream_t s) {
+int launch_merge(const JobDev *jobs, uint32_t njobs, const uint32_t *row_starts, uint32_t rows,
+                 uint32_t kpl, cudaStream_t s) {
     const int blocks = (int)((rows + 7) / 8);
     ScopedKernelTimer timer(HM_KCLASS_SELECT, s);
-    switch (kpl_for_k(k)) {
-    case 1: merge_splits_kernel<1><<<blocks, 256, 0, s>>>(partial, rows, k, splits, idx_out, dist_out); break;
-    case 2: merge_splits_kernel<2><<<blocks, 256, 0, s>>>(partial, rows, k, splits, idx_out, dist_out); break;
-    case 4: merge_splits_kernel<4><<<blocks, 256, 0, s>>>(partial, rows, k, splits, idx_out, dist_out); break;
-    case 8: merge_splits_kernel<8><<<blocks, 256, 0, s>>>(partial, rows, k, splits, idx_out, dist_out); break;
-    default: return set_error(HM_ERR_UNSUPPORTED, "k=%u exceeds 256", k);
+    switch (kpl) {
+    case 1: merge_splits_kernel<1><<<blocks, 256, 0, s>>>(jobs, njobs, row_starts, rows); break;
+    case 2: merge_splits_kernel<2><<<blocks, 256, 0, s>>>(jobs, njobs, row_starts, rows); break;
+    case 4: merge_splits_kernel<4><<<blocks, 256, 0, s>>>(jobs, njobs, row_starts, rows); break;
+    case 8: merge_splits_kernel<8><<<blocks, 256, 0, s>>>(jobs, njobs, row_starts, rows); break;
+    default: return set_error(HM_ERR_UNSUPPORTED, "select width %u", kpl);
     }
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();

@@ -30,24 +30,32 @@ __device__ __forceinline__ double step(double acc, double x, double y) {
 constexpr int RR_WARPS = 8;
 constexpr int RR_LIST = 256;  // compacted candidates per warp between flushes
 
-// One warp per query row; candidates are evaluated 32 at a time, one per lane.
+// One warp per group row; candidates are evaluated 32 at a time, one per lane.
 template <int METRIC, int KPL>
-__global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs a, uint32_t dstride) {
+__global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const JobDev *__restrict__ jobs,
+                                                               const GroupDev *__restrict__ Gp,
+                                                               uint32_t dstride) {
     extern __shared__ double rr_smem[];
+    const GroupDev &G = *Gp;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t row = blockIdx.x * RR_WARPS + warp;
-    if (row >= a.n) return;
+    const uint32_t gr = blockIdx.x * RR_WARPS + warp;
+    if (gr >= G.rows) return;
+    const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
+    if ((int)J.metric != METRIC) return;
+    const uint32_t row = gr - J.row0;
+    if (row >= J.n) return;  // padding between jobs
+    const uint32_t k = J.k, d = J.d, lists = 2 * J.parts;
+    const size_t l0 = list_index(J, row, 0);
     double *xi = rr_smem + (size_t)warp * dstride;
     uint32_t *list = reinterpret_cast<uint32_t *>(rr_smem + (size_t)RR_WARPS * dstride) + warp * RR_LIST;
 
     // overflow / unbounded rows go to the exact plain path
-    bool ovf = a.force_exact[row] != 0;
-    for (uint32_t p = 0; p < a.parts; ++p) ovf |= a.cand_cnt[(size_t)row * a.parts + p] > a.cap;
+    bool ovf = G.force[gr] != 0;
+    for (uint32_t p = 0; p < lists; ++p) ovf |= G.cand_cnt[l0 + p] > J.cap;
     if (ovf) {
         if (lane == 0) {
-            const uint32_t at = atomicAdd(a.ovf_cnt, 1u);
-            a.ovf_list[at] = row;
-            atomicAdd(&a.counters->overflow_rows, 1u);
+            const uint32_t at = atomicAdd(&J.cnt->ovf_count, 1u);
+            J.ovf_list[at] = row;
         }
         return;
     }
@@ -57,27 +65,27 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs 
     // arrays is exactly that value.
     WarpTopK<KPL> sel;
     sel.reset();
-    for (uint32_t p = 0; p < a.parts; ++p) {
-        const float *kk = a.part_topk + ((size_t)row * a.parts + p) * a.k;
-        for (uint32_t e0 = 0; e0 < a.k; e0 += 32) {
+    for (uint32_t p = 0; p < lists; ++p) {
+        const float *kk = G.topk + J.topk0 + (l0 + p - J.slot0) * k;
+        for (uint32_t e0 = 0; e0 < k; e0 += 32) {
             uint64_t key = KEY_NONE;
-            if (e0 + lane < a.k) {
+            if (e0 + lane < k) {
                 const uint32_t b = __float_as_uint(kk[e0 + lane]);
                 const uint32_t ord = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-                key = ((uint64_t)ord << 32) | (p * a.k + e0 + lane);
+                key = ((uint64_t)ord << 32) | (p * k + e0 + lane);
             }
             if (!__any_sync(0xffffffffu, key < sel.tau)) break;  // arrays are ascending
-            sel.offer(key, a.k, lane);
+            sel.offer(key, k, lane);
         }
     }
     const uint32_t tord = (uint32_t)(sel.tau >> 32);
     const float tau = sel.tau == KEY_NONE ? __int_as_float(0x7f800000)
                                           : __uint_as_float((tord & 0x80000000u) ? (tord & 0x7fffffffu) : ~tord);
-    const float thr = __fadd_ru(tau, a.band[row]);
+    const float thr = __fadd_ru(tau, G.band[gr]);
 
-    for (uint32_t t = lane; t < a.d; t += 32) xi[t] = (double)a.x[(size_t)row * a.d + t];
+    for (uint32_t t = lane; t < d; t += 32) xi[t] = (double)J.x[(size_t)row * d + t];
     __syncwarp();
-    const double rn_i = (METRIC == HM_METRIC_COSINE) ? a.rnorm[row] : 0.0;
+    const double rn_i = (METRIC == HM_METRIC_COSINE) ? J.rnorm[row] : 0.0;
 
     WarpTopK<KPL> top;
     top.reset();
@@ -91,14 +99,14 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs 
         for (uint32_t b = 0; b < m; b += 32) {
             const bool mine = b + lane < m;
             const uint32_t j = mine ? list[b + lane] : row;
-            const float *xj = a.x + (size_t)j * a.d;
+            const float *xj = J.x + (size_t)j * d;
             double acc = 0.0;
             uint32_t t = 0;
-            if ((a.d & 3u) == 0) {
+            if ((d & 3u) == 0) {
                 const float4 *xj4 = reinterpret_cast<const float4 *>(xj);
                 const double2 *xi2 = reinterpret_cast<const double2 *>(xi);
 #pragma unroll 4
-                for (uint32_t q = 0; q < a.d / 4; ++q) {
+                for (uint32_t q = 0; q < d / 4; ++q) {
                     const float4 y = __ldg(xj4 + q);
                     const double2 p0 = xi2[2 * q], p1 = xi2[2 * q + 1];
                     acc = step<METRIC>(acc, p0.x, (double)y.x);
@@ -106,9 +114,9 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs 
                     acc = step<METRIC>(acc, p1.x, (double)y.z);
                     acc = step<METRIC>(acc, p1.y, (double)y.w);
                 }
-                t = a.d;
+                t = d;
             }
-            for (; t < a.d; ++t) acc = step<METRIC>(acc, xi[t], (double)__ldg(xj + t));
+            for (; t < d; ++t) acc = step<METRIC>(acc, xi[t], (double)__ldg(xj + t));
             uint64_t key = KEY_NONE;
             if (mine) {
                 float dist;
@@ -117,21 +125,20 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs 
                 } else if (METRIC == HM_METRIC_EUCLIDEAN) {
                     dist = __double2float_rn(__dsqrt_rn(acc));
                 } else {
-                    const double q = __ddiv_rn(acc, __dmul_rn(rn_i, a.rnorm[j]));
+                    const double q = __ddiv_rn(acc, __dmul_rn(rn_i, J.rnorm[j]));
                     const double r = __dsub_rn(1.0, q);
                     dist = (r > 0.0) ? __double2float_rn(r) : 0.0f;
                 }
                 key = make_key(dist, j);
             }
-            top.offer(key, a.k, lane);
+            top.offer(key, k, lane);
         }
         __syncwarp();
     };
 
-    for (uint32_t p = 0; p < a.parts; ++p) {
-        const size_t slot = (size_t)row * a.parts + p;
-        const uint32_t cnt = a.cand_cnt[slot];
-        const unsigned long long *cand = a.cand + slot * a.cap;
+    for (uint32_t p = 0; p < lists; ++p) {
+        const uint32_t cnt = G.cand_cnt[l0 + p];
+        const unsigned long long *cand = G.cand + J.cand0 + (l0 + p - J.slot0) * J.cap;
         for (uint32_t e0 = 0; e0 < cnt; e0 += 32) {
             bool pass = false;
             uint32_t j = 0;
@@ -157,27 +164,28 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const RerankArgs 
 #pragma unroll
     for (int q = 0; q < KPL; ++q) {
         const uint32_t e = q * 32 + lane;
-        if (e < a.k) {
-            a.idx_out[(size_t)row * a.k + e] = key_idx(top.v[q]);
-            a.dist_out[(size_t)row * a.k + e] = key_dist(top.v[q]);
+        if (e < k) {
+            J.idx[(size_t)row * k + e] = key_idx(top.v[q]);
+            J.dist[(size_t)row * k + e] = key_dist(top.v[q]);
         }
     }
     if (lane == 0) {
-        atomicAdd(&a.counters->candidates, (unsigned long long)kept);
-        atomicMax(&a.counters->max_row, kept);
+        atomicAdd(&J.cnt->candidates, (unsigned long long)kept);
+        atomicMax(&J.cnt->max_row, kept);
     }
 }
 
 template <int METRIC>
-static int launch_metric(const RerankArgs &a, uint32_t kpl, cudaStream_t s) {
-    const uint32_t dstride = (uint32_t)round_up(a.d, 4);
+static int launch_metric(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t kpl,
+                         uint32_t dmax, cudaStream_t s) {
+    const uint32_t dstride = (uint32_t)round_up(dmax, 4);
     const size_t smem = (size_t)RR_WARPS * dstride * sizeof(double) + RR_WARPS * RR_LIST * sizeof(uint32_t);
-    const int blocks = (int)((a.n + RR_WARPS - 1) / RR_WARPS);
+    const int blocks = (int)((G.rows + RR_WARPS - 1) / RR_WARPS);
 #define HM_RR_CASE(K)                                                                       \
     case K: {                                                                               \
         HM_CUDA_TRY(cudaFuncSetAttribute(rerank_kernel<METRIC, K>,                          \
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
-        rerank_kernel<METRIC, K><<<blocks, RR_WARPS * 32, smem, s>>>(a, dstride);           \
+        rerank_kernel<METRIC, K><<<blocks, RR_WARPS * 32, smem, s>>>(jobs, Gd, dstride);    \
         break;                                                                              \
     }
     switch (kpl) {
@@ -191,11 +199,16 @@ static int launch_metric(const RerankArgs &a, uint32_t kpl, cudaStream_t s) {
     return HM_OK;
 }
 
-int launch_rerank(const RerankArgs &a, int metric, uint32_t kpl, cudaStream_t s) {
+// one launch per metric present in the group
+int launch_rerank(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t kpl,
+                  uint32_t dmax, int metric_mask, cudaStream_t s) {
+    if (G.rows == 0) return HM_OK;
     ScopedKernelTimer timer(HM_KCLASS_SELECT, s);
-    if (metric == HM_METRIC_EUCLIDEAN) return launch_metric<HM_METRIC_EUCLIDEAN>(a, kpl, s);
-    if (metric == HM_METRIC_COSINE) return launch_metric<HM_METRIC_COSINE>(a, kpl, s);
-    return set_error(HM_ERR_UNSUPPORTED, "metric %d has no screened path", metric);
+    if (metric_mask & (1 << HM_METRIC_EUCLIDEAN))
+        HM_TRY(launch_metric<HM_METRIC_EUCLIDEAN>(jobs, G, Gd, kpl, dmax, s));
+    if (metric_mask & (1 << HM_METRIC_COSINE))
+        HM_TRY(launch_metric<HM_METRIC_COSINE>(jobs, G, Gd, kpl, dmax, s));
+    return HM_OK;
 }
 
 }  // namespace hm

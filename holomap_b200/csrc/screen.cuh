@@ -27,18 +27,9 @@
 #include <stddef.h>
 #include <stdint.h>
 
-namespace hm {
+#include "hm_internal.cuh"
 
-// Counters the screened path leaves in the workspace (device-written).
-struct ScreenCounters {
-    unsigned long long candidates;  // candidates reranked exactly, all rows
-    uint32_t max_row;               // most candidates reranked in one row
-    uint32_t overflow_rows;         // rows sent to the exact fallback
-    uint32_t band_max_bits;         // widest keep band 2E_i (binary32 bits)
-    uint32_t error_code;            // nonzero if a bounded wait gave up
-    uint32_t pad;
-    unsigned long long emitted;     // candidates the screen wrote, all rows
-};
+namespace hm {
 
 // Screen GEMM tile: 128 query rows (UMMA M) x 256 columns (UMMA N), 128-byte
 // K slices (64 bf16 or 32 tf32 elements) per pipeline stage.
@@ -51,41 +42,6 @@ constexpr int SC_THREADS = 64 + 32 * SC_EPI_WARPS;  // warp 0 TMA, warp 1 MMA, w
 
 enum ScreenKind { SCREEN_KIND_BF16 = 0, SCREEN_KIND_TF32 = 1 };
 
-struct ScreenLayout {
-    int kind = SCREEN_KIND_BF16;
-    bool split = false;       // operand is [hi|hi|lo] x [hi|lo|hi]
-    uint32_t elem_bytes = 2;  // operand element size
-    uint32_t kslice = 64;     // elements per 128-byte slice
-    uint32_t kp1 = 0;         // one copy of d, padded to kslice
-    uint32_t kp = 0;          // operand row length (kp1 or 3*kp1)
-    uint32_t k_stages = 0;    // kp / kslice
-    uint32_t row_blocks = 0, col_tiles = 0, parts = 1, part_tiles = 0, units = 0;
-    uint32_t cap = 0;         // candidate slots per (row, part)
-    uint32_t kpl = 1;         // rerank select width (WarpTopK slots per lane)
-    uint32_t csum_blocks = 0; // euclidean column-mean partial blocks
-    size_t off_a = 0, off_b = 0, off_csum = 0, off_mu = 0, off_max = 0, off_rowstat = 0;
-    size_t off_rowterm = 0, off_colterm = 0, off_band = 0, off_force = 0;
-    size_t off_cand = 0, off_cnt = 0, off_tau = 0, off_ovf = 0, off_ovf_cnt = 0, off_rowthr = 0;
-    size_t total = 0;
-};
-
-struct ScreenRun {
-    const float *data;
-    const double *x64;
-    const double *rnorm;
-    uint32_t n, d, ldd, n_pad, k;
-    int metric, path;
-    uint32_t *idx_out;
-    float *dist_out;
-    ScreenCounters *counters;
-    float *debug_dump;  // optional n x n screened values (tests only)
-};
-
-int screen_plan(uint64_t n, uint32_t d, uint32_t k, int metric, int path, ScreenLayout &L);
-int screen_run(const ScreenRun &r, const ScreenLayout &L, char *ws, cudaStream_t s);
-
-// ---- pieces (screen_prep.cu, screen_gemm.cu, rerank.cu) -------------------
-
 // Per-row statistics of the operand rounding, binary64.
 struct RowStat {
     double unorm;   // ||u_i||
@@ -95,53 +51,38 @@ struct RowStat {
     double bnorm;   // ||B row||
     double sqnorm;  // ||u_i||^2
 };
-constexpr int ROWSTAT_FIELDS = 6;
 
-struct ScreenPrepArgs {
-    const float *x;
-    const double *rnorm_ref;  // cosine: sqrt of the sequential sum of squares
-    uint32_t n, d, metric;
-    ScreenLayout L;
-    char *ws;
+// One screen group: the screened jobs that share an operand format.  Their
+// rows are concatenated into the group's row space (job g owns rows
+// [row_starts[g], row_starts[g+1])), one operand matrix of rows x kpmax
+// elements serves all of them through one TMA map, and the persistent
+// screen kernel drains the group's (job, row block, column part) units.
+struct GroupDev {
+    uint32_t rows, njobs, units;
+    uint32_t kind, split, elem_bytes, kslice, kpmax;
+    const uint32_t *job_ids;      // [njobs] index of each group job in the job table
+    const uint32_t *row_starts;   // [njobs + 1]
+    const uint32_t *unit_starts;  // [njobs + 1]
+    void *opa, *opb;              // rows x kpmax operands (opb == opa unless split)
+    RowStat *rowstat;
+    float *rowterm, *colterm, *band;  // colterm padded by SC_BN zeros
+    uint8_t *force;               // rows the screen cannot bound (cosine zero vectors)
+    uint32_t *rowthr;             // per row: smallest list threshold so far (ordered key)
+    unsigned long long *cand;     // candidate lists, (c^ bits << 32) | job-local column
+    uint32_t *cand_cnt;
+    float *topk;                  // each list's k smallest c^, ascending
 };
-int launch_screen_prep(const ScreenPrepArgs &a, cudaStream_t s);
-int launch_screen_band(uint32_t n, uint32_t d, int metric, const ScreenLayout &L, char *ws,
-                       uint32_t *band_max_bits, cudaStream_t s);
 
-struct ScreenGemmArgs {
-    uint32_t n, k, k_stages, col_tiles, parts, part_tiles, units, cap;
-    float scale;              // 1 (cosine) or 2 (euclidean)
-    const float *rowterm;     // euclidean ||u_i||^2 (binary32); null for cosine
-    const float *colterm;     // per column additive term
-    const float *band;        // per row keep band 2E_i
-    unsigned long long *cand; // [slot*cap] = (c^ bits << 32) | j, slot = (row*parts + part)*2 + half
-    uint32_t *cand_cnt;       // [slot]
-    float *part_topk;         // [slot * k]: each list's k smallest c^, ascending
-    uint32_t *error_code;
-    unsigned long long *emitted;
-    const unsigned long long *zero_rows;  // cosine: rows with ||x|| = 0
-    uint32_t *rowthr;         // per row: smallest list threshold so far (order-preserving key)
-    float *dump;
-    uint32_t idesc;
-};
-int launch_screen_gemm(const ScreenGemmArgs &g, int kind, uint32_t kpl_regs,
-                       const CUtensorMap &ta, const CUtensorMap &tb, cudaStream_t s);
+// Locations of row i's list s (s < 2 * parts) of job J.
+__device__ __forceinline__ size_t list_index(const JobDev &J, uint32_t i, uint32_t s) {
+    return (size_t)J.slot0 + (size_t)i * 2 * J.parts + s;
+}
 
-struct RerankArgs {
-    const float *x;
-    const double *rnorm;
-    uint32_t n, d, k, parts, cap;
-    const unsigned long long *cand;
-    const uint32_t *cand_cnt;
-    const float *part_topk;
-    const float *band;
-    const uint8_t *force_exact;
-    uint32_t *ovf_list;
-    uint32_t *ovf_cnt;
-    uint32_t *idx_out;
-    float *dist_out;
-    ScreenCounters *counters;
-};
-int launch_rerank(const RerankArgs &a, int metric, uint32_t kpl, cudaStream_t s);
+int launch_screen_prep(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, cudaStream_t s);
+int launch_screen_band(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, cudaStream_t s);
+int launch_screen_gemm(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t kp,
+                       const CUtensorMap &ta, const CUtensorMap &tb, float *dump, cudaStream_t s);
+int launch_rerank(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t kpl,
+                  uint32_t dmax, int metric_mask, cudaStream_t s);
 
 }  // namespace hm

@@ -195,22 +195,26 @@ __device__ __forceinline__ void raise_error(volatile uint32_t *abort_flag, uint3
 }
 
 struct UnitTiles {
-    uint32_t rb, part, ct_begin, ct_end;
+    uint32_t job, rb, part, ct_begin, ct_end;
 };
 
-__device__ __forceinline__ UnitTiles unit_tiles(const ScreenGemmArgs &g, uint32_t u) {
+__device__ __forceinline__ UnitTiles unit_tiles(const JobDev *jobs, const GroupDev &G, uint32_t u) {
+    const uint32_t g = find_job(G.unit_starts, G.njobs, u);
     UnitTiles t;
-    t.rb = u / g.parts;
-    t.part = u % g.parts;
-    t.ct_begin = t.part * g.part_tiles;
-    t.ct_end = min(g.col_tiles, t.ct_begin + g.part_tiles);
+    t.job = G.job_ids[g];
+    const JobDev &J = jobs[t.job];
+    const uint32_t lu = u - G.unit_starts[g];
+    t.rb = lu / J.parts;
+    t.part = lu % J.parts;
+    t.ct_begin = t.part * J.part_tiles;
+    t.ct_end = min(J.col_tiles, t.ct_begin + J.part_tiles);
     return t;
 }
 
 template <int KIND, int KP>
 __global__ void __launch_bounds__(SC_THREADS, 1)
     screen_gemm_kernel(const __grid_constant__ CUtensorMap tma, const __grid_constant__ CUtensorMap tmb,
-                       const ScreenGemmArgs g) {
+                       const JobDev *__restrict__ jobs, const GroupDev G, float *dump, uint32_t idesc) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                 ~(uintptr_t)1023);
@@ -254,21 +258,22 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         if (lane == 0) {
             uint32_t it = 0;
             bool ok = true;
-            for (uint32_t u = blockIdx.x; ok && u < g.units; u += gridDim.x) {
-                const UnitTiles ut = unit_tiles(g, u);
+            for (uint32_t u = blockIdx.x; ok && u < G.units; u += gridDim.x) {
+                const UnitTiles ut = unit_tiles(jobs, G, u);
+                const JobDev &J = jobs[ut.job];
                 for (uint32_t ct = ut.ct_begin; ok && ct < ut.ct_end; ++ct) {
-                    for (uint32_t ks = 0; ks < g.k_stages; ++ks, ++it) {
+                    for (uint32_t ks = 0; ks < J.k_stages; ++ks, ++it) {
                         const uint32_t s = it % SC_STAGES, r = it / SC_STAGES;
                         if (!mbar_wait(smem_u32(&empty[s]), (r & 1) ^ 1, abort_flag)) {
-                            raise_error(abort_flag, g.error_code, SC_ERR_PRODUCER);
+                            raise_error(abort_flag, &J.cnt->error_code, SC_ERR_PRODUCER);
                             ok = false;
                             break;
                         }
                         const uint32_t fb = smem_u32(&full[s]);
                         mbar_arrive_expect_tx(fb, SC_A_BYTES + SC_B_BYTES);
                         const int32_t kx = (int32_t)(ks * (SC_SLICE_BYTES / (KIND == SCREEN_KIND_BF16 ? 2 : 4)));
-                        tma_load_2d(smem_u32(sA + s * SC_A_BYTES), &tma, fb, kx, (int32_t)(ut.rb * SC_BM));
-                        tma_load_2d(smem_u32(sB + s * SC_B_BYTES), &tmb, fb, kx, (int32_t)(ct * SC_BN));
+                        tma_load_2d(smem_u32(sA + s * SC_A_BYTES), &tma, fb, kx, (int32_t)(J.row0 + ut.rb * SC_BM));
+                        tma_load_2d(smem_u32(sB + s * SC_B_BYTES), &tmb, fb, kx, (int32_t)(J.row0 + ct * SC_BN));
                     }
                 }
             }
@@ -277,7 +282,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
             for (uint32_t t = issued > SC_STAGES ? issued - SC_STAGES : 0; t < issued; ++t) {
                 const uint32_t s = t % SC_STAGES, r = t / SC_STAGES;
                 if (!mbar_wait(smem_u32(&full[s]), r & 1, abort_flag, true)) {
-                    raise_error(abort_flag, g.error_code, SC_ERR_DRAIN);
+                    raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN);
                     break;
                 }
             }
@@ -288,22 +293,22 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         if (lane == 0) {
             uint32_t it = 0, tile = 0;
             bool ok = true;
-            constexpr uint32_t kM = SC_BM, kN = SC_BN;
-            for (uint32_t u = blockIdx.x; ok && u < g.units; u += gridDim.x) {
-                const UnitTiles ut = unit_tiles(g, u);
+            for (uint32_t u = blockIdx.x; ok && u < G.units; u += gridDim.x) {
+                const UnitTiles ut = unit_tiles(jobs, G, u);
+                const JobDev &J = jobs[ut.job];
                 for (uint32_t ct = ut.ct_begin; ok && ct < ut.ct_end; ++ct, ++tile) {
                     const uint32_t buf = tile & 1, use = tile >> 1;
                     if (!mbar_wait(smem_u32(&acce[buf]), (use & 1) ^ 1, abort_flag)) {
-                        raise_error(abort_flag, g.error_code, SC_ERR_MMA_ACC);
+                        raise_error(abort_flag, &J.cnt->error_code, SC_ERR_MMA_ACC);
                         ok = false;
                         break;
                     }
                     fence_after_sync();
-                    const uint32_t d_tmem = tmem_base + buf * kN;
-                    for (uint32_t ks = 0; ks < g.k_stages; ++ks, ++it) {
+                    const uint32_t d_tmem = tmem_base + buf * SC_BN;
+                    for (uint32_t ks = 0; ks < J.k_stages; ++ks, ++it) {
                         const uint32_t s = it % SC_STAGES, r = it / SC_STAGES;
                         if (!mbar_wait(smem_u32(&full[s]), r & 1, abort_flag)) {
-                            raise_error(abort_flag, g.error_code, SC_ERR_MMA_FULL);
+                            raise_error(abort_flag, &J.cnt->error_code, SC_ERR_MMA_FULL);
                             ok = false;
                             break;
                         }
@@ -313,19 +318,18 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
 #pragma unroll
                         for (uint32_t kk = 0; kk < SC_SLICE_BYTES / 32; ++kk)
                             mma_issue<KIND>(d_tmem, smem_desc(a0 + kk * 32), smem_desc(b0 + kk * 32),
-                                            g.idesc, (ks | kk) != 0);
+                                            idesc, (ks | kk) != 0);
                         mma_commit(smem_u32(&empty[s]));
                     }
                     if (!ok) break;
                     mma_commit(smem_u32(&accf[buf]));
-                    (void)kM;
                 }
             }
             // drain: the last commit must have landed before TMEM is freed
             if (it > 0) {
                 const uint32_t s = (it - 1) % SC_STAGES, r = (it - 1) / SC_STAGES;
                 if (!mbar_wait(smem_u32(&empty[s]), r & 1, abort_flag, true))
-                    raise_error(abort_flag, g.error_code, SC_ERR_DRAIN);
+                    raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN);
             }
         }
         __syncwarp();
@@ -337,37 +341,43 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         const uint32_t half = (uint32_t)(warp - 2) >> 2;
         const uint32_t row_in_tile = quad * 32 + lane;
         const float INF = __int_as_float(0x7f800000);
-        // cosine fast test needs every column term to be 1 (no zero rows)
-        const bool fast_cos = g.rowterm == nullptr && *g.zero_rows == 0;
         uint32_t tile = 0;
         bool ok = true;
-        for (uint32_t u = blockIdx.x; ok && u < g.units; u += gridDim.x) {
-            const UnitTiles ut = unit_tiles(g, u);
-            const uint32_t row = ut.rb * SC_BM + row_in_tile;
-            const bool valid = row < g.n;
-            // sorted k smallest chunk minima; arr[KP-1] is the running tau
+        for (uint32_t u = blockIdx.x; ok && u < G.units; u += gridDim.x) {
+            const UnitTiles ut = unit_tiles(jobs, G, u);
+            const JobDev &J = jobs[ut.job];
+            const uint32_t n = J.n;
+            const uint32_t row = ut.rb * SC_BM + row_in_tile;  // job-local
+            const bool valid = row < n;
+            const size_t gr = (size_t)J.row0 + row;              // group row
+            // cosine rows compare 1 - v directly (every column term is 1 when
+            // the job has no zero vectors)
+            const bool fast_cos = J.metric == HM_METRIC_COSINE && J.cnt->maxb[7] == 0;
+            // sorted k smallest screened values; arr[KP-1] is the running tau
             float arr[KP];
 #pragma unroll
-            for (int q = 0; q < KP; ++q) arr[q] = (q < KP - (int)g.k) ? -INF : INF;
-            const float band = valid ? g.band[row] : 0.0f;
-            const float rowterm = (valid && g.rowterm) ? g.rowterm[row] : 0.0f;
+            for (int q = 0; q < KP; ++q) arr[q] = (q < KP - (int)J.k) ? -INF : INF;
+            const float band = valid ? G.band[gr] : 0.0f;
+            const float rowterm = valid ? G.rowterm[gr] : 0.0f;
+            const float scale = J.scale;
             float thr = valid ? INF : -INF;  // invalid rows never emit
             float tglob = INF;      // the row's shared threshold, last seen
             float published = INF;  // this list's tau, last shared
             uint32_t cnt = 0;
-            const size_t slot = ((size_t)row * g.parts + ut.part) * 2 + half;
-            unsigned long long *cand = g.cand + slot * g.cap;
+            const size_t list = list_index(J, valid ? row : 0, ut.part * 2 + half);
+            unsigned long long *cand = G.cand + J.cand0 + (list - J.slot0) * J.cap;
+            const float *colterm = G.colterm + J.row0;
 
             for (uint32_t ct = ut.ct_begin; ct < ut.ct_end; ++ct, ++tile) {
                 const uint32_t buf = tile & 1, use = tile >> 1;
                 if (!mbar_wait(smem_u32(&accf[buf]), use & 1, abort_flag)) {
-                    raise_error(abort_flag, g.error_code, SC_ERR_EPILOGUE);
+                    raise_error(abort_flag, &J.cnt->error_code, SC_ERR_EPILOGUE);
                     ok = false;
                     break;
                 }
                 fence_after_sync();
                 if (valid) {  // the row's other lists may have tightened its threshold
-                    const float tg = unord32(*(volatile const uint32_t *)(g.rowthr + row));
+                    const float tg = unord32(*(volatile const uint32_t *)(G.rowthr + gr));
                     if (tg < tglob) {
                         tglob = tg;
                         thr = __fadd_ru(fminf(arr[KP - 1], tglob), band);
@@ -382,22 +392,22 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                 auto process = [&](uint32_t (&v)[32], uint32_t ch) {
                     // c overwrites the accumulator registers in place
                     float (&c)[32] = reinterpret_cast<float (&)[32]>(v);
-                    const uint32_t j0 = c_base + ch * 32;
-                    // columns past n: never emitted, never the chunk minimum
-                    const uint32_t vmask = (j0 + 32 <= g.n) ? 0xffffffffu
-                                           : (j0 >= g.n ? 0u : (0xffffffffu >> (32 - (g.n - j0))));
+                    const uint32_t j0 = c_base + ch * 32;  // job-local column
+                    // columns past n: never emitted
+                    const uint32_t vmask = (j0 + 32 <= n) ? 0xffffffffu
+                                           : (j0 >= n ? 0u : (0xffffffffu >> (32 - (n - j0))));
                     if (fast_cos) {
 #pragma unroll
                         for (int t = 0; t < 32; ++t) c[t] = __fsub_rn(1.0f, c[t]);
                     } else {
-                        const float4 *ctp = reinterpret_cast<const float4 *>(g.colterm + j0);
+                        const float4 *ctp = reinterpret_cast<const float4 *>(colterm + j0);
 #pragma unroll
                         for (int q = 0; q < 8; ++q) {
                             const float4 cq = __ldg(ctp + q);
                             const float cs[4] = {cq.x, cq.y, cq.z, cq.w};
 #pragma unroll
                             for (int e = 0; e < 4; ++e)
-                                c[4 * q + e] = __fsub_rn(__fadd_rn(rowterm, cs[e]), __fmul_rn(g.scale, c[4 * q + e]));
+                                c[4 * q + e] = __fsub_rn(__fadd_rn(rowterm, cs[e]), __fmul_rn(scale, c[4 * q + e]));
                         }
                     }
                     if (diag) {
@@ -405,14 +415,9 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                         for (int t = 0; t < 32; ++t)
                             if (j0 + t == row) c[t] = 0.0f;
                     }
-                    if (vmask != 0xffffffffu) {
-#pragma unroll
+                    if (dump && valid) {
                         for (int t = 0; t < 32; ++t)
-                            if (!((vmask >> t) & 1u)) c[t] = INF;
-                    }
-                    if (g.dump && valid) {
-                        for (int t = 0; t < 32; ++t)
-                            if (j0 + t < g.n) g.dump[(size_t)row * g.n + j0 + t] = c[t];
+                            if (j0 + t < n) dump[(size_t)row * n + j0 + t] = c[t];
                     }
                     // columns within the threshold: one predicate word per
                     // column (set.leu keeps a NaN), OR-reduced as a tree
@@ -427,7 +432,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                     for (int w = 16; w > 0; w >>= 1)
 #pragma unroll
                         for (int t = 0; t < w; ++t) pw[t] |= pw[t + w];
-                    uint32_t pm = pw[0] & vmask;
+                    uint32_t pm = valid ? (pw[0] & vmask) : 0u;
                     if (pm) {
                         // emit each passing column and insert it into the
                         // running k smallest when it improves them
@@ -439,7 +444,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                             const int t = __ffs(pm) - 1;
                             pm &= pm - 1;
                             const float x = cl[t];
-                            if (cnt < g.cap) cand[cnt] = ((unsigned long long)__float_as_uint(x) << 32) | (j0 + t);
+                            if (cnt < J.cap) cand[cnt] = ((unsigned long long)__float_as_uint(x) << 32) | (j0 + t);
                             ++cnt;
                             if (x < arr[KP - 1]) {
 #pragma unroll
@@ -452,7 +457,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                             const float tl = arr[KP - 1];
                             if (tl < published) {  // share with the row's other lists
                                 const uint32_t o = ord32(tl);
-                                const uint32_t prev = atomicMin(g.rowthr + row, o);
+                                const uint32_t prev = atomicMin(G.rowthr + gr, o);
                                 tglob = fminf(tglob, unord32(prev < o ? prev : o));
                                 published = tl;
                             }
@@ -477,14 +482,14 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                 if (lane == 0) mbar_arrive(smem_u32(&acce[buf]));
             }
             if (valid) {
-                // the list's k smallest screened values (sorted; the global k
-                // smallest of the row are all among the union of these)
-                g.cand_cnt[slot] = cnt;
-                float *kk = g.part_topk + slot * g.k;
+                // the list's k smallest screened values (ascending; the row's
+                // global k smallest are all among the union of these)
+                G.cand_cnt[list] = cnt;
+                float *kk = G.topk + J.topk0 + (list - J.slot0) * J.k;
 #pragma unroll
                 for (int q = 0; q < KP; ++q)
-                    if (q >= KP - (int)g.k) kk[q - (KP - (int)g.k)] = arr[q];
-                atomicAdd(g.emitted, (unsigned long long)cnt);
+                    if (q >= KP - (int)J.k) kk[q - (KP - (int)J.k)] = arr[q];
+                atomicAdd(&J.cnt->emitted, (unsigned long long)cnt);
             }
         }
     }
@@ -499,30 +504,40 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
 }
 
 template <int KIND, int KP>
-static int launch_kind(const ScreenGemmArgs &g, const CUtensorMap &ta, const CUtensorMap &tb,
-                       cudaStream_t s) {
+static int launch_kind(const JobDev *jobs, const GroupDev &G, const CUtensorMap &ta,
+                       const CUtensorMap &tb, float *dump, uint32_t idesc, cudaStream_t s) {
     HM_CUDA_TRY(cudaFuncSetAttribute(screen_gemm_kernel<KIND, KP>,
                                      cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)SC_SMEM_BYTES));
     int dev = 0, sms = 148;
     HM_CUDA_TRY(cudaGetDevice(&dev));
     HM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const uint32_t grid = g.units < (uint32_t)sms ? g.units : (uint32_t)sms;
-    screen_gemm_kernel<KIND, KP><<<grid, SC_THREADS, SC_SMEM_BYTES, s>>>(ta, tb, g);
+    const uint32_t grid = G.units < (uint32_t)sms ? G.units : (uint32_t)sms;
+    screen_gemm_kernel<KIND, KP><<<grid, SC_THREADS, SC_SMEM_BYTES, s>>>(ta, tb, jobs, G, dump, idesc);
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();
     return HM_OK;
 }
 
-int launch_screen_gemm(const ScreenGemmArgs &g, int kind, uint32_t kp, const CUtensorMap &ta,
-                       const CUtensorMap &tb, cudaStream_t s) {
+static uint32_t make_idesc(int kind) {
+    const uint32_t fmt = kind == SCREEN_KIND_BF16 ? 1u : 2u;  // BF16 / TF32 operands
+    return (1u << 4)                    // accumulator: F32
+           | (fmt << 7) | (fmt << 10)   // A, B formats
+           | (0u << 15) | (0u << 16)    // A, B K-major
+           | ((uint32_t)(SC_BN >> 3) << 17) | ((uint32_t)(SC_BM >> 4) << 24);
+}
+
+int launch_screen_gemm(const JobDev *jobs, const GroupDev &G, const GroupDev *, uint32_t kp,
+                       const CUtensorMap &ta, const CUtensorMap &tb, float *dump, cudaStream_t s) {
+    if (G.units == 0) return HM_OK;
     ScopedKernelTimer timer(HM_KCLASS_BULK, s);
-    if (kind == SCREEN_KIND_BF16) {
-        if (kp == 32) return launch_kind<SCREEN_KIND_BF16, 32>(g, ta, tb, s);
-        if (kp == 64) return launch_kind<SCREEN_KIND_BF16, 64>(g, ta, tb, s);
+    const uint32_t idesc = make_idesc((int)G.kind);
+    if (G.kind == SCREEN_KIND_BF16) {
+        if (kp == 32) return launch_kind<SCREEN_KIND_BF16, 32>(jobs, G, ta, tb, dump, idesc, s);
+        if (kp == 64) return launch_kind<SCREEN_KIND_BF16, 64>(jobs, G, ta, tb, dump, idesc, s);
     } else {
-        if (kp == 32) return launch_kind<SCREEN_KIND_TF32, 32>(g, ta, tb, s);
-        if (kp == 64) return launch_kind<SCREEN_KIND_TF32, 64>(g, ta, tb, s);
+        if (kp == 32) return launch_kind<SCREEN_KIND_TF32, 32>(jobs, G, ta, tb, dump, idesc, s);
+        if (kp == 64) return launch_kind<SCREEN_KIND_TF32, 64>(jobs, G, ta, tb, dump, idesc, s);
     }
     return set_error(HM_ERR_UNSUPPORTED, "screen top-k width %u", kp);
 }

@@ -32,44 +32,50 @@ __device__ __forceinline__ void atomic_max_pos(unsigned long long *p, double v) 
     atomicMax(p, (unsigned long long)__double_as_longlong(v));
 }
 
-// Column sums of the rows in [blockIdx.x * rows_per, ...), binary64.
-__global__ void colsum_partial_kernel(const float *__restrict__ x, uint32_t n, uint32_t d,
-                                      uint32_t rows_per, double *__restrict__ partial) {
-    const uint32_t r0 = blockIdx.x * rows_per;
-    const uint32_t r1 = min(n, r0 + rows_per);
-    for (uint32_t c = threadIdx.x; c < d; c += blockDim.x) {
+constexpr uint32_t CSUM_BLOCKS = 64;  // column-sum partial blocks per euclidean job
+
+// Column sums of one slice of a job's rows, binary64 (block = job x slice).
+__global__ void colsum_partial_kernel(const JobDev *__restrict__ jobs, const GroupDev *__restrict__ G) {
+    const uint32_t g = blockIdx.x / CSUM_BLOCKS, b = blockIdx.x % CSUM_BLOCKS;
+    const JobDev &J = jobs[G->job_ids[g]];
+    if (J.metric != HM_METRIC_EUCLIDEAN) return;
+    const uint32_t per = (J.n + CSUM_BLOCKS - 1) / CSUM_BLOCKS;
+    const uint32_t r0 = b * per, r1 = min(J.n, r0 + per);
+    for (uint32_t c = threadIdx.x; c < J.d; c += blockDim.x) {
         double s = 0.0;
-        for (uint32_t r = r0; r < r1; ++r) s += (double)x[(size_t)r * d + c];
-        partial[(size_t)blockIdx.x * d + c] = s;
+        for (uint32_t r = r0; r < r1; ++r) s += (double)J.x[(size_t)r * J.d + c];
+        J.csum[(size_t)b * J.d + c] = s;
     }
 }
 
-__global__ void colmean_kernel(const double *__restrict__ partial, uint32_t blocks, uint32_t n,
-                               uint32_t d, double *__restrict__ mu) {
-    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < d; c += gridDim.x * blockDim.x) {
+__global__ void colmean_kernel(const JobDev *__restrict__ jobs, const GroupDev *__restrict__ G) {
+    const JobDev &J = jobs[G->job_ids[blockIdx.x]];
+    if (J.metric != HM_METRIC_EUCLIDEAN) return;
+    for (uint32_t c = threadIdx.x; c < J.d; c += blockDim.x) {
         double s = 0.0;
-        for (uint32_t b = 0; b < blocks; ++b) s += partial[(size_t)b * d + c];
-        mu[c] = s / (double)n;
+        for (uint32_t b = 0; b < CSUM_BLOCKS; ++b) s += J.csum[(size_t)b * J.d + c];
+        J.mu[c] = s / (double)J.n;
     }
 }
 
-// Largest ||x_i - mu||^2 (euclidean), for the power-of-two scale.
-__global__ void centred_norm_max_kernel(const float *__restrict__ x, uint32_t n, uint32_t d,
-                                        const double *__restrict__ mu,
-                                        unsigned long long *__restrict__ maxbits) {
+// Largest ||x_i - mu||^2 of each euclidean job, for its power-of-two scale.
+__global__ void centred_norm_max_kernel(const JobDev *__restrict__ jobs, const GroupDev *__restrict__ G) {
     const int lane = threadIdx.x & 31;
-    const uint32_t row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (row >= n) return;
+    const uint32_t gr = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (gr >= G->rows) return;
+    const uint32_t g = find_job(G->row_starts, G->njobs, gr);
+    const JobDev &J = jobs[G->job_ids[g]];
+    if (J.metric != HM_METRIC_EUCLIDEAN) return;
+    const uint32_t row = gr - J.row0;
+    if (row >= J.n) return;  // padding between jobs
     double s = 0.0;
-    for (uint32_t t = lane; t < d; t += 32) {
-        const double v = (double)x[(size_t)row * d + t] - mu[t];
+    for (uint32_t t = lane; t < J.d; t += 32) {
+        const double v = (double)J.x[(size_t)row * J.d + t] - J.mu[t];
         s += v * v;
     }
     s = warp_sum(s);
-    if (lane == 0) atomic_max_pos(maxbits, s);
+    if (lane == 0) atomic_max_pos(&J.cnt->maxb[6], s);
 }
-
-__device__ __forceinline__ double flush_tiny(double v) { return fabs(v) < kFltMin ? 0.0 : v; }
 
 __device__ __forceinline__ uint16_t to_bf16_bits(double v, double *rounded) {
     const __nv_bfloat16 h = __float2bfloat16_rn((float)v);
@@ -94,56 +100,54 @@ __device__ __forceinline__ uint32_t to_tf32_bits(double v, double *rounded) {
     return b;
 }
 
-// One warp per row: operand row(s), binary64 error statistics, additive
-// terms of the screen epilogue.
-__global__ void __launch_bounds__(256) operand_kernel(const float *__restrict__ x,
-                                                     const double *__restrict__ rnorm_ref,
-                                                     uint32_t n, uint32_t d, uint32_t metric,
-                                                     ScreenLayout L, char *__restrict__ ws) {
+// One warp per group row: operand row(s), binary64 error statistics,
+// additive terms of the screen epilogue, and the row's shared threshold.
+__global__ void __launch_bounds__(256) operand_kernel(const JobDev *__restrict__ jobs,
+                                                     const GroupDev *__restrict__ Gp) {
+    const GroupDev &G = *Gp;
     const int lane = threadIdx.x & 31;
-    const uint32_t row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (row >= n) return;
-    const double *mu = reinterpret_cast<const double *>(ws + L.off_mu);
-    unsigned long long *maxb = reinterpret_cast<unsigned long long *>(ws + L.off_max);
-    RowStat *stats = reinterpret_cast<RowStat *>(ws + L.off_rowstat);
-    float *rowterm = reinterpret_cast<float *>(ws + L.off_rowterm);
-    float *colterm = reinterpret_cast<float *>(ws + L.off_colterm);
-    uint8_t *force = reinterpret_cast<uint8_t *>(ws + L.off_force);
+    const uint32_t gr = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (gr >= G.rows) return;
+    const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
+    const uint32_t row = gr - J.row0;
+    if (row >= J.n) return;  // padding between jobs (never read as a valid row)
+    unsigned long long *maxb = J.cnt->maxb;
 
     double scale = 1.0;
     bool zero_row = false;
-    if (metric == HM_METRIC_EUCLIDEAN) {
-        const double m = sqrt(__longlong_as_double((long long)maxb[ROWSTAT_FIELDS]));
+    if (J.metric == HM_METRIC_EUCLIDEAN) {
+        const double m = sqrt(__longlong_as_double((long long)maxb[6]));
         if (m > 0.0) {
             int e;
             frexp(m, &e);  // m = f * 2^e, f in [0.5, 1)
             scale = ldexp(1.0, -e);
         }
     } else {
-        const double rn = rnorm_ref[row];
+        const double rn = J.rnorm[row];
         zero_row = !(rn > 0.0);
         scale = zero_row ? 0.0 : 1.0 / rn;
     }
 
+    const size_t kp = G.kpmax;
     double uu = 0.0, ee = 0.0, rr = 0.0, aa = 0.0;
-    const float *xr = x + (size_t)row * d;
-    for (uint32_t t = lane; t < L.kp1; t += 32) {
+    const float *xr = J.x + (size_t)row * J.d;
+    for (uint32_t t = lane; t < J.kp1; t += 32) {
         double u = 0.0;
-        if (t < d) {
-            u = (metric == HM_METRIC_EUCLIDEAN) ? ((double)xr[t] - mu[t]) * scale
-                                                : (zero_row ? 0.0 : (double)xr[t] / rnorm_ref[row]);
+        if (t < J.d) {
+            u = (J.metric == HM_METRIC_EUCLIDEAN) ? ((double)xr[t] - J.mu[t]) * scale
+                                                  : (zero_row ? 0.0 : (double)xr[t] / J.rnorm[row]);
         }
         uu += u * u;
-        if (L.kind == SCREEN_KIND_TF32) {
+        if (G.kind == SCREEN_KIND_TF32) {
             double r;
             const uint32_t b = to_tf32_bits(u, &r);
-            reinterpret_cast<uint32_t *>(ws + L.off_a)[(size_t)row * L.kp + t] = b;
+            reinterpret_cast<uint32_t *>(G.opa)[(size_t)gr * kp + t] = b;
             ee += (r - u) * (r - u);
             aa += r * r;
-        } else if (!L.split) {
+        } else if (!G.split) {
             double r;
             const uint16_t b = to_bf16_bits(u, &r);
-            reinterpret_cast<uint16_t *>(ws + L.off_a)[(size_t)row * L.kp + t] = b;
+            reinterpret_cast<uint16_t *>(G.opa)[(size_t)gr * kp + t] = b;
             ee += (r - u) * (r - u);
             aa += r * r;
         } else {
@@ -151,14 +155,14 @@ __global__ void __launch_bounds__(256) operand_kernel(const float *__restrict__ 
             const uint16_t bh = to_bf16_bits(u, &hi);
             const uint16_t bl = to_bf16_bits(u - hi, &lo);
             const double res = (u - hi) - lo;
-            uint16_t *A = reinterpret_cast<uint16_t *>(ws + L.off_a) + (size_t)row * L.kp;
-            uint16_t *B = reinterpret_cast<uint16_t *>(ws + L.off_b) + (size_t)row * L.kp;
+            uint16_t *A = reinterpret_cast<uint16_t *>(G.opa) + (size_t)gr * kp;
+            uint16_t *B = reinterpret_cast<uint16_t *>(G.opb) + (size_t)gr * kp;
             A[t] = bh;
-            A[L.kp1 + t] = bh;
-            A[2 * L.kp1 + t] = bl;
+            A[J.kp1 + t] = bh;
+            A[2 * J.kp1 + t] = bl;
             B[t] = bh;
-            B[L.kp1 + t] = bl;
-            B[2 * L.kp1 + t] = bh;
+            B[J.kp1 + t] = bl;
+            B[2 * J.kp1 + t] = bh;
             ee += lo * lo;
             rr += res * res;
             aa += 2.0 * hi * hi + lo * lo;
@@ -176,88 +180,77 @@ __global__ void __launch_bounds__(256) operand_kernel(const float *__restrict__ 
         st.anorm = sqrt(aa);
         st.bnorm = st.anorm;  // both operand layouts have the same row norm
         st.sqnorm = uu;
-        stats[row] = st;
+        G.rowstat[gr] = st;
         atomic_max_pos(&maxb[0], st.unorm);
         atomic_max_pos(&maxb[1], st.enorm);
         atomic_max_pos(&maxb[2], st.rnorm);
         atomic_max_pos(&maxb[3], st.anorm);
         atomic_max_pos(&maxb[4], st.bnorm);
         atomic_max_pos(&maxb[5], st.sqnorm);
-        if (metric == HM_METRIC_EUCLIDEAN) {
+        if (J.metric == HM_METRIC_EUCLIDEAN) {
             const float nsq = __double2float_rn(uu);
-            rowterm[row] = nsq;
-            colterm[row] = nsq;
+            G.rowterm[gr] = nsq;
+            G.colterm[gr] = nsq;
         } else {
-            colterm[row] = zero_row ? 0.0f : 1.0f;
+            G.rowterm[gr] = 0.0f;
+            G.colterm[gr] = zero_row ? 0.0f : 1.0f;
         }
-        force[row] = zero_row ? 1 : 0;
-        // shared screen threshold of the row starts at +inf (order-preserving key)
-        reinterpret_cast<uint32_t *>(ws + L.off_rowthr)[row] = 0xff800000u;
+        G.force[gr] = zero_row ? 1 : 0;
         if (zero_row) atomicAdd(&maxb[7], 1ull);
+        G.rowthr[gr] = 0xff800000u;  // the row's shared threshold starts at +inf
     }
 }
 
 // Keep band 2E_i per row (see screen.cuh for the terms).
-__global__ void band_kernel(uint32_t n, uint32_t d, uint32_t metric, ScreenLayout L,
-                            char *__restrict__ ws, uint32_t *__restrict__ band_max_bits) {
-    const uint32_t row = blockIdx.x * blockDim.x + threadIdx.x;
-    if (row >= n) return;
-    const unsigned long long *maxb = reinterpret_cast<const unsigned long long *>(ws + L.off_max);
-    const RowStat st = reinterpret_cast<const RowStat *>(ws + L.off_rowstat)[row];
+__global__ void band_kernel(const JobDev *__restrict__ jobs, const GroupDev *__restrict__ Gp) {
+    const GroupDev &G = *Gp;
+    const uint32_t gr = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gr >= G.rows) return;
+    const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
+    if (gr - J.row0 >= J.n) return;  // padding between jobs
+    const unsigned long long *maxb = J.cnt->maxb;
+    const RowStat st = G.rowstat[gr];
     const double Umax = __longlong_as_double((long long)maxb[0]);
     const double Emax = __longlong_as_double((long long)maxb[1]);
     const double Rmax = __longlong_as_double((long long)maxb[2]);
     const double Bmax = __longlong_as_double((long long)maxb[4]);
     const double SQmax = __longlong_as_double((long long)maxb[5]);
-    const double K = (double)L.kp;
+    const double K = (double)(G.split ? 3 * J.kp1 : J.kp1);
     const double gam = K * 0x1p-22;  // fp32 accumulation, any summation order
     const double tiny = K * 0x1p-125;
     double eps;
-    if (!L.split) {
+    if (!G.split) {
         eps = st.enorm * Umax + st.unorm * Emax + st.enorm * Emax;
     } else {
         eps = st.enorm * Emax + st.rnorm * Umax + (st.unorm + st.rnorm) * Rmax;
     }
     eps += gam * st.anorm * Bmax + tiny;
     double E;
-    if (metric == HM_METRIC_EUCLIDEAN)
-        E = 2.0 * eps + (st.sqnorm + SQmax) * (0x1p-21 + (double)(d + 8) * 0x1p-50);
+    if (J.metric == HM_METRIC_EUCLIDEAN)
+        E = 2.0 * eps + (st.sqnorm + SQmax) * (0x1p-21 + (double)(J.d + 8) * 0x1p-50);
     else
-        E = eps + 0x1p-21 + (double)(d + 8) * 0x1p-51;
+        E = eps + 0x1p-21 + (double)(J.d + 8) * 0x1p-51;
     const double B = 2.0 * E * (1.0 + 0x1p-10);
     const float bf = __double2float_ru(B);
-    reinterpret_cast<float *>(ws + L.off_band)[row] = bf;
-    atomicMax(band_max_bits, __float_as_uint(bf));
+    G.band[gr] = bf;
+    atomicMax(&J.cnt->band_max_bits, __float_as_uint(bf));
 }
 
-int launch_screen_prep(const ScreenPrepArgs &a, cudaStream_t s) {
+int launch_screen_prep(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, cudaStream_t s) {
     ScopedKernelTimer timer(HM_KCLASS_PREP, s);
-    const ScreenLayout &L = a.L;
-    HM_CUDA_TRY(cudaMemsetAsync(a.ws + L.off_max, 0, 8 * sizeof(unsigned long long), s));
-    HM_CUDA_TRY(cudaMemsetAsync(a.ws + L.off_colterm, 0, round_up(a.n, SC_BN) * sizeof(float), s));
-    if (a.metric == HM_METRIC_EUCLIDEAN) {
-        const uint32_t rows_per = (a.n + L.csum_blocks - 1) / L.csum_blocks;
-        colsum_partial_kernel<<<L.csum_blocks, 128, 0, s>>>(
-            a.x, a.n, a.d, rows_per, reinterpret_cast<double *>(a.ws + L.off_csum));
-        colmean_kernel<<<(a.d + 127) / 128, 128, 0, s>>>(
-            reinterpret_cast<double *>(a.ws + L.off_csum), L.csum_blocks, a.n, a.d,
-            reinterpret_cast<double *>(a.ws + L.off_mu));
-        centred_norm_max_kernel<<<(a.n + 7) / 8, 256, 0, s>>>(
-            a.x, a.n, a.d, reinterpret_cast<double *>(a.ws + L.off_mu),
-            reinterpret_cast<unsigned long long *>(a.ws + L.off_max) + ROWSTAT_FIELDS);
-        HM_CUDA_TRY(cudaGetLastError());
-        count_launch(3);
-    }
-    operand_kernel<<<(a.n + 7) / 8, 256, 0, s>>>(a.x, a.rnorm_ref, a.n, a.d, a.metric, L, a.ws);
+    HM_CUDA_TRY(cudaMemsetAsync(G.colterm, 0, round_up(G.rows, SC_BN) * sizeof(float) + SC_BN * sizeof(float), s));
+    colsum_partial_kernel<<<G.njobs * CSUM_BLOCKS, 128, 0, s>>>(jobs, Gd);
+    colmean_kernel<<<G.njobs, 128, 0, s>>>(jobs, Gd);
+    centred_norm_max_kernel<<<(G.rows + 7) / 8, 256, 0, s>>>(jobs, Gd);
+    operand_kernel<<<(G.rows + 7) / 8, 256, 0, s>>>(jobs, Gd);
     HM_CUDA_TRY(cudaGetLastError());
-    count_launch();
+    count_launch(4);
     return HM_OK;
 }
 
-int launch_screen_band(uint32_t n, uint32_t d, int metric, const ScreenLayout &L, char *ws,
-                       uint32_t *band_max_bits, cudaStream_t s) {
+int launch_screen_band(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, cudaStream_t s) {
     ScopedKernelTimer timer(HM_KCLASS_PREP, s);
-    band_kernel<<<(n + 255) / 256, 256, 0, s>>>(n, d, (uint32_t)metric, L, ws, band_max_bits);
+    band_kernel<<<(G.rows + 255) / 256, 256, 0, s>>>(jobs, Gd);
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();
     return HM_OK;

@@ -4,7 +4,7 @@
 // MIN_K_DIST_SCALE floors), mean at :82-84, and libm::expf reached through
 // src/fmath.rs:119-122.
 //
-// One warp per row.  Lanes evaluate the row's exp terms in parallel; the
+// One warp per row (of any job).  Lanes evaluate the row's exp terms in parallel; the
 // binary32 partial sum is then formed in the reference's order (j = 1, 2, ...,
 // k-1, each add rounded) by broadcasting the terms, so every lane holds the
 // same psum and all control flow is warp-uniform.  All arithmetic uses
@@ -92,18 +92,19 @@ __device__ __forceinline__ float expf_libm(float x) {
     return k == 0 ? y : scalbnf_dev(y, k);
 }
 
-// Row values are read per 32-element chunk from global memory (L1 resident
-// after the first pass).
-__global__ void __launch_bounds__(256) smooth_knn_kernel(const float *__restrict__ dists,
-                                                         uint32_t n, uint32_t k, double target,
-                                                         float *__restrict__ sigma,
-                                                         float *__restrict__ rho,
-                                                         uint32_t *__restrict__ zero_count,
-                                                         uint32_t *__restrict__ zero_rows) {
+// One warp per row of the all-rows space; the row's values are read per
+// 32-element chunk from global memory (L1 resident after the first pass).
+__global__ void __launch_bounds__(256) smooth_knn_kernel(const JobDev *__restrict__ jobs, uint32_t njobs,
+                                                         const uint32_t *__restrict__ row_starts,
+                                                         uint32_t rows) {
     const int lane = threadIdx.x & 31;
-    const uint32_t row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (row >= n) return;
-    const float *v = dists + (size_t)row * k;
+    const uint32_t ar = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (ar >= rows) return;
+    const JobDev &J = jobs[row_starts ? find_job(row_starts, njobs, ar) : 0];
+    if (!J.sigma || !J.rho) return;
+    const uint32_t row = ar - J.arow0, k = J.k;
+    const double target = J.target;
+    const float *v = J.dist + (size_t)row * k;
     const uint32_t chunks = (k + 31) / 32;
 
     // rho: first positive distance in row order, else 0 (src/smooth_knn.rs:35)
@@ -164,23 +165,21 @@ __global__ void __launch_bounds__(256) smooth_knn_kernel(const float *__restrict
         const float floor_v = __fmul_rn(1e-3f, mean_row);
         if (sg < floor_v) sg = floor_v;
     } else if (lane == 0) {
-        // floored later with the global mean (launch_mean_all_floor)
-        const uint32_t slot = atomicAdd(zero_count, 1u);
-        zero_rows[slot] = row;
+        // floored later with the job's global mean (mean_all_floor_kernel)
+        const uint32_t slot = atomicAdd(&J.cnt->zero_count, 1u);
+        J.zero_rows[slot] = row;
     }
     if (lane == 0) {
-        sigma[row] = sg;
-        rho[row] = rh;
+        J.sigma[row] = sg;
+        J.rho[row] = rh;
     }
 }
 
-int launch_smooth_knn(const float *dists, uint32_t n, uint32_t k, double target, float *sigma,
-                      float *rho, uint32_t *zero_count, uint32_t *zero_rows, cudaStream_t s) {
-    HM_CUDA_TRY(cudaMemsetAsync(zero_count, 0, sizeof(uint32_t), s));
-    const int blocks = (int)((n + 7) / 8);
+int launch_smooth(const JobDev *jobs, uint32_t njobs, const uint32_t *row_starts, uint32_t rows,
+                  cudaStream_t s) {
+    const int blocks = (int)((rows + 7) / 8);
     ScopedKernelTimer timer(HM_KCLASS_SMOOTH, s);
-    smooth_knn_kernel<<<blocks, 256, 0, s>>>(dists, n, k, target, sigma, rho, zero_count,
-                                             zero_rows);
+    smooth_knn_kernel<<<blocks, 256, 0, s>>>(jobs, njobs, row_starts, rows);
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();
     return HM_OK;
@@ -188,17 +187,18 @@ int launch_smooth_knn(const float *dists, uint32_t n, uint32_t k, double target,
 
 // mean_all = f32(sequential binary64 sum of all n*k distances / (n*k))
 // (src/smooth_knn.rs:26, :82-84).  The reference's order is one dependent
-// chain, so one thread forms it; the other 255 threads stage the next values
-// through shared memory.  Runs only when some row had rho == 0.
-__global__ void __launch_bounds__(256) mean_all_floor_kernel(const float *__restrict__ dists,
-                                                             uint64_t total,
-                                                             const uint32_t *__restrict__ zero_count,
-                                                             const uint32_t *__restrict__ zero_rows,
-                                                             float *__restrict__ sigma) {
-    const uint32_t cnt = *zero_count;
+// chain, so one thread forms it; the other 255 threads of the job's block
+// stage the next values through shared memory.  Idle when no row of the job
+// had rho == 0.
+__global__ void __launch_bounds__(256) mean_all_floor_kernel(const JobDev *__restrict__ jobs) {
+    const JobDev &J = jobs[blockIdx.x];
+    if (!J.sigma || !J.rho) return;
+    const uint32_t cnt = J.cnt->zero_count;
     if (cnt == 0) return;
     __shared__ float stage[2][2048];
     __shared__ float floor_v;
+    const float *dists = J.dist;
+    const uint64_t total = (uint64_t)J.n * J.k;
     double s = 0.0;
     const uint64_t chunk = 2048;
     for (uint64_t base = 0; base < total; base += chunk) {
@@ -209,7 +209,7 @@ __global__ void __launch_bounds__(256) mean_all_floor_kernel(const float *__rest
         if (threadIdx.x == 0)
             for (uint64_t t = 0; t < len; ++t) s = __dadd_rn(s, (double)stage[buf][t]);
         // the double buffer lets the next fill overlap the chain; the barrier
-        // at the top of the iteration after next protects reuse
+        // of the iteration after next protects reuse
     }
     if (threadIdx.x == 0) {
         const float mean_all = __double2float_rn(__ddiv_rn(s, (double)total));
@@ -217,14 +217,14 @@ __global__ void __launch_bounds__(256) mean_all_floor_kernel(const float *__rest
     }
     __syncthreads();
     for (uint32_t t = threadIdx.x; t < cnt; t += blockDim.x) {
-        const uint32_t row = zero_rows[t];
-        if (sigma[row] < floor_v) sigma[row] = floor_v;
+        const uint32_t row = J.zero_rows[t];
+        if (J.sigma[row] < floor_v) J.sigma[row] = floor_v;
     }
 }
 
-int launch_mean_all_floor(const float *dists, uint64_t total, const uint32_t *zero_count,
-                          const uint32_t *zero_rows, float *sigma, cudaStream_t s) {
-    mean_all_floor_kernel<<<1, 256, 0, s>>>(dists, total, zero_count, zero_rows, sigma);
+int launch_mean_all_floor(const JobDev *jobs, uint32_t njobs, cudaStream_t s) {
+    ScopedKernelTimer timer(HM_KCLASS_SMOOTH, s);
+    mean_all_floor_kernel<<<njobs, 256, 0, s>>>(jobs);
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();
     return HM_OK;

@@ -52,3 +52,68 @@ class DeviceKnnProblem:
 
     def indices_u32(self) -> torch.Tensor:
         return self.idx
+
+
+class DeviceBatch:
+    """Many independent kNN + smooth-kNN problems run as one batch on the
+    device (one pass of the pipeline; screened jobs of one operand format
+    share one persistent screen launch).  ``problems`` is a list of
+    (data tensor [n, d] float32 on the GPU, k, metric[, path])."""
+
+    def __init__(self, problems, device: int | torch.device = 0, smooth: bool = True):
+        from ._lib import HmJob, KnnPath
+        self.device = torch.device("cuda", device) if isinstance(device, int) else device
+        self.problems = []
+        jobs = (HmJob * len(problems))()
+        for i, prob in enumerate(problems):
+            data, k, metric = prob[0], int(prob[1]), Metric.parse(prob[2])
+            path = KnnPath.parse(prob[3]) if len(prob) > 3 else KnnPath.AUTO
+            assert data.is_cuda and data.dtype == torch.float32 and data.is_contiguous()
+            n, d = data.shape
+            idx = torch.empty(n * k, dtype=torch.int32, device=self.device)
+            dist = torch.empty(n * k, dtype=torch.float32, device=self.device)
+            sig = torch.empty(n, dtype=torch.float32, device=self.device) if smooth else None
+            rho = torch.empty(n, dtype=torch.float32, device=self.device) if smooth else None
+            self.problems.append((data, idx, dist, sig, rho, k))
+            jobs[i] = HmJob(data.data_ptr(), n, d, k, int(metric), int(path), idx.data_ptr(),
+                            dist.data_ptr(), sig.data_ptr() if smooth else None,
+                            rho.data_ptr() if smooth else None)
+        self._jobs = jobs
+        h = ctypes.c_void_p()
+        check(lib().hm_batch_create(jobs, len(problems), ctypes.byref(h)))
+        self.handle = h
+        ws = lib().hm_batch_workspace_bytes(h)
+        self.workspace = torch.empty(ws + 256, dtype=torch.uint8, device=self.device)
+        self.ws_ptr = (self.workspace.data_ptr() + 255) // 256 * 256
+        s = torch.cuda.current_stream(self.device)
+        check(lib().hm_batch_bind(h, self.ws_ptr, ws, s.cuda_stream))
+        s.synchronize()  # the job tables are staged from host memory
+
+    def run(self, stream: torch.cuda.Stream | None = None, graph: bool = False) -> None:
+        s = stream if stream is not None else torch.cuda.current_stream(self.device)
+        fn = lib().hm_batch_graph_launch if graph else lib().hm_batch_run
+        check(fn(self.handle, s.cuda_stream))
+
+    def stats(self, job: int) -> HmStats:
+        st = HmStats()
+        check(lib().hm_batch_job_stats(self.handle, job, ctypes.byref(st)))
+        return st
+
+    def path(self, job: int) -> int:
+        return lib().hm_batch_job_path(self.handle, job)
+
+    def result(self, job: int):
+        """(indices uint32, dists, sigmas, rhos) of one job as numpy arrays."""
+        import numpy as np
+        _, idx, dist, sig, rho, _ = self.problems[job]
+        out = [idx.cpu().numpy().view(np.uint32), dist.cpu().numpy()]
+        out += [sig.cpu().numpy(), rho.cpu().numpy()] if sig is not None else [None, None]
+        return out
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h is not None and h.value:
+            try:
+                lib().hm_batch_destroy(h)
+            except Exception:
+                pass

@@ -131,6 +131,49 @@ HM_API int hm_smooth_knn_device(const float *d_dists, uint64_t n, uint32_t k, fl
                          float *d_rho, void *d_workspace, void *stream);
 
 /* ----------------------------------------------------------------------------
+ * Batches: many independent problems of uneven n, d, k and metric in one
+ * pass of the device pipeline (every kernel works on the whole batch; the
+ * screened jobs of one operand format share one persistent screen launch).
+ * No reference counterpart: the reference embeds one dataset per call; each
+ * job is the same computation as exact_knn + smooth_knn on its own data.
+ * ------------------------------------------------------------------------- */
+
+/* One problem of a batch.  All pointers are device pointers; sigma_out /
+ * rho_out NULL skips smooth-kNN for the job. */
+typedef struct hm_job {
+    const float *data;  /* n x d row-major */
+    uint64_t n;
+    uint32_t d, k;
+    int32_t metric, path;
+    uint32_t *idx_out;  /* n x k */
+    float *dist_out;    /* n x k */
+    float *sigma_out;   /* n (or NULL) */
+    float *rho_out;     /* n (or NULL) */
+} hm_job;
+
+typedef struct hm_batch hm_batch; /* opaque plan of one batch */
+
+/* Validate and lay out a batch (host only; no device work). */
+HM_API int hm_batch_create(const hm_job *jobs, uint32_t njobs, hm_batch **out);
+HM_API void hm_batch_destroy(hm_batch *batch);
+/* Device scratch the batch needs. */
+HM_API size_t hm_batch_workspace_bytes(const hm_batch *batch);
+/* Attach the workspace (256-byte aligned) and write the batch's job tables
+ * into it, ordered on `stream`. */
+HM_API int hm_batch_bind(hm_batch *batch, void *d_workspace, size_t workspace_bytes, void *stream);
+/* Enqueue the whole pipeline on `stream` (kernel launches only: no host
+ * synchronisation, no allocation). */
+HM_API int hm_batch_run(hm_batch *batch, void *stream);
+/* Same work as hm_batch_run, through a CUDA graph that the first call
+ * captures on `stream` and later calls replay with one launch. */
+HM_API int hm_batch_graph_launch(hm_batch *batch, void *stream);
+/* Counters of one job after the stream has finished (synchronous read).
+ * Returns HM_ERR_INVALID when the job's data held a non-finite value. */
+HM_API int hm_batch_job_stats(const hm_batch *batch, uint32_t job, hm_stats *stats);
+/* The path the planner resolved for one job. */
+HM_API int hm_batch_job_path(const hm_batch *batch, uint32_t job);
+
+/* ----------------------------------------------------------------------------
  * Allocation-free entry point.  No counterpart in the reference (its Rust
  * path allocates its Vecs freely); this exists for callers that cannot call
  * cudaMalloc: a plugin inside a host engine that has already reserved the
