@@ -46,7 +46,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="embed_50k",
-                    choices=["embed_50k", "dups_20k", "blobs_1k"])
+                    choices=["embed_50k", "dups_20k", "blobs_1k", "batch_256"])
     ap.add_argument("--path", default="auto")
     ap.add_argument("--rows", type=int, default=None,
                     help="use only the first ROWS points of the workload (a smaller case "
@@ -147,31 +147,72 @@ def reference_arm(args):
         return 0
     import holomap_oracle
     holomap_oracle.build()
-    wl = workload(args.workload, args.rows)
     threads = os.cpu_count() or 1
-    # one step = a bounded sample of rows, sized for about 4 s of host work
-    probe_rows = max(threads, 4)
-    t = oracle_sample_time(wl, probe_rows, threads)
-    rows = int(max(probe_rows, min(wl.n, probe_rows * 4.0 / max(t, 1e-6))))
-    for _ in range(args.warmup):
-        oracle_sample_time(wl, rows, threads)
-    times = [oracle_sample_time(wl, rows, threads) for _ in range(args.steps)]
-    per_graph = sum(times) / len(times) * wl.n / rows
-    value = 1.0 / per_graph
+    if args.workload == "batch_256":
+        from holomap_b200.synth import batch_256
+        wls = batch_256()
+        # one step = row samples of 8 datasets on all host threads, fitted per
+        # row x point x dimension and scaled to the whole batch
+        g = np.random.default_rng(1)
+        total_units = sum(w.n * w.n * w.d for w in wls)
+
+        def sample():
+            pick = g.choice(len(wls), size=8, replace=False)
+            t0 = time.perf_counter()
+            u = 0
+            for j in pick:
+                w = wls[j]
+                r = min(w.n, 8 * threads)
+                holomap_oracle.exact_knn(w.data, w.k, w.metric, rows=(0, r), threads=threads)
+                u += r * w.n * w.d
+            return (time.perf_counter() - t0) / u * total_units
+
+        for _ in range(args.warmup):
+            sample()
+        per_step = [sample() for _ in range(args.steps)]
+        per_batch = sum(per_step) / len(per_step)
+        value = len(wls) / per_batch
+        cfg = batch_config(wls)
+        sample_txt = (f"row samples of 8 of {len(wls)} datasets per step on {threads} threads, "
+                      "scaled to the whole batch")
+        ms = per_batch * 1e3
+    else:
+        wl = workload(args.workload, args.rows)
+        # one step = a bounded sample of rows, sized for about 4 s of host work
+        probe_rows = max(threads, 4)
+        t = oracle_sample_time(wl, probe_rows, threads)
+        rows = int(max(probe_rows, min(wl.n, probe_rows * 4.0 / max(t, 1e-6))))
+        for _ in range(args.warmup):
+            oracle_sample_time(wl, rows, threads)
+        times = [oracle_sample_time(wl, rows, threads) for _ in range(args.steps)]
+        per_graph = sum(times) / len(times) * wl.n / rows
+        value = 1.0 / per_graph
+        cfg = config_of(wl)
+        sample_txt = f"{rows} of {wl.n} query rows per step, scaled by {wl.n}/{rows}"
+        ms = per_graph * 1e3
     line = {
         "metric": METRIC_NAME, "value": value, "unit": UNIT, "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": per_graph * 1e3, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": config_of(wl), "path": "reference (host cores)",
+        "config": cfg, "path": "reference (host cores)",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{rows} of {wl.n} query rows per step, scaled by "
-                                   f"{wl.n}/{rows}; Rust reference not buildable here (no cargo), "
-                                   "timed through its C restatement"},
+                         "sample": sample_txt + "; the Rust reference cannot be built here (no "
+                                   "cargo), so its algorithm runs as the C restatement"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
     return 0
+
+
+def batch_config(wls) -> dict:
+    ns = [w.n for w in wls]
+    return {"workload": "batch_256", "datasets": len(wls), "n_min": min(ns), "n_max": max(ns),
+            "rows_total": int(sum(ns)), "d": sorted({w.d for w in wls}),
+            "k": sorted({w.k for w in wls}),
+            "metrics": {m: sum(w.metric == m for w in wls) for m in ("euclidean", "cosine")},
+            "smooth_knn": True, "launch": "one CUDA graph per step",
+            "l2": "flushed before every timed step (256 MiB write)", "parallelism": "replicas"}
 
 
 def config_of(wl) -> dict:
@@ -181,6 +222,176 @@ def config_of(wl) -> dict:
 
 
 # ------------------------------------------------------------------ ours
+class SingleRunner:
+    """One dataset per step, device-resident input (hm_knn_smooth_device)."""
+
+    def __init__(self, wl, path, dev):
+        import torch
+
+        import holomap_b200 as hm
+        from holomap_b200.device import DeviceKnnProblem
+        self.wl, self.dev = wl, dev
+        p = hm.KnnPath.parse(path)
+        self.path = hm.autotune_path(wl.n, wl.d, wl.k, wl.metric) if p == hm.KnnPath.AUTO else p
+        self.prob = DeviceKnnProblem(wl.n, wl.d, wl.k, wl.metric, self.path, device=dev)
+        self.x_dev = torch.from_numpy(wl.data).to(dev)
+        self.graphs_per_step = 1
+        self.plain = self.path == hm.KnnPath.PLAIN
+
+    def step(self, stream, graph=False):
+        self.prob.run(self.x_dev, stream)
+
+    def e2e_prepare(self):
+        import torch
+        wl = self.wl
+        self.pin_x = torch.from_numpy(wl.data).pin_memory()
+        outs = (torch.empty(wl.n * wl.k, dtype=torch.int32).pin_memory(),
+                torch.empty(wl.n * wl.k, dtype=torch.float32).pin_memory(),
+                torch.empty(wl.n, dtype=torch.float32).pin_memory(),
+                torch.empty(wl.n, dtype=torch.float32).pin_memory())
+        self.outs = outs
+        self.outs_np = (outs[0].numpy().view(np.uint32), outs[1].numpy(), outs[2].numpy(),
+                        outs[3].numpy())
+
+    def e2e_step(self):
+        import holomap_b200 as hm
+        wl = self.wl
+        hm.knn_smooth(self.pin_x.numpy(), wl.d, wl.k, wl.metric, self.path, out=self.outs_np)
+
+    def e2e_matches(self) -> bool:
+        return bool(np.array_equal(self.outs_np[0], self.prob.idx.cpu().numpy().view(np.uint32)) and
+                    np.array_equal(self.outs_np[2].view(np.uint32),
+                                   self.prob.sigma.cpu().numpy().view(np.uint32)))
+
+    def io_bytes(self):
+        wl = self.wl
+        return int(wl.n * wl.d * 4), int(wl.n * wl.k * 8 + wl.n * 8)
+
+    def stats(self) -> dict:
+        st = self.prob.stats()
+        n = self.wl.n
+        return {"path_used": int(st.path_used), "col_splits": int(st.col_splits),
+                "candidates_per_row": st.candidates_total / n,
+                "emitted_per_row": st.candidates_emitted / n,
+                "candidates_max_row": int(st.candidates_max_row),
+                "candidate_cap": int(st.candidate_cap), "overflow_rows": int(st.overflow_rows),
+                "zero_rho_rows": int(st.zero_rho_rows), "screen_band": st.screen_band}
+
+    def config(self):
+        return config_of(self.wl)
+
+    def screened_work(self):
+        """[(n, d)] of the screened problems, [(n, d, metric)] of the exact ones."""
+        wl = self.wl
+        return ([] if self.plain else [(wl.n, wl.d)]), ([(wl.n, wl.d, wl.metric)] if self.plain else [])
+
+    def cpu_baseline(self, seconds):
+        return cpu_baseline(self.wl, seconds, threads=1)
+
+
+class BatchRunner:
+    """All datasets of a batch in one pass of the pipeline, replayed as one
+    captured CUDA graph per step (hm_batch_graph_launch)."""
+
+    def __init__(self, wls, dev):
+        import torch
+
+        from holomap_b200.device import DeviceBatch
+        self.wls, self.dev = wls, dev
+        self.x_dev = [torch.from_numpy(w.data).to(dev) for w in wls]
+        self.batch = DeviceBatch([(x, w.k, w.metric) for x, w in zip(self.x_dev, wls)], device=dev)
+        self.graphs_per_step = len(wls)
+        self.paths = [self.batch.path(j) for j in range(len(wls))]
+        self.plain = False
+
+    def step(self, stream, graph=True):
+        self.batch.run(stream, graph=graph)
+
+    def e2e_prepare(self):
+        import torch
+        self.pin_x = [torch.from_numpy(w.data).pin_memory() for w in self.wls]
+        self.pin_out = [[torch.empty_like(t, device="cpu").pin_memory() for t in prob[1:5]]
+                        for prob in self.batch.problems]
+
+    def e2e_step(self):
+        import torch
+        s = torch.cuda.current_stream(self.dev)
+        for x, p in zip(self.x_dev, self.pin_x):
+            x.copy_(p, non_blocking=True)
+        self.batch.run(s, graph=True)
+        for prob, outs in zip(self.batch.problems, self.pin_out):
+            for t, o in zip(prob[1:5], outs):
+                o.copy_(t, non_blocking=True)
+        s.synchronize()
+
+    def e2e_matches(self) -> bool:
+        return all(np.array_equal(o[0].numpy(), prob[1].cpu().numpy())
+                   for prob, o in zip(self.batch.problems, self.pin_out))
+
+    def io_bytes(self):
+        h2d = sum(int(w.n * w.d * 4) for w in self.wls)
+        d2h = sum(int(w.n * w.k * 8 + w.n * 8) for w in self.wls)
+        return h2d, d2h
+
+    def stats(self) -> dict:
+        import holomap_b200 as hm
+        paths = {}
+        cand = emitted = rows = ovf = 0
+        for j, w in enumerate(self.wls):
+            st = self.batch.stats(j)
+            name = hm.KnnPath(int(st.path_used)).name.lower()
+            paths[name] = paths.get(name, 0) + 1
+            if st.path_used != hm.KnnPath.PLAIN:
+                cand += st.candidates_total
+                emitted += st.candidates_emitted
+                rows += w.n
+                ovf += st.overflow_rows
+        return {"jobs": len(self.wls), "paths": paths,
+                "screened_candidates_per_row": cand / max(rows, 1),
+                "screened_emitted_per_row": emitted / max(rows, 1), "overflow_rows": int(ovf)}
+
+    def config(self):
+        return batch_config(self.wls)
+
+    def screened_work(self):
+        import holomap_b200 as hm
+        scr = [(w.n, w.d) for w, p in zip(self.wls, self.paths) if p != hm.KnnPath.PLAIN]
+        exact = [(w.n, w.d, w.metric) for w, p in zip(self.wls, self.paths) if p == hm.KnnPath.PLAIN]
+        return scr, exact
+
+    def cpu_baseline(self, seconds):
+        return batch_cpu_baseline(self.wls, seconds)
+
+
+def batch_cpu_baseline(wls, target_s: float) -> dict:
+    """The oracle's cost is rows x n x d for every job; time a row sample of
+    eight jobs, fit seconds per row-point-dimension, scale to the batch."""
+    import holomap_oracle
+    g = np.random.default_rng(0)
+    pick = g.choice(len(wls), size=min(8, len(wls)), replace=False)
+    units = secs = 0.0
+    rows = 4
+    while True:
+        t0 = time.perf_counter()
+        u = 0
+        for j in pick:
+            w = wls[j]
+            r = min(rows, w.n)
+            holomap_oracle.exact_knn(w.data, w.k, w.metric, rows=(0, r))
+            u += r * w.n * w.d
+        secs += time.perf_counter() - t0
+        units += u
+        if secs > target_s / 4 or rows > 4096:
+            break
+        rows *= 4
+    per_unit = secs / units
+    total = sum(w.n * w.n * w.d for w in wls) * per_unit
+    return {"value": len(wls) / total, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"row samples of 8 of the {len(wls)} datasets (all points searched), "
+                      f"fitted at {per_unit * 1e9:.3f} ns per row x point x dimension and "
+                      f"scaled to the whole batch; C restatement, 1 thread"}
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -189,9 +400,7 @@ def main():
     import torch
     import torch.distributed as dist
 
-    import holomap_b200 as hm
     from holomap_b200 import _lib
-    from holomap_b200.device import DeviceKnnProblem
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -206,108 +415,100 @@ def main():
         if world > 1:
             dist.barrier()
 
-    wl = workload(args.workload, args.rows)
-    path = hm.KnnPath.parse(args.path)
-    resolved = hm.autotune_path(wl.n, wl.d, wl.k, wl.metric) if path == hm.KnnPath.AUTO else path
-    prob = DeviceKnnProblem(wl.n, wl.d, wl.k, wl.metric, resolved, device=dev)
-    x_dev = torch.from_numpy(wl.data).to(dev)
+    if args.workload == "batch_256":
+        from holomap_b200.synth import batch_256
+        runner = BatchRunner(batch_256(), dev)
+    else:
+        runner = SingleRunner(workload(args.workload, args.rows), args.path, dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
 
-    for _ in range(args.warmup):
-        prob.run(x_dev, stream)
+    # launches per step, counted on a direct (non-graph) run
+    l0 = _lib.launch_count()
+    runner.step(stream, graph=False)
     torch.cuda.synchronize(dev)
-    st = prob.stats()
+    launches_per_step = _lib.launch_count() - l0
+    for _ in range(args.warmup):
+        runner.step(stream)
+    torch.cuda.synchronize(dev)
+    stats = runner.stats()
 
     # timed region: K steps, each bracketed by CUDA events on the launching
     # stream, L2 flushed before each step
-    _lib.timing_enable(True)
-    for cls in _lib.KCLASS:
-        _lib.timing_read(cls, reset=True)
     clocks = ClockSampler(local)
     clocks.start()
     barrier()
     torch.cuda.synchronize(dev)
-    launches0 = _lib.launch_count()
     evs = []
     for _ in range(args.steps):
         flush.zero_()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        prob.run(x_dev, stream)
+        runner.step(stream)
         e1.record(stream)
         evs.append((e0, e1))
     torch.cuda.synchronize(dev)
-    launches = _lib.launch_count() - launches0
     barrier()
     clk = clocks.stop()
-    _lib.timing_enable(False)
     step_ms = [a.elapsed_time(b) for a, b in evs]
     total_ms = sum(step_ms)
-    kern = {cls: _lib.timing_read(cls, reset=True) for cls in _lib.KCLASS}
     if world > 1:
         t = torch.tensor([total_ms], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-    value = world * args.steps / (total_ms / 1e3)
+    value = world * args.steps * runner.graphs_per_step / (total_ms / 1e3)
 
-    # end to end through the public host API: pinned host input, H2D, both
-    # stages, D2H of indices/dists/sigma/rho, every step
+    # per-kernel-class CUDA-event times over the same number of direct
+    # (non-graph) steps: the roofline of the dominant kernel
+    _lib.timing_enable(True)
+    for cls in _lib.KCLASS:
+        _lib.timing_read(cls, reset=True)
+    for _ in range(args.steps):
+        flush.zero_()
+        runner.step(stream, graph=False)
+    torch.cuda.synchronize(dev)
+    _lib.timing_enable(False)
+    kern = {cls: _lib.timing_read(cls, reset=True) for cls in _lib.KCLASS}
+
+    # end to end through the public API: pinned host inputs, H2D, both stages,
+    # D2H of indices/dists/sigma/rho, every step
     e2e_steps = args.e2e_steps or max(3, min(args.steps, 10))
-    pin_x = torch.from_numpy(wl.data).pin_memory()
-    outs = (torch.empty(wl.n * wl.k, dtype=torch.int32).pin_memory(),
-            torch.empty(wl.n * wl.k, dtype=torch.float32).pin_memory(),
-            torch.empty(wl.n, dtype=torch.float32).pin_memory(),
-            torch.empty(wl.n, dtype=torch.float32).pin_memory())
-    outs_np = (outs[0].numpy().view(np.uint32), outs[1].numpy(), outs[2].numpy(), outs[3].numpy())
-    x_np = pin_x.numpy()
-    hm.knn_smooth(x_np, wl.d, wl.k, wl.metric, resolved, out=outs_np)  # warm
+    runner.e2e_prepare()
+    runner.e2e_step()  # warm
     barrier()
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        hm.knn_smooth(x_np, wl.d, wl.k, wl.metric, resolved, out=outs_np)
+        runner.e2e_step()
     e2e_s = time.perf_counter() - t0
     if world > 1:
         t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e_value = world * e2e_steps / e2e_s
-    # the end-to-end result equals the device-resident result
-    same = bool(np.array_equal(outs_np[0], prob.idx.cpu().numpy().view(np.uint32)) and
-                np.array_equal(outs_np[2].view(np.uint32), prob.sigma.cpu().numpy().view(np.uint32)))
+    e2e_value = world * e2e_steps * runner.graphs_per_step / e2e_s
+    same = runner.e2e_matches()
 
-    line = None
     if rank == 0:
-        bulk_ms, bulk_n = kern["bulk"]
-        roof = roofline(wl, resolved, bulk_ms, bulk_n, clk)
+        h2d, d2h = runner.io_bytes()
         line = {
             "metric": METRIC_NAME, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if resolved == hm.KnnPath.PLAIN else "bf16+f64",
-            "data": "synthetic", "config": config_of(wl), "path": str(resolved.name).lower(),
-            "e2e": {"value": e2e_value, "unit": UNIT,
-                    "h2d_bytes_per_step": int(wl.n * wl.d * 4),
-                    "d2h_bytes_per_step": int(wl.n * wl.k * 8 + wl.n * 8),
-                    "steps": e2e_steps, "matches_device_run": same},
-            "gpu_launches": int(launches),
-            "roofline": roof,
+            "dtype": "f64" if runner.plain else "bf16+f64",
+            "data": "synthetic", "config": runner.config(),
+            "path": str(getattr(runner, "path", "auto")).split(".")[-1].lower(),
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": e2e_steps, "matches_device_run": same},
+            "gpu_launches": int(launches_per_step * args.steps),
+            "roofline": roofline(runner, kern, clk, args.workload),
             "kernels_ms_per_step": {c: kern[c][0] / max(args.steps, 1) for c in kern},
             "clocks": clk,
             "step_ms": {"min": min(step_ms), "median": statistics.median(step_ms),
                         "max": max(step_ms)},
-            "stats": {"path_used": int(st.path_used), "col_splits": int(st.col_splits),
-                      "candidates_per_row": st.candidates_total / wl.n,
-                      "emitted_per_row": st.candidates_emitted / wl.n,
-                      "candidates_max_row": int(st.candidates_max_row),
-                      "candidate_cap": int(st.candidate_cap),
-                      "overflow_rows": int(st.overflow_rows),
-                      "zero_rho_rows": int(st.zero_rho_rows),
-                      "screen_band": st.screen_band},
+            "stats": stats,
         }
         if world == 1 and not args.no_cpu_baseline:
-            cb = cpu_baseline(wl, args.cpu_seconds, threads=1)
+            cb = runner.cpu_baseline(args.cpu_seconds)
             cb.pop("seconds", None)
             line["cpu_baseline"] = cb
         print(json.dumps(line), flush=True)
@@ -329,35 +530,40 @@ def traffic_table() -> dict:
     return json.loads(p.read_text()) if p.exists() else {}
 
 
-def roofline(wl, path, bulk_ms, bulk_launches, clk) -> dict:
-    import holomap_b200 as hm
-    avg_s = bulk_ms / max(bulk_launches, 1) / 1e3
+def roofline(runner, kern, clk, workload_name) -> dict:
+    """Roofline of the dominant kernel class: the tensor-core screen (bound
+    'tensor', 2 n^2 d flops per screened problem) or, on the plain path, the
+    exact binary64 kernel (bound 'fp64', per pair and dimension euclidean
+    sub+mul+add, cosine mul+add, manhattan sub+add)."""
     peaks = measured_peaks()
-    key = f"{wl.name}/{str(path).lower()}"
-    traffic = traffic_table().get(key)
-    if path == hm.KnnPath.PLAIN:
-        # binary64 SIMT pipe: per pair and dimension, euclidean sub+mul+add,
-        # cosine mul+add, manhattan sub+add (+abs)
-        per_dim = {"euclidean": 3, "cosine": 2, "manhattan": 2}[wl.metric]
-        ops = float(wl.n) * wl.n * wl.d * per_dim
-        mhz = clk.get("sm_mhz") or 1965.0
-        peak = 148 * 64 * mhz * 1e6  # 64 binary64 lanes per SM, one op each per clock
-        return {"bound": "fp64", "kernel": "plain_knn_kernel",
-                "achieved": ops / avg_s / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
-                "frac": ops / avg_s / peak, "traffic": traffic,
-                "algorithmic": f"{per_dim} binary64 ops x N^2 x d = {ops:.3e} per launch",
-                "peak_source": f"nominal: 148 SMs x 64 FP64 lanes x measured median "
-                               f"{mhz:.0f} MHz (no measured FP64 peak available)",
-                "launches": bulk_launches, "avg_launch_ms": avg_s * 1e3}
-    flops = 2.0 * wl.n * wl.n * wl.d
-    peak = peaks.get("bf16_tflops_sustained", 1400.0)
-    src = "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)" if peaks else \
-        "fallback 1.4 PFLOP/s sustained (of fallback)"
-    return {"bound": "tensor", "kernel": "screen_gemm",
-            "achieved": flops / avg_s / 1e12, "peak": peak, "unit": "TFLOP/s",
-            "frac": flops / avg_s / 1e12 / peak, "traffic": traffic,
-            "algorithmic": f"2 x N^2 x d = {flops:.3e} flops per launch",
-            "peak_source": src, "launches": bulk_launches, "avg_launch_ms": avg_s * 1e3}
+    scr, exact = runner.screened_work()
+    traffic = traffic_table().get(f"{workload_name}/{'plain' if not scr else 'screen'}")
+    if scr:
+        ms, launches = kern["bulk"]
+        flops = sum(2.0 * n * n * d for n, d in scr)
+        peak = peaks.get("bf16_tflops_sustained", 1400.0)
+        src = "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)" if peaks else \
+            "fallback 1.4 PFLOP/s sustained (of fallback)"
+        avg_s = ms / max(launches, 1) / 1e3
+        return {"bound": "tensor", "kernel": "screen_gemm_kernel",
+                "achieved": flops / avg_s / 1e12, "peak": peak, "unit": "TFLOP/s",
+                "frac": flops / avg_s / 1e12 / peak, "traffic": traffic,
+                "algorithmic": f"2 x n^2 x d over {len(scr)} screened problem(s) = "
+                               f"{flops:.3e} flops per launch",
+                "peak_source": src, "launches": launches, "avg_launch_ms": avg_s * 1e3}
+    ms, launches = kern["exact"]
+    per_dim = {"euclidean": 3, "cosine": 2, "manhattan": 2}
+    ops = sum(float(n) * n * d * per_dim[m] for n, d, m in exact)
+    avg_s = ms / max(launches, 1) / 1e3
+    mhz = clk.get("sm_mhz") or 1965.0
+    peak = 148 * 64 * mhz * 1e6  # 64 binary64 lanes per SM, one op each per clock
+    return {"bound": "fp64", "kernel": "plain_knn_kernel",
+            "achieved": ops / avg_s / 1e12, "peak": peak / 1e12, "unit": "TFLOP/s",
+            "frac": ops / avg_s / peak, "traffic": traffic,
+            "algorithmic": f"binary64 ops x n^2 x d = {ops:.3e} per launch",
+            "peak_source": f"nominal: 148 SMs x 64 FP64 lanes x measured median "
+                           f"{mhz:.0f} MHz (no measured FP64 peak available)",
+            "launches": launches, "avg_launch_ms": avg_s * 1e3}
 
 
 if __name__ == "__main__":

@@ -160,7 +160,7 @@ SIGNATURES = {
     "hm_batch_job_path": (_i32, [_vp, _u32]),
 }
 
-KCLASS = {"bulk": 0, "select": 1, "smooth": 2, "prep": 3}
+KCLASS = {"bulk": 0, "select": 1, "smooth": 2, "prep": 3, "exact": 4}
 
 
 def timing_enable(on: bool = True) -> None:

@@ -57,14 +57,7 @@ static uint32_t pow2ceil(uint32_t v) {
     return p;
 }
 
-static int sm_count() {
-    int dev = 0, sms = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && sms > 0)
-        return sms;
-    cudaGetLastError();  // no device here: plan for a B200
-    return 148;
-}
+static int sm_count() { return device_sm_count(); }
 
 // ------------------------------------------------------------ validation
 static int validate_shape(uint64_t n, uint32_t d, uint32_t k, int metric) {
@@ -134,7 +127,7 @@ struct hm_batch {
     bool any_plain = false, any_screen = false, any_smooth = false, any_split = false;
     size_t off_tables = 0, off_jobs = 0, off_counters = 0, off_row_starts = 0, off_job_blocks = 0;
     size_t off_items[3] = {}, off_fb[3] = {};
-    size_t tables_bytes = 0, total = 0;
+    size_t tables_bytes = 0, tables_used = 0, total = 0;
     // bound state
     char *ws = nullptr;
     std::vector<char> table;           // host image of the tables
@@ -312,23 +305,31 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B) {
         off = align256(off + std::max<size_t>(bytes, 1));
         return where;
     };
-    // tables (written by bind, contiguous)
+    // tables (written by bind as one blob; packed at 16-byte alignment so a
+    // single job's tables fit in one kernel's parameters)
     B.off_tables = off;
-    B.off_jobs = take(sizeof(JobDev) * njobs);
-    B.off_row_starts = take(sizeof(uint32_t) * (njobs + 1));
-    B.off_job_blocks = take(sizeof(uint32_t) * (njobs + 1));
+    auto pack = [&](size_t bytes) {
+        const size_t where = off;
+        off = round_up(off + bytes, 16);
+        return where;
+    };
+    B.off_jobs = pack(sizeof(JobDev) * njobs);
+    B.off_row_starts = pack(sizeof(uint32_t) * (njobs + 1));
+    B.off_job_blocks = pack(sizeof(uint32_t) * (njobs + 1));
     for (int m = 0; m < 3; ++m) {
-        B.off_items[m] = take(sizeof(uint2) * B.items[m].size());
-        B.off_fb[m] = take(sizeof(uint32_t) * B.fb_jobs[m].size());
+        B.off_items[m] = pack(sizeof(uint2) * B.items[m].size());
+        B.off_fb[m] = pack(sizeof(uint32_t) * B.fb_jobs[m].size());
     }
     for (int g = 0; g < 3; ++g) {
         GroupPlan &Gp = B.groups[g];
         if (Gp.jobs.empty()) continue;
-        Gp.off_gdev = take(sizeof(GroupDev));
-        Gp.off_job_ids = take(sizeof(uint32_t) * Gp.jobs.size());
-        Gp.off_row_starts = take(sizeof(uint32_t) * (Gp.jobs.size() + 1));
-        Gp.off_unit_starts = take(sizeof(uint32_t) * (Gp.jobs.size() + 1));
+        Gp.off_gdev = pack(sizeof(GroupDev));
+        Gp.off_job_ids = pack(sizeof(uint32_t) * Gp.jobs.size());
+        Gp.off_row_starts = pack(sizeof(uint32_t) * (Gp.jobs.size() + 1));
+        Gp.off_unit_starts = pack(sizeof(uint32_t) * (Gp.jobs.size() + 1));
     }
+    B.tables_used = off - B.off_tables;
+    off = align256(off);
     B.tables_bytes = off - B.off_tables;
     // device-written
     B.off_counters = take(sizeof(JobCounters) * njobs);
@@ -368,7 +369,7 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B) {
 // --------------------------------------------------------------- binding
 // Small tables are written by a kernel from its parameters (no host memory
 // stays referenced); larger ones by one copy from pinned staging.
-constexpr uint32_t kParamTable = 3072;
+constexpr uint32_t kParamTable = 3968;  // + the destination pointer: within 4 KB
 struct ParamTable {
     uint32_t bytes;
     unsigned char data[kParamTable];
@@ -498,10 +499,11 @@ static int bind_batch(hm_batch &B, void *d_ws, size_t bytes, cudaStream_t s) {
     }
 
     char *dst = ws + B.off_tables;
-    if (B.tables_bytes <= kParamTable) {
+    const size_t used = B.tables_used;  // tables_bytes adds the 256-byte padding
+    if (used <= kParamTable) {
         ParamTable t;
-        t.bytes = (uint32_t)B.tables_bytes;
-        memcpy(t.data, B.table.data(), B.tables_bytes);
+        t.bytes = (uint32_t)used;
+        memcpy(t.data, B.table.data(), used);
         write_table_kernel<<<1, 256, 0, s>>>(dst, t);
         HM_CUDA_TRY(cudaGetLastError());
         count_launch();

@@ -38,6 +38,12 @@ void clear_error();
 
 inline size_t round_up(size_t x, size_t m) { return (x + m - 1) / m * m; }
 
+// Sets a kernel's dynamic shared-memory limit once per device (the attribute
+// call is kept off the per-launch path).
+int ensure_dynamic_smem(const void *func, int bytes);
+// Multiprocessor count of the current device (cached; 148 without a device).
+int device_sm_count();
+
 // ----------------------------------------------------------- instrumentation
 // Every kernel launch calls count_launch(); ScopedKernelTimer records an
 // event pair around the launches in its scope when timing is enabled.

@@ -295,7 +295,7 @@ static int launch_plain_metric(const PlainWork &w, uint32_t grid, cudaStream_t s
 int launch_plain(const PlainWork &w, int metric, cudaStream_t s) {
     const uint32_t grid = w.fallback ? w.fb_njobs * w.per_job : w.nitems;
     if (grid == 0) return HM_OK;
-    ScopedKernelTimer timer(HM_KCLASS_BULK, s);
+    ScopedKernelTimer timer(HM_KCLASS_EXACT, s);
     switch (metric) {
     case HM_METRIC_EUCLIDEAN: return launch_plain_metric<HM_METRIC_EUCLIDEAN>(w, grid, s);
     case HM_METRIC_COSINE: return launch_plain_metric<HM_METRIC_COSINE>(w, grid, s);

@@ -183,8 +183,7 @@ static int launch_metric(const JobDev *jobs, const GroupDev &G, const GroupDev *
     const int blocks = (int)((G.rows + RR_WARPS - 1) / RR_WARPS);
 #define HM_RR_CASE(K)                                                                       \
     case K: {                                                                               \
-        HM_CUDA_TRY(cudaFuncSetAttribute(rerank_kernel<METRIC, K>,                          \
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+        HM_TRY(ensure_dynamic_smem((const void *)rerank_kernel<METRIC, K>, (int)smem));     \
         rerank_kernel<METRIC, K><<<blocks, RR_WARPS * 32, smem, s>>>(jobs, Gd, dstride);    \
         break;                                                                              \
     }

@@ -506,13 +506,9 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
 template <int KIND, int KP>
 static int launch_kind(const JobDev *jobs, const GroupDev &G, const CUtensorMap &ta,
                        const CUtensorMap &tb, float *dump, uint32_t idesc, cudaStream_t s) {
-    HM_CUDA_TRY(cudaFuncSetAttribute(screen_gemm_kernel<KIND, KP>,
-                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)SC_SMEM_BYTES));
-    int dev = 0, sms = 148;
-    HM_CUDA_TRY(cudaGetDevice(&dev));
-    HM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const uint32_t grid = G.units < (uint32_t)sms ? G.units : (uint32_t)sms;
+    HM_TRY(ensure_dynamic_smem((const void *)screen_gemm_kernel<KIND, KP>, (int)SC_SMEM_BYTES));
+    const uint32_t sms = (uint32_t)device_sm_count();
+    const uint32_t grid = G.units < sms ? G.units : sms;
     screen_gemm_kernel<KIND, KP><<<grid, SC_THREADS, SC_SMEM_BYTES, s>>>(ta, tb, jobs, G, dump, idesc);
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();

@@ -26,6 +26,50 @@ static ClassTimes g_classes[HM_KCLASS_COUNT];
 static std::vector<cudaEvent_t> g_free;
 
 void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+namespace {
+struct SmemSetting {
+    const void *func;
+    int device;
+    int bytes;
+};
+std::mutex g_attr_mu;
+std::vector<SmemSetting> g_attr;
+int g_sms[64] = {};
+}  // namespace
+
+int ensure_dynamic_smem(const void *func, int bytes) {
+    int dev = 0;
+    HM_CUDA_TRY(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    for (const SmemSetting &a : g_attr)
+        if (a.func == func && a.device == dev && a.bytes >= bytes) return HM_OK;
+    HM_CUDA_TRY(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    for (SmemSetting &a : g_attr)
+        if (a.func == func && a.device == dev) {
+            a.bytes = bytes;
+            return HM_OK;
+        }
+    g_attr.push_back({func, dev, bytes});
+    return HM_OK;
+}
+
+int device_sm_count() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return 148;
+    }
+    if (!g_sms[dev]) {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
+            cudaGetLastError();
+            return 148;
+        }
+        g_sms[dev] = sms;
+    }
+    return g_sms[dev];
+}
 bool timing_enabled() { return g_timing.load(std::memory_order_relaxed); }
 
 static cudaEvent_t take_event() {

@@ -216,11 +216,12 @@ HM_API int hm_autotune_path(uint64_t n, uint32_t d, uint32_t k, int metric);
  * this path).  With timing enabled the library records a CUDA event pair, on
  * the launching stream, around every launch of each kernel class below.
  * ------------------------------------------------------------------------- */
-#define HM_KCLASS_BULK 0   /* N x N distance bulk: plain kernel or tensor-core screen */
+#define HM_KCLASS_BULK 0   /* tensor-core screen (the screened paths' N x N bulk) */
 #define HM_KCLASS_SELECT 1 /* split merge / exact rerank + select */
 #define HM_KCLASS_SMOOTH 2 /* smooth-kNN calibration */
 #define HM_KCLASS_PREP 3   /* input checks, binary64 copy, operand prep */
-#define HM_KCLASS_COUNT 4
+#define HM_KCLASS_EXACT 4  /* exact binary64 kernel (plain path and fallback rows) */
+#define HM_KCLASS_COUNT 5
 
 HM_API int hm_timing_enable(int on);
 /* Sum of event-timed milliseconds and launch count of one class since the
