@@ -119,7 +119,7 @@ struct GroupPlan {
 struct hm_batch {
     std::vector<hm::JobPlan> jobs;
     hm::GroupPlan groups[3];  // bf16, tf32, split bf16
-    uint32_t all_rows = 0, kpl_all = 1, kpl_plain[3] = {1, 1, 1}, kpl_fb[3] = {1, 1, 1};
+    uint32_t all_rows = 0, kmax = 0, kpl_all = 1, kpl_plain[3] = {1, 1, 1}, kpl_fb[3] = {1, 1, 1};
     std::vector<uint2> items[3];       // exact-path work per metric
     std::vector<uint32_t> fb_jobs[3];  // screened jobs per metric (fallback rows)
     uint32_t fb_per_job[3] = {1, 1, 1};
@@ -184,6 +184,7 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B) {
         P.arow0 = B.all_rows;
         B.all_rows += (uint32_t)s.n;
         B.kpl_all = std::max<uint32_t>(B.kpl_all, (uint32_t)kpl_for_k(s.k));
+        B.kmax = std::max<uint32_t>(B.kmax, s.k);
         if (s.sigma_out && s.rho_out) B.any_smooth = true;
         if (path == HM_PATH_PLAIN) plain_groups += (s.n + PL_BM - 1) / PL_BM;
     }
@@ -566,7 +567,7 @@ static int run_batch(hm_batch &B, cudaStream_t s) {
     if (B.any_split)
         HM_TRY(launch_merge(jobs, njobs, njobs > 1 ? row_starts : nullptr, B.all_rows, B.kpl_all, s));
     if (B.any_smooth) {
-        HM_TRY(launch_smooth(jobs, njobs, njobs > 1 ? row_starts : nullptr, B.all_rows, s));
+        HM_TRY(launch_smooth(jobs, njobs, njobs > 1 ? row_starts : nullptr, B.all_rows, B.kmax, s));
         HM_TRY(launch_mean_all_floor(jobs, njobs, s));
     }
     return HM_OK;
@@ -818,7 +819,7 @@ int hm_smooth_knn_device(const float *d_dists, uint64_t n, uint32_t k, float *d_
     write_smooth_job_kernel<<<1, 32, 0, s>>>(jd, J);
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();
-    HM_TRY(launch_smooth(jd, 1, nullptr, (uint32_t)n, s));
+    HM_TRY(launch_smooth(jd, 1, nullptr, (uint32_t)n, k, s));
     HM_TRY(launch_mean_all_floor(jd, 1, s));
     return HM_OK;
 }

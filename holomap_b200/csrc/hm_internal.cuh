@@ -243,7 +243,7 @@ int launch_merge(const JobDev *jobs, uint32_t njobs, const uint32_t *row_starts,
 // rows whose rho is 0 get their unfloored sigma and are listed for the
 // job's global-mean floor.
 int launch_smooth(const JobDev *jobs, uint32_t njobs, const uint32_t *row_starts, uint32_t rows,
-                  cudaStream_t s);
+                  uint32_t kmax, cudaStream_t s);
 // Sequential binary64 mean of each job's n*k distances, applied as the floor
 // of its listed rows; one block per job, idle when its list is empty.
 int launch_mean_all_floor(const JobDev *jobs, uint32_t njobs, cudaStream_t s);

@@ -66,10 +66,16 @@ using namespace hm;
 extern "C" {
 
 // Autotuner table: the path HM_PATH_AUTO takes.  Screened paths need an inner
-// product form (euclidean, cosine), k <= 64 and d <= 2048; below a few
-// thousand points the plain path's single pass is as fast as screen + rerank.
+// product form (euclidean, cosine), k <= 64 and d <= 2048.  Below 512 points
+// the exact pass is a few microseconds and the screen's extra launches do not
+// pay.  Up to d = 256 the screen is bound by its per-column epilogue, not by
+// the tensor cores, so the split-bf16 operand (three products, error ~2^-16
+// of the norms) costs little over one product and keeps the keep band tight
+// for tightly clustered data; above that, bf16 (cosine: unit vectors, band
+// ~2^-7) or tf32 (euclidean) single products.
 int hm_autotune_path(uint64_t n, uint32_t d, uint32_t k, int metric) {
-    if (metric == HM_METRIC_MANHATTAN || k > 64 || d > 2048 || n < 4096) return HM_PATH_PLAIN;
+    if (metric == HM_METRIC_MANHATTAN || k > 64 || d > 2048 || n < 512) return HM_PATH_PLAIN;
+    if (d <= 256) return HM_PATH_SCREEN_BF16X3;
     if (metric == HM_METRIC_COSINE) return HM_PATH_SCREEN_BF16;
     return HM_PATH_SCREEN_TF32;
 }

@@ -4,7 +4,9 @@
 // MIN_K_DIST_SCALE floors), mean at :82-84, and libm::expf reached through
 // src/fmath.rs:119-122.
 //
-// One warp per row (of any job).  Lanes evaluate the row's exp terms in parallel; the
+// Rows of jobs with k <= 32 take one thread each (smooth_knn_row_kernel: the
+// row in registers, the reference's loop as written).  Larger k: one warp per
+// row (of any job).  Lanes evaluate the row's exp terms in parallel; the
 // binary32 partial sum is then formed in the reference's order (j = 1, 2, ...,
 // k-1, each add rounded) by broadcasting the terms, so every lane holds the
 // same psum and all control flow is warp-uniform.  All arithmetic uses
@@ -101,7 +103,7 @@ __global__ void __launch_bounds__(256) smooth_knn_kernel(const JobDev *__restric
     const uint32_t ar = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (ar >= rows) return;
     const JobDev &J = jobs[row_starts ? find_job(row_starts, njobs, ar) : 0];
-    if (!J.sigma || !J.rho) return;
+    if (!J.sigma || !J.rho || J.k <= 32) return;  // k <= 32: smooth_knn_row_kernel
     const uint32_t row = ar - J.arow0, k = J.k;
     const double target = J.target;
     const float *v = J.dist + (size_t)row * k;
@@ -175,13 +177,92 @@ __global__ void __launch_bounds__(256) smooth_knn_kernel(const JobDev *__restric
     }
 }
 
+// One thread per row for k <= KC: the row stays in registers and the whole
+// calibration is the reference's sequential loop, with no shuffles.  Rows of
+// jobs with k > KC are left to smooth_knn_kernel.
+template <int KC>
+__global__ void __launch_bounds__(128) smooth_knn_row_kernel(const JobDev *__restrict__ jobs, uint32_t njobs,
+                                                             const uint32_t *__restrict__ row_starts,
+                                                             uint32_t rows) {
+    const uint32_t ar = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ar >= rows) return;
+    const JobDev &J = jobs[row_starts ? find_job(row_starts, njobs, ar) : 0];
+    if (!J.sigma || !J.rho || J.k > KC) return;
+    const uint32_t row = ar - J.arow0, k = J.k;
+    const double target = J.target;
+    const float *src = J.dist + (size_t)row * k;
+    float v[KC];
+#pragma unroll
+    for (int j = 0; j < KC; ++j) v[j] = (j < (int)k) ? src[j] : 0.0f;
+
+    // rho: first positive distance in row order, else 0 (src/smooth_knn.rs:35)
+    float rh = 0.0f;
+    bool found = false;
+#pragma unroll
+    for (int j = 0; j < KC; ++j) {
+        if (!found && j < (int)k && v[j] > 0.0f) {
+            rh = v[j];
+            found = true;
+        }
+    }
+    // bisection, binary32 state, hi seeded at f32::MAX (src/smooth_knn.rs:39-65)
+    const float f32max = __uint_as_float(0x7f7fffffu);
+    float lo = 0.0f, hi = f32max, mid = 1.0f;
+    for (int it = 0; it < 64; ++it) {
+        float psum = 0.0f;
+#pragma unroll
+        for (int j = 1; j < KC; ++j) {
+            if (j < (int)k) {
+                const float dd = __fsub_rn(v[j], rh);
+                psum = __fadd_rn(psum, (dd > 0.0f) ? expf_libm(-__fdiv_rn(dd, mid)) : 1.0f);
+            }
+        }
+        const double ps = (double)psum;
+        if (fabs(__dsub_rn(ps, target)) < 1e-5) break;
+        if (ps > target) {
+            hi = mid;
+            mid = __fdiv_rn(__fadd_rn(lo, hi), 2.0f);
+        } else {
+            lo = mid;
+            if (hi >= f32max)
+                mid = __fmul_rn(mid, 2.0f);
+            else
+                mid = __fdiv_rn(__fadd_rn(lo, hi), 2.0f);
+        }
+    }
+    float sg = mid;
+    if (rh > 0.0f) {
+        // floor = 1e-3 * mean(row), mean = f32(sequential f64 sum / k)
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < KC; ++j)
+            if (j < (int)k) s = __dadd_rn(s, (double)v[j]);
+        const float floor_v = __fmul_rn(1e-3f, __double2float_rn(__ddiv_rn(s, (double)k)));
+        if (sg < floor_v) sg = floor_v;
+    } else {
+        // floored later with the job's global mean (mean_all_floor_kernel)
+        const uint32_t slot = atomicAdd(&J.cnt->zero_count, 1u);
+        J.zero_rows[slot] = row;
+    }
+    J.sigma[row] = sg;
+    J.rho[row] = rh;
+}
+
 int launch_smooth(const JobDev *jobs, uint32_t njobs, const uint32_t *row_starts, uint32_t rows,
-                  cudaStream_t s) {
-    const int blocks = (int)((rows + 7) / 8);
+                  uint32_t kmax, cudaStream_t s) {
     ScopedKernelTimer timer(HM_KCLASS_SMOOTH, s);
-    smooth_knn_kernel<<<blocks, 256, 0, s>>>(jobs, njobs, row_starts, rows);
+    // every job with k <= 32 (the kernel returns for rows of larger k)
+    if (kmax <= 16)
+        smooth_knn_row_kernel<16><<<(rows + 127) / 128, 128, 0, s>>>(jobs, njobs, row_starts, rows);
+    else
+        smooth_knn_row_kernel<32><<<(rows + 127) / 128, 128, 0, s>>>(jobs, njobs, row_starts, rows);
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();
+    if (kmax > 32) {  // rows of jobs with k > 32, one warp per row
+        smooth_knn_kernel<<<(int)((rows + 7) / 8), 256, 0, s>>>(jobs, njobs, row_starts, rows);
+        HM_CUDA_TRY(cudaGetLastError());
+        count_launch();
+    }
     return HM_OK;
 }
 
