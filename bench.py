@@ -46,7 +46,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="embed_50k",
-                    choices=["embed_50k", "dups_20k", "blobs_1k", "batch_256"])
+                    choices=["embed_50k", "dups_20k", "blobs_1k", "batch_256", "serve_2000"])
     ap.add_argument("--path", default="auto")
     ap.add_argument("--rows", type=int, default=None,
                     help="use only the first ROWS points of the workload (a smaller case "
@@ -55,6 +55,21 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the oracle baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    # serve_2000 only
+    ap.add_argument("--requests", type=int, default=2000)
+    ap.add_argument("--window", type=int, default=96,
+                    help="serving: requests a client keeps outstanding (output buffers)")
+    ap.add_argument("--inflight", type=int, default=4, help="serving: batches on the device")
+    ap.add_argument("--batch-jobs", type=int, default=32, help="serving: requests per batch")
+    ap.add_argument("--batch-work", type=float, default=4e11,
+                    help="serving: a batch closes once its sum of n*n*d passes this")
+    ap.add_argument("--rate-fracs", type=float, nargs="*", default=[0.5, 0.8, 1.0],
+                    help="serving: open-loop arrival rates as fractions of saturation")
+    ap.add_argument("--serial-seconds", type=float, default=20.0,
+                    help="serving: time bound of each one-request-at-a-time baseline")
+    ap.add_argument("--verify", type=int, default=200,
+                    help="serving: compare the first VERIFY served results with the same "
+                         "requests run one at a time")
     return ap.parse_args()
 
 
@@ -148,9 +163,15 @@ def reference_arm(args):
     import holomap_oracle
     holomap_oracle.build()
     threads = os.cpu_count() or 1
-    if args.workload == "batch_256":
-        from holomap_b200.synth import batch_256
-        wls = batch_256()
+    if args.workload in ("batch_256", "serve_2000"):
+        if args.workload == "batch_256":
+            from holomap_b200.synth import batch_256
+            wls = batch_256()
+        else:
+            from holomap_b200.synth import SERVE_POOL_SLOTS, Workload, serve_2000, serve_pool
+            reqs = serve_2000(1.0, count=args.requests)
+            pools = {(d, s_): serve_pool(d, s_) for d in (32, 64, 300) for s_ in range(SERVE_POOL_SLOTS)}
+            wls = [Workload(f"req_{r.seq}", r.points(pools), r.k, r.metric) for r in reqs]
         # one step = row samples of 8 datasets on all host threads, fitted per
         # row x point x dimension and scaled to the whole batch
         g = np.random.default_rng(1)
@@ -172,9 +193,14 @@ def reference_arm(args):
         per_step = [sample() for _ in range(args.steps)]
         per_batch = sum(per_step) / len(per_step)
         value = len(wls) / per_batch
-        cfg = batch_config(wls)
+        if args.workload == "batch_256":
+            cfg = batch_config(wls)
+        else:
+            cfg = {"workload": "serve_2000", "requests": len(wls), "n": "log-uniform [500, 50000]",
+                   "d": [32, 64, 300], "k": [15, 30], "metrics": "50/40/10 euclidean/cosine/manhattan",
+                   "parallelism": "replicas"}
         sample_txt = (f"row samples of 8 of {len(wls)} datasets per step on {threads} threads, "
-                      "scaled to the whole batch")
+                      "scaled to the whole set (one request at a time)")
         ms = per_batch * 1e3
     else:
         wl = workload(args.workload, args.rows)
@@ -396,6 +422,8 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.workload == "serve_2000":
+        return serve_main(args)
 
     import torch
     import torch.distributed as dist
@@ -511,6 +539,190 @@ def main():
             cb = runner.cpu_baseline(args.cpu_seconds)
             cb.pop("seconds", None)
             line["cpu_baseline"] = cb
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def serve_main(args) -> int:
+    """serve_2000: fit requests through the request loop (hm_ctx_* /
+    hm_submit / hm_wait).  Reports the saturation throughput (a closed loop
+    of clients keeping ``window`` requests outstanding), p50/p99 latency of
+    open-loop Poisson arrivals at fractions of that throughput, and the same
+    requests run one at a time through hm_knn_smooth (plain and auto path).
+    Every request goes host -> device -> host (pinned buffers)."""
+    import threading
+
+    import torch
+    import torch.distributed as dist
+
+    from holomap_b200 import _lib
+    from holomap_b200.serve import Server, host_buffer
+    from holomap_b200.synth import SERVE_POOL_N, SERVE_POOL_SLOTS, serve_2000, serve_pool
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    count = args.requests
+    reqs = serve_2000(1.0, count=count)
+    pools = {}
+    for d in (32, 64, 300):
+        for slot in range(SERVE_POOL_SLOTS):
+            a = host_buffer((SERVE_POOL_N, d), np.float32)
+            a[:] = serve_pool(d, slot)
+            pools[(d, slot)] = a
+    window = args.window
+    kmax = 30
+    outs = [(host_buffer((SERVE_POOL_N, kmax), np.uint32), host_buffer((SERVE_POOL_N, kmax), np.float32),
+             host_buffer(SERVE_POOL_N, np.float32), host_buffer(SERVE_POOL_N, np.float32))
+            for _ in range(window)]
+
+    def out_views(slot, r):
+        i, dd, sg, rh = outs[slot]
+        n, k = r.n, r.k
+        return (i.reshape(-1)[: n * k].reshape(n, k), dd.reshape(-1)[: n * k].reshape(n, k),
+                sg[:n], rh[:n])
+
+    def run(srv, arrivals, keep=None):
+        """Submit reqs at the given offsets (s; None = as fast as the window
+        allows); returns per-request latency (ms) and the wall time."""
+        free = list(range(window))
+        cv = threading.Condition()
+        lat = [0.0] * count
+        outstanding = []
+        done_flag = [False]
+
+        def collector():
+            while True:
+                with cv:
+                    while not outstanding and not done_flag[0]:
+                        cv.wait()
+                    if not outstanding and done_flag[0]:
+                        return
+                    j, t, slot, lag = outstanding.pop(0)
+                srv.wait(t)
+                inf = t.info
+                lat[j] = inf["done_ms"] - inf["submit_ms"] + lag
+                if keep is not None and j < args.verify:
+                    keep[j] = (t.indices.copy(), t.dists.copy(), t.sigmas.copy(), t.rhos.copy())
+                srv.release(t)
+                with cv:
+                    free.append(slot)
+                    cv.notify_all()
+
+        th = threading.Thread(target=collector)
+        th.start()
+        t0 = time.perf_counter()
+        for j, r in enumerate(reqs):
+            if arrivals is not None:
+                wait_s = arrivals[j] - (time.perf_counter() - t0)
+                if wait_s > 0:
+                    time.sleep(wait_s)
+            with cv:
+                while not free:
+                    cv.wait()
+                slot = free.pop()
+            lag = 0.0 if arrivals is None else max(0.0, (time.perf_counter() - t0) - arrivals[j]) * 1e3
+            t = srv.submit(r.points(pools), r.k, r.metric, outputs=out_views(slot, r))
+            with cv:
+                outstanding.append((j, t, slot, lag))
+                cv.notify_all()
+        with cv:
+            done_flag[0] = True
+            cv.notify_all()
+        th.join()
+        return lat, time.perf_counter() - t0
+
+    srv = Server(max_inflight=args.inflight, max_batch_jobs=args.batch_jobs,
+                 max_batch_work=args.batch_work)
+    # warm-up: the first requests once
+    saved = reqs
+    reqs = saved[: min(64, count)]
+    count = len(reqs)
+    run(srv, None)
+    reqs, count = saved, len(saved)
+    if world > 1:
+        dist.barrier()
+    l0 = _lib.launch_count()
+    keep = {}
+    lat_sat, wall = run(srv, None, keep=keep)
+    launches = _lib.launch_count() - l0
+    sat = count / wall
+    if world > 1:
+        t = torch.tensor([wall], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sat = world * count / float(t.item())
+    lat_runs = []
+    for frac in args.rate_fracs:
+        rate = frac * count / wall
+        arr = np.cumsum(np.random.default_rng(5000).exponential(1.0 / rate, size=count))
+        lat, w = run(srv, list(arr))
+        lat_runs.append({"rate_frac_of_saturation": frac, "rate_per_s": rate,
+                         "achieved_graphs_per_s": count / w,
+                         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                         "max_ms": float(max(lat))})
+    totals = srv.totals()
+    srv.close()
+
+    # one request at a time through hm_knn_smooth, bounded to ~args.serial_seconds
+    def serial(path):
+        t0 = time.perf_counter()
+        m = 0
+        same = True
+        for j, r in enumerate(reqs):
+            i, dd, sg, rh = out_views(0, r)
+            x = r.points(pools)
+            _lib.check(_lib.lib().hm_knn_smooth(
+                x.ctypes.data, r.n, r.d, r.k, int(_lib.Metric.parse(r.metric)),
+                int(_lib.KnnPath.parse(path)), i.ctypes.data, dd.ctypes.data, sg.ctypes.data,
+                rh.ctypes.data, None))
+            if j in keep:
+                ki, kd, ks, kr = keep[j]
+                same &= (ki.tobytes() == i.tobytes() and kd.tobytes() == dd.tobytes()
+                         and ks.tobytes() == sg.tobytes() and kr.tobytes() == rh.tobytes())
+            m += 1
+            if time.perf_counter() - t0 > args.serial_seconds:
+                break
+        return m / (time.perf_counter() - t0), m, same
+
+    plain_gs, plain_m, plain_same = serial("plain")
+    auto_gs, auto_m, auto_same = serial("auto")
+    if rank == 0:
+        h2d = sum(r.n * r.d * 4 for r in reqs) / count
+        d2h = sum(r.n * (r.k * 8 + 8) for r in reqs) / count
+        line = {
+            "metric": METRIC_NAME + " + p50/p99 latency", "value": sat, "unit": UNIT,
+            "n_gpus": world, "steps": count, "warmup": 64, "ms_per_step": wall / count * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16+f64", "data": "synthetic",
+            "config": {"workload": "serve_2000", "requests": count,
+                       "n": "log-uniform [500, 50000]", "d": [32, 64, 300], "k": [15, 30],
+                       "metrics": "50/40/10 euclidean/cosine/manhattan",
+                       "client": f"closed loop, {window} requests outstanding (saturation); "
+                                 "open-loop Poisson arrivals for latency",
+                       "max_inflight": args.inflight, "max_batch_jobs": args.batch_jobs,
+                       "max_batch_work": args.batch_work,
+                       "l2": "every request copies its points in from host memory",
+                       "parallelism": "replicas"},
+            "path": "auto",
+            "e2e": {"value": sat, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "note": "serving is host to host: value is already end to end"},
+            "latency": lat_runs,
+            "saturation_latency_ms": {"p50": float(np.percentile(lat_sat, 50)),
+                                      "p99": float(np.percentile(lat_sat, 99))},
+            "one_at_a_time": {
+                "plain": {"graphs_per_s": plain_gs, "requests": plain_m, "same_bytes": plain_same},
+                "auto": {"graphs_per_s": auto_gs, "requests": auto_m, "same_bytes": auto_same}},
+            "gpu_launches": int(launches),
+            "totals": totals,
+        }
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -128,6 +128,50 @@ class HmJob(ctypes.Structure):
     ]
 
 
+class HmCtxConfig(ctypes.Structure):
+    """``hm_ctx_config``: device arena bytes, batches in flight, requests per
+    batch, and the batch's work cap (sum of n*n*d); zeros take the defaults."""
+
+    _fields_ = [
+        ("memory_bytes", ctypes.c_uint64),
+        ("max_inflight", ctypes.c_uint32),
+        ("max_batch_jobs", ctypes.c_uint32),
+        ("max_batch_work", ctypes.c_double),
+    ]
+
+
+class HmRequestInfo(ctypes.Structure):
+    """``hm_request_info``: status, path, batch and steady-clock times (ms)."""
+
+    _fields_ = [
+        ("status", ctypes.c_int32),
+        ("path_used", ctypes.c_int32),
+        ("batch", ctypes.c_uint64),
+        ("batch_jobs", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+        ("submit_ms", ctypes.c_double),
+        ("admit_ms", ctypes.c_double),
+        ("done_ms", ctypes.c_double),
+        ("stats", HmStats),
+    ]
+
+
+class HmCtxTotals(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_uint64),
+        ("finished", ctypes.c_uint64),
+        ("failed", ctypes.c_uint64),
+        ("batches", ctypes.c_uint64),
+        ("arena_bytes", ctypes.c_uint64),
+        ("arena_peak_bytes", ctypes.c_uint64),
+        ("max_batch_jobs_seen", ctypes.c_uint32),
+        ("max_inflight_seen", ctypes.c_uint32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
 # (name, restype, argtypes) for every symbol of include/holomap_cuda.h
 _u64, _u32, _i32, _vp, _sz = (ctypes.c_uint64, ctypes.c_uint32, ctypes.c_int, ctypes.c_void_p,
                               ctypes.c_size_t)
@@ -158,6 +202,17 @@ SIGNATURES = {
     "hm_batch_graph_launch": (_i32, [_vp, _vp]),
     "hm_batch_job_stats": (_i32, [_vp, _u32, _vp]),
     "hm_batch_job_path": (_i32, [_vp, _u32]),
+    "hm_knn_rows_workspace_bytes": (_sz, [_u64, _u32, _u32, _i32, _i32, _u64, _u64]),
+    "hm_knn_rows_device": (_i32, [_vp, _u64, _u32, _u32, _i32, _i32, _u64, _u64, _vp, _vp, _vp, _sz,
+                                  _vp, _vp]),
+    "hm_knn_rows_stats": (_i32, [_vp, _u64, _u32, _u32, _i32, _i32, _u64, _u64, _vp]),
+    "hm_ctx_create": (_i32, [_vp, _vp]),
+    "hm_ctx_destroy": (_i32, [_vp]),
+    "hm_submit": (_i32, [_vp, _vp, _vp]),
+    "hm_poll": (_i32, [_vp, _u64, _vp]),
+    "hm_wait": (_i32, [_vp, _u64, _u64, _vp]),
+    "hm_release": (_i32, [_vp, _u64]),
+    "hm_ctx_totals_read": (_i32, [_vp, _vp]),
 }
 
 KCLASS = {"bulk": 0, "select": 1, "smooth": 2, "prep": 3, "exact": 4}

@@ -90,6 +90,7 @@ struct JobPlan {
     hm_job spec{};
     int path = HM_PATH_PLAIN;
     uint32_t ldd = 0, n_pad = 0, splits = 1, split_cols = 0, arow0 = 0;
+    uint32_t q0 = 0, q1 = 0, rb0 = 0;  // query rows [q0, q1) (a row shard)
     size_t off_x64 = 0, off_rnorm = 0, off_partial = 0, off_zero_rows = 0, off_ovf = 0;
     size_t off_mu = 0, off_csum = 0;
     int group = -1;
@@ -131,13 +132,11 @@ struct hm_batch {
     // bound state
     char *ws = nullptr;
     std::vector<char> table;           // host image of the tables
-    void *pinned = nullptr;            // pinned staging for large tables
     cudaGraphExec_t graph = nullptr;
     cudaStream_t capture = nullptr;    // private stream the graph is captured on
     ~hm_batch() {
         if (graph) cudaGraphExecDestroy(graph);
         if (capture) cudaStreamDestroy(capture);
-        if (pinned) cudaFreeHost(pinned);
     }
 };
 
@@ -152,7 +151,9 @@ static int group_of_path(int path) {
     }
 }
 
-static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B) {
+// `ranges` (optional): 2 per job, the job's query rows [begin, end); every
+// point stays a column.  NULL: all rows.
+static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const uint64_t *ranges = nullptr) {
     if (njobs == 0) return set_error(HM_ERR_INVALID, "empty batch");
     if (njobs > (1u << 16)) return set_error(HM_ERR_UNSUPPORTED, "more than 65536 jobs");
     const uint32_t G = (uint32_t)sm_count();
@@ -179,6 +180,14 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B) {
             return set_error(HM_ERR_UNSUPPORTED,
                              "the screened paths need euclidean or cosine, k <= 64 and d <= 2048");
         P.path = path;
+        const uint64_t q0 = ranges ? ranges[2 * j] : 0, q1 = ranges ? ranges[2 * j + 1] : s.n;
+        if (q0 >= q1 || q1 > s.n)
+            return set_error(HM_ERR_INVALID, "query rows [%llu, %llu) outside [0, %llu)",
+                             (unsigned long long)q0, (unsigned long long)q1, (unsigned long long)s.n);
+        if (ranges && (s.sigma_out || s.rho_out))
+            return set_error(HM_ERR_INVALID, "a row shard has no smooth-kNN outputs");
+        P.q0 = (uint32_t)q0;
+        P.q1 = (uint32_t)q1;
         P.ldd = (uint32_t)round_up(s.d, PL_BK);
         P.n_pad = (uint32_t)(round_up(s.n, PL_ROW_PAD) + PL_ROW_PAD);
         P.arow0 = B.all_rows;
@@ -186,7 +195,7 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B) {
         B.kpl_all = std::max<uint32_t>(B.kpl_all, (uint32_t)kpl_for_k(s.k));
         B.kmax = std::max<uint32_t>(B.kmax, s.k);
         if (s.sigma_out && s.rho_out) B.any_smooth = true;
-        if (path == HM_PATH_PLAIN) plain_groups += (s.n + PL_BM - 1) / PL_BM;
+        if (path == HM_PATH_PLAIN) plain_groups += (P.q1 + PL_BM - 1) / PL_BM - P.q0 / PL_BM;
     }
     // column splits of the exact path: about 4 CTAs per SM slot over the batch
     uint32_t S = plain_groups ? (uint32_t)((1184 + plain_groups - 1) / plain_groups) : 1;
@@ -224,7 +233,8 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B) {
             Gp.kpl = 2;
         }
         Gp.metric_mask |= 1 << P.spec.metric;
-        P.row_blocks = (uint32_t)((P.spec.n + SC_BM - 1) / SC_BM);
+        P.rb0 = P.q0 / SC_BM;
+        P.row_blocks = (P.q1 + SC_BM - 1) / SC_BM - P.rb0;
         P.col_tiles = (uint32_t)((P.spec.n + SC_BN - 1) / SC_BN);
     }
     for (int g = 0; g < 3; ++g) {
@@ -277,8 +287,8 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B) {
         const JobPlan &P = B.jobs[j];
         const int m = P.spec.metric;
         if (P.path == HM_PATH_PLAIN) {
-            const uint32_t groups = (uint32_t)((P.spec.n + PL_BM - 1) / PL_BM);
-            for (uint32_t gi = 0; gi < groups; ++gi)
+            const uint32_t g_end = (P.q1 + PL_BM - 1) / PL_BM;
+            for (uint32_t gi = P.q0 / PL_BM; gi < g_end; ++gi)
                 for (uint32_t sp = 0; sp < P.splits; ++sp) B.items[m].push_back(make_uint2(j, gi << 6 | sp));
             B.kpl_plain[m] = std::max<uint32_t>(B.kpl_plain[m], (uint32_t)kpl_for_k(P.spec.k));
         } else {
@@ -368,8 +378,8 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B) {
 }
 
 // --------------------------------------------------------------- binding
-// Small tables are written by a kernel from its parameters (no host memory
-// stays referenced); larger ones by one copy from pinned staging.
+// Tables are written by kernels from their parameters (no host memory stays
+// referenced).
 constexpr uint32_t kParamTable = 3968;  // + the destination pointer: within 4 KB
 struct ParamTable {
     uint32_t bytes;
@@ -412,9 +422,15 @@ static int bind_batch(hm_batch &B, void *d_ws, size_t bytes, cudaStream_t s) {
         J.metric = (uint32_t)s.metric;
         J.path = (uint32_t)P.path;
         J.arow0 = P.arow0;
+        J.q0 = P.q0;
+        J.q1 = P.q1;
+        J.rb0 = P.rb0;
         J.x = s.data;
-        J.idx = s.idx_out;
-        J.dist = s.dist_out;
+        // outputs hold rows [q0, q1): kernels address them as row * k
+        J.idx = reinterpret_cast<uint32_t *>(reinterpret_cast<uintptr_t>(s.idx_out) -
+                                             (uintptr_t)P.q0 * s.k * sizeof(uint32_t));
+        J.dist = reinterpret_cast<float *>(reinterpret_cast<uintptr_t>(s.dist_out) -
+                                           (uintptr_t)P.q0 * s.k * sizeof(float));
         J.sigma = (s.sigma_out && s.rho_out) ? s.sigma_out : nullptr;
         J.rho = (s.sigma_out && s.rho_out) ? s.rho_out : nullptr;
         J.x64 = at<double>(ws, P.off_x64);
@@ -499,19 +515,17 @@ static int bind_batch(hm_batch &B, void *d_ws, size_t bytes, cudaStream_t s) {
         HM_TRY(make_operand_map(&Gp.tb, D.opb, Gp.rows, Gp.kpmax, Gp.elem_bytes, Gp.kslice, SC_BN));
     }
 
+    // written by kernels from their parameters, 3968 bytes per launch: no
+    // host memory stays referenced by the stream or by a captured graph
     char *dst = ws + B.off_tables;
     const size_t used = B.tables_used;  // tables_bytes adds the 256-byte padding
-    if (used <= kParamTable) {
+    for (size_t o = 0; o < used; o += kParamTable) {
         ParamTable t;
-        t.bytes = (uint32_t)used;
-        memcpy(t.data, B.table.data(), used);
-        write_table_kernel<<<1, 256, 0, s>>>(dst, t);
+        t.bytes = (uint32_t)std::min<size_t>(kParamTable, used - o);
+        memcpy(t.data, B.table.data() + o, t.bytes);
+        write_table_kernel<<<1, 256, 0, s>>>(dst + o, t);
         HM_CUDA_TRY(cudaGetLastError());
         count_launch();
-    } else {
-        if (!B.pinned) HM_CUDA_TRY(cudaMallocHost(&B.pinned, B.tables_bytes));
-        memcpy(B.pinned, B.table.data(), B.tables_bytes);
-        HM_CUDA_TRY(cudaMemcpyAsync(dst, B.pinned, B.tables_bytes, cudaMemcpyHostToDevice, s));
     }
     return HM_OK;
 }
@@ -597,6 +611,14 @@ static int check_counters(const JobCounters &c) {
     if (c.error_code)
         return set_error(HM_ERR_TIMEOUT, "screen kernel gave up waiting (code %u)", c.error_code);
     return HM_OK;
+}
+
+// batch internals for the request loop (serve.cu)
+size_t batch_counters_offset(const hm_batch *B) { return B->off_counters; }
+
+int batch_job_result(const hm_batch *B, uint32_t job, const JobCounters &c, hm_stats *st) {
+    stats_from_counters(*B, job, c, st);
+    return check_counters(c);
 }
 
 // ---------------------------------------------- per-thread device context
@@ -776,6 +798,54 @@ int hm_stats_from_workspace(const void *d_workspace, uint64_t n, uint32_t d, uin
     hm_batch B;
     hm_job spec = one_job(nullptr, n, d, k, metric, path, nullptr, nullptr, nullptr, nullptr);
     HM_TRY(plan_batch(&spec, 1, B));
+    JobCounters c{};
+    HM_CUDA_TRY(cudaMemcpy(&c, static_cast<const char *>(d_workspace) + B.off_counters, sizeof c,
+                           cudaMemcpyDeviceToHost));
+    stats_from_counters(B, 0, c, stats);
+    return check_counters(c);
+}
+
+// A row shard: query rows [row_begin, row_end) against all n points.
+size_t hm_knn_rows_workspace_bytes(uint64_t n, uint32_t d, uint32_t k, int metric, int path,
+                                   uint64_t row_begin, uint64_t row_end) {
+    clear_error();
+    hm_batch B;
+    hm_job spec = one_job(nullptr, n, d, k, metric, path, nullptr, nullptr, nullptr, nullptr);
+    const uint64_t r[2] = {row_begin, row_end};
+    if (plan_batch(&spec, 1, B, r) != HM_OK) return 0;
+    return B.total;
+}
+
+int hm_knn_rows_device(const float *d_data, uint64_t n, uint32_t d, uint32_t k, int metric, int path,
+                       uint64_t row_begin, uint64_t row_end, uint32_t *d_idx, float *d_dist,
+                       void *d_workspace, size_t workspace_bytes, void *stream, hm_stats *stats) {
+    clear_error();
+    if (!d_data) return set_error(HM_ERR_INVALID, "data is NULL");
+    hm_batch B;
+    hm_job spec = one_job(d_data, n, d, k, metric, path, d_idx, d_dist, nullptr, nullptr);
+    const uint64_t r[2] = {row_begin, row_end};
+    HM_TRY(plan_batch(&spec, 1, B, r));
+    if (!d_idx || !d_dist || !d_workspace) return set_error(HM_ERR_INVALID, "NULL pointer argument");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    HM_TRY(bind_batch(B, d_workspace, workspace_bytes, s));
+    HM_TRY(run_batch(B, s));
+    if (stats) {
+        memset(stats, 0, sizeof *stats);
+        stats->path_used = B.jobs[0].path;
+        stats->col_splits = B.jobs[0].splits;
+        stats->candidate_cap = B.jobs[0].path == HM_PATH_PLAIN ? 0 : B.jobs[0].cap;
+    }
+    return HM_OK;
+}
+
+int hm_knn_rows_stats(const void *d_workspace, uint64_t n, uint32_t d, uint32_t k, int metric, int path,
+                      uint64_t row_begin, uint64_t row_end, hm_stats *stats) {
+    clear_error();
+    if (!d_workspace || !stats) return set_error(HM_ERR_INVALID, "NULL pointer argument");
+    hm_batch B;
+    hm_job spec = one_job(nullptr, n, d, k, metric, path, nullptr, nullptr, nullptr, nullptr);
+    const uint64_t r[2] = {row_begin, row_end};
+    HM_TRY(plan_batch(&spec, 1, B, r));
     JobCounters c{};
     HM_CUDA_TRY(cudaMemcpy(&c, static_cast<const char *>(d_workspace) + B.off_counters, sizeof c,
                            cudaMemcpyDeviceToHost));

@@ -168,8 +168,10 @@ struct JobDev {
     // problem and caller buffers (device pointers)
     uint32_t n, d, k, metric, path;
     uint32_t arow0;  // first row in the all-rows space
+    uint32_t q0, q1; // query rows [q0, q1): a row shard; every row is a column
+    uint32_t rb0;    // first 128-row screen block of the query rows
     const float *x;
-    uint32_t *idx;
+    uint32_t *idx;              // addressed as idx[row * k] for rows in [q0, q1)
     float *dist, *sigma, *rho;  // sigma / rho null: no smooth-kNN
     // exact path (and the screened path's fallback)
     double *x64;                 // n_pad x ldd binary64 copy
@@ -247,5 +249,11 @@ int launch_smooth(const JobDev *jobs, uint32_t njobs, const uint32_t *row_starts
 // Sequential binary64 mean of each job's n*k distances, applied as the floor
 // of its listed rows; one block per job, idle when its list is empty.
 int launch_mean_all_floor(const JobDev *jobs, uint32_t njobs, cudaStream_t s);
+
+// batch internals used by the request loop: where a bound batch keeps its
+// per-job counters in the workspace, and a job's stats/status from a host
+// copy of its counters
+size_t batch_counters_offset(const hm_batch *B);
+int batch_job_result(const hm_batch *B, uint32_t job, const JobCounters &c, hm_stats *st);
 
 }  // namespace hm

@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(PL_THREADS, (KPL <= 2 ? 2 : 1)) plain_knn_kern
                 r = at < J.cnt->ovf_count ? J.ovf_list[at] : 0xffffffffu;
             } else {
                 r = grp * PL_BM + tid;
-                if (r >= J.n) r = 0xffffffffu;
+                if (r < J.q0 || r >= J.q1) r = 0xffffffffu;
             }
             s_rows[tid] = r;
         }
@@ -317,6 +317,7 @@ __global__ void __launch_bounds__(256) merge_splits_kernel(const JobDev *__restr
     const JobDev &J = jobs[jb];
     if (J.path != HM_PATH_PLAIN || J.splits <= 1) return;
     const uint32_t row = ar - J.arow0, k = J.k;
+    if (row < J.q0 || row >= J.q1) return;
     WarpTopK<KPL> top;
 #pragma unroll
     for (int q = 0; q < KPL; ++q) {

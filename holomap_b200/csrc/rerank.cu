@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const JobDev *__r
     const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
     if ((int)J.metric != METRIC) return;
     const uint32_t row = gr - J.row0;
-    if (row >= J.n) return;  // padding between jobs
+    if (row < J.q0 || row >= J.q1) return;  // padding between jobs, rows of other shards
     const uint32_t k = J.k, d = J.d, lists = 2 * J.parts;
     const size_t l0 = list_index(J, row, 0);
     double *xi = rr_smem + (size_t)warp * dstride;

@@ -204,7 +204,7 @@ __device__ __forceinline__ UnitTiles unit_tiles(const JobDev *jobs, const GroupD
     t.job = G.job_ids[g];
     const JobDev &J = jobs[t.job];
     const uint32_t lu = u - G.unit_starts[g];
-    t.rb = lu / J.parts;
+    t.rb = J.rb0 + lu / J.parts;
     t.part = lu % J.parts;
     t.ct_begin = t.part * J.part_tiles;
     t.ct_end = min(J.col_tiles, t.ct_begin + J.part_tiles);
@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
             const JobDev &J = jobs[ut.job];
             const uint32_t n = J.n;
             const uint32_t row = ut.rb * SC_BM + row_in_tile;  // job-local
-            const bool valid = row < n;
+            const bool valid = row >= J.q0 && row < J.q1;
             const size_t gr = (size_t)J.row0 + row;              // group row
             // cosine rows compare 1 - v directly (every column term is 1 when
             // the job has no zero vectors)

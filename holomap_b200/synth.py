@@ -17,7 +17,9 @@ row-major, in the orders spelled out below.
                      seed 11.
 * ``serve_2000``    2000 requests, N log-uniform [500, 50000], d in {32, 64, 300},
                      metric 50/40/10 euclidean/cosine/manhattan, k in {15, 30},
-                     one seed per request.
+                     Poisson arrivals, one seed per request; the points of a
+                     request are a prefix of one of four seeded 50,000-point
+                     mixtures of its d (``serve_pool``).
 """
 from __future__ import annotations
 
@@ -121,6 +123,15 @@ class Request:
         return Workload(f"req_{self.seq}", np.ascontiguousarray(x.astype(np.float32)), self.k,
                         self.metric)
 
+    @property
+    def pool_slot(self) -> int:
+        return self.seed % SERVE_POOL_SLOTS
+
+    def points(self, pools: dict) -> np.ndarray:
+        """The request's n x d points: a prefix of its pool (``serve_pool``);
+        ``pools[(d, slot)]`` holds the pool arrays."""
+        return pools[(self.d, self.pool_slot)][: self.n]
+
 
 def serve_2000(rate_per_s: float, count: int = 2000, seed: int = 5000,
                n_lo: int = 500, n_hi: int = 50000) -> list[Request]:
@@ -137,6 +148,21 @@ def serve_2000(rate_per_s: float, count: int = 2000, seed: int = 5000,
         k = int(g.choice([15, 30]))
         reqs.append(Request(i, t, n, d, k, metric, seed + 1 + i))
     return reqs
+
+
+SERVE_POOL_SLOTS = 4
+SERVE_POOL_N = 50000
+
+
+def serve_pool(d: int, slot: int, n: int = SERVE_POOL_N) -> np.ndarray:
+    """One of the seeded 50,000-point Gaussian mixtures of dimension ``d`` that
+    serving requests draw their points from: request i uses the first N rows
+    of slot ``(seed + i) % SERVE_POOL_SLOTS`` of its d (a prefix of a mixture
+    sample is itself a mixture sample), so 2000 requests need 12 pools, not
+    2000 generated datasets."""
+    g = _rng(700000 + 10 * d + slot)
+    clusters = int(g.integers(3, 21))
+    return np.ascontiguousarray(gaussian_mixture(g, n, d, clusters, 4.0, 0.3, 3.0).astype(np.float32))
 
 
 WORKLOADS = {"blobs_1k": blobs_1k, "dups_20k": dups_20k, "embed_50k": embed_50k}

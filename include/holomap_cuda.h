@@ -124,6 +124,25 @@ HM_API int hm_knn_smooth_device(const float *d_data, uint64_t n, uint32_t d, uin
 HM_API int hm_stats_from_workspace(const void *d_workspace, uint64_t n, uint32_t d, uint32_t k,
                             int metric, int path, hm_stats *stats);
 
+/* A row shard of exact_knn (src/knn.rs:22-55): query rows [row_begin,
+ * row_end) against all n points, for splitting one dataset across GPUs (each
+ * rank holds all points and computes its rows).  Row i of d_idx / d_dist
+ * ((row_end - row_begin) x k) is point row_begin + i; indices refer to all n
+ * points; the bytes equal rows [row_begin, row_end) of the whole graph.
+ * smooth-kNN is not part of a shard (a rho == 0 row's sigma floor needs the
+ * mean over all n*k distances): gather the shards' distances and run
+ * hm_smooth_knn_device over all n rows. */
+HM_API size_t hm_knn_rows_workspace_bytes(uint64_t n, uint32_t d, uint32_t k, int metric, int path,
+                                          uint64_t row_begin, uint64_t row_end);
+HM_API int hm_knn_rows_device(const float *d_data, uint64_t n, uint32_t d, uint32_t k, int metric,
+                              int path, uint64_t row_begin, uint64_t row_end, uint32_t *d_idx,
+                              float *d_dist, void *d_workspace, size_t workspace_bytes,
+                              void *stream, hm_stats *stats);
+/* Counters of a finished hm_knn_rows_device call (synchronous read). */
+HM_API int hm_knn_rows_stats(const void *d_workspace, uint64_t n, uint32_t d, uint32_t k,
+                             int metric, int path, uint64_t row_begin, uint64_t row_end,
+                             hm_stats *stats);
+
 /* smooth-kNN alone on device memory (src/smooth_knn.rs:23-80). d_workspace:
  * hm_smooth_workspace_bytes(n) bytes. */
 HM_API size_t hm_smooth_workspace_bytes(uint64_t n);
@@ -172,6 +191,67 @@ HM_API int hm_batch_graph_launch(hm_batch *batch, void *stream);
 HM_API int hm_batch_job_stats(const hm_batch *batch, uint32_t job, hm_stats *stats);
 /* The path the planner resolved for one job. */
 HM_API int hm_batch_job_path(const hm_batch *batch, uint32_t job);
+
+/* ----------------------------------------------------------------------------
+ * Serving: a request loop on one device.  No reference counterpart (the
+ * reference answers one fit_transform call at a time); each request is the
+ * computation of src/api.rs:147-148 on its own data and returns the same
+ * bytes alone or in any mix.
+ *
+ * A context owns a device arena of `memory_bytes`.  Submitted requests wait
+ * in arrival order; a scheduler thread admits them while their device
+ * footprint (points + outputs + pipeline scratch) fits the arena and a batch
+ * slot is free, runs each admitted group as one batch on its own stream
+ * (copy in, pipeline, copy out), and forms the next batch from whatever has
+ * arrived as soon as a slot frees, so batches overlap on the device.
+ * Requests whose footprint exceeds the arena fail with HM_ERR_ADMISSION.
+ * ------------------------------------------------------------------------- */
+
+typedef struct hm_ctx hm_ctx; /* opaque serving context */
+
+typedef struct hm_ctx_config {
+    uint64_t memory_bytes;   /* device arena; 0 = 3/4 of the device's free memory */
+    uint32_t max_inflight;   /* batches on the device at once; 0 = 4 */
+    uint32_t max_batch_jobs; /* requests per batch; 0 = 64 */
+    double max_batch_work;   /* a batch closes once its sum of n*n*d passes this; 0 = 4e11 */
+} hm_ctx_config;
+
+/* What a finished (or pending) request reports. */
+typedef struct hm_request_info {
+    int32_t status;      /* HM_OK, HM_ERR_NOT_READY while queued/running, or its error */
+    int32_t path_used;   /* HM_PATH_* the planner chose */
+    uint64_t batch;      /* sequence number of the batch that ran it */
+    uint32_t batch_jobs; /* requests in that batch */
+    uint32_t reserved;
+    double submit_ms;    /* steady-clock times since hm_ctx_create */
+    double admit_ms;
+    double done_ms;
+    hm_stats stats;      /* the request's counters (device_ms is 0) */
+} hm_request_info;
+
+/* Start a context on the current device (starts the scheduler thread). */
+HM_API int hm_ctx_create(const hm_ctx_config *config_or_null, hm_ctx **out);
+/* Finish every submitted request, stop the scheduler and free the context. */
+HM_API int hm_ctx_destroy(hm_ctx *ctx);
+/* Queue one request.  In a request, data / idx_out / dist_out / sigma_out /
+ * rho_out are HOST pointers (page-locked memory lets the copies overlap;
+ * sigma_out / rho_out may be NULL) that must stay valid until the request
+ * is finished.  Returns a ticket. */
+HM_API int hm_submit(hm_ctx *ctx, const hm_job *request, uint64_t *ticket);
+/* HM_OK when finished successfully, HM_ERR_NOT_READY while pending, else
+ * the request's error.  info (optional) is filled in every case. */
+HM_API int hm_poll(hm_ctx *ctx, uint64_t ticket, hm_request_info *info);
+/* Block until the request finishes or timeout_ns passes (HM_ERR_NOT_READY). */
+HM_API int hm_wait(hm_ctx *ctx, uint64_t ticket, uint64_t timeout_ns, hm_request_info *info);
+/* Forget a finished ticket (its info is no longer kept). */
+HM_API int hm_release(hm_ctx *ctx, uint64_t ticket);
+
+typedef struct hm_ctx_totals {
+    uint64_t submitted, finished, failed, batches;
+    uint64_t arena_bytes, arena_peak_bytes; /* capacity and high-water mark */
+    uint32_t max_batch_jobs_seen, max_inflight_seen;
+} hm_ctx_totals;
+HM_API int hm_ctx_totals_read(hm_ctx *ctx, hm_ctx_totals *totals);
 
 /* ----------------------------------------------------------------------------
  * Allocation-free entry point.  No counterpart in the reference (its Rust

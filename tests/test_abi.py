@@ -89,3 +89,12 @@ def test_null_outputs_rejected():
     x = np.zeros(40, np.float32)
     rc = lib.hm_knn(x.ctypes.data, 20, 2, 3, 0, 1, None, None, None)
     assert rc == hm.HM_ERR_INVALID
+
+
+def test_row_shard_ranges_are_validated_on_cpu():
+    lib = hm.lib()
+    assert lib.hm_knn_rows_workspace_bytes(1000, 8, 5, 0, 1, 0, 1000) > 0
+    assert lib.hm_knn_rows_workspace_bytes(1000, 8, 5, 0, 1, 100, 228) > 0
+    for b, e in [(0, 0), (10, 5), (0, 1001)]:
+        assert lib.hm_knn_rows_workspace_bytes(1000, 8, 5, 0, 1, b, e) == 0
+        assert "query rows" in lib.hm_last_error().decode()
