@@ -95,7 +95,7 @@ struct JobPlan {
     size_t off_mu = 0, off_csum = 0;
     int group = -1;
     uint32_t row0 = 0, unit0 = 0, kp1 = 0, k_stages = 0, row_blocks = 0, col_tiles = 0;
-    uint32_t parts = 1, part_tiles = 0, cap = 0;
+    uint32_t parts = 1, part_tiles = 0, cap = 0, seed_tiles = 0;
     uint64_t slot0 = 0, cand0 = 0, topk0 = 0;
 };
 
@@ -265,6 +265,12 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
                 P.part_tiles = (P.col_tiles + parts - 1) / parts;
                 P.parts = (P.col_tiles + P.part_tiles - 1) / P.part_tiles;
             }
+            // threshold-pass sample: a quarter of the columns, at least 2048
+            // (all of them for small jobs), spread over the parts
+            const uint64_t seed_cols = std::max<uint64_t>(P.spec.n / 4, 2048);
+            P.seed_tiles = std::min<uint32_t>(
+                P.part_tiles, (uint32_t)((seed_cols + (uint64_t)SC_BN * P.parts - 1) / ((uint64_t)SC_BN * P.parts)));
+            P.seed_tiles = std::max<uint32_t>(P.seed_tiles, 1);
             const double per_list = (double)P.spec.n / (2.0 * P.parts);
             const double expect = 1.5 * P.spec.k * (2.0 + std::log(std::fmax(1.0, per_list / P.spec.k)));
             P.cap = std::min<uint32_t>(std::max<uint32_t>(pow2ceil((uint32_t)expect), 128), 4096);
@@ -451,6 +457,7 @@ static int bind_batch(hm_batch &B, void *d_ws, size_t bytes, cudaStream_t s) {
         J.col_tiles = P.col_tiles;
         J.parts = P.parts;
         J.part_tiles = P.part_tiles;
+        J.seed_tiles = P.seed_tiles;
         J.cap = P.cap;
         J.slot0 = P.slot0;
         J.cand0 = P.cand0;
@@ -558,7 +565,9 @@ static int run_batch(hm_batch &B, cudaStream_t s) {
         const GroupDev *Gd = at<GroupDev>(ws, Gp.off_gdev);
         HM_TRY(launch_screen_prep(jobs, Gp.host, Gd, s));
         HM_TRY(launch_screen_band(jobs, Gp.host, Gd, s));
-        HM_TRY(launch_screen_gemm(jobs, Gp.host, Gd, Gp.kp, Gp.ta, Gp.tb, debug_dump_pointer(), s));
+        HM_TRY(launch_screen_gemm(jobs, Gp.host, Gd, Gp.kp, Gp.ta, Gp.tb, debug_dump_pointer(), 0, s));
+        HM_TRY(launch_screen_threshold(jobs, Gp.host, Gd, Gp.kpl, s));
+        HM_TRY(launch_screen_gemm(jobs, Gp.host, Gd, Gp.kp, Gp.ta, Gp.tb, nullptr, 1, s));
         HM_TRY(launch_rerank(jobs, Gp.host, Gd, Gp.kpl, Gp.dmax, Gp.metric_mask, s));
     }
     if (B.any_screen) {

@@ -183,6 +183,7 @@ struct JobDev {
     uint32_t *zero_rows;         // n
     // screened path
     uint32_t group, row0, unit0, kp1, k_stages, row_blocks, col_tiles, parts, part_tiles, cap;
+    uint32_t seed_tiles;         // leading column tiles of each part in the threshold pass
     unsigned long long slot0;    // first candidate list (2 * parts lists per row)
     unsigned long long cand0;    // first candidate slot: list l holds [cand0 + (l - slot0) * cap, +cap)
     unsigned long long topk0;    // first k-array entry: list l's is [topk0 + (l - slot0) * k, +k)

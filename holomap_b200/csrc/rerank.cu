@@ -1,14 +1,21 @@
-// rerank.cu -- exact rerank of the screen's candidates.
+// rerank.cu -- the row threshold between the two screen passes, and the
+// exact rerank of the screen's candidates.
 //
-// One warp per query row.  The row's final screen threshold is the smallest
-// of its parts' k-th screened values (each is an upper bound of the row's
-// k-th); candidates with c^ <= tau + band are compacted into shared memory,
-// and each lane then evaluates one candidate's distance exactly as the
-// reference does (src/metric.rs:42-53 euclidean, :58-70 cosine: binary64,
-// dimension order, no contraction, self forced to 0 as in src/knn.rs:38-39),
-// feeding the (distance bits, index) keys to a warp top-k list.  Rows whose
-// candidate list overflowed, or that the screen cannot bound (zero vectors
-// under cosine), are appended to the overflow list for the exact plain path.
+// threshold: one warp per row merges the k smallest mini-chunk minima of the
+// row's lists into tau1, the k-th smallest of their union.  Every mini-chunk
+// minimum is a screened value of the row, so at least k screened values are
+// <= tau1 and the row's k-th smallest screened value tau^ <= tau1.
+//
+// rerank: one warp per query row.  tau^ is recomputed exactly as the k-th
+// smallest screened value among the emitted candidates (pass 1 emitted every
+// column with c^ <= tau1 + band, which includes the k smallest); candidates
+// with c^ <= tau^ + band are compacted into shared memory, and each lane then
+// evaluates one candidate's distance exactly as the reference does
+// (src/metric.rs:42-53 euclidean, :58-70 cosine: binary64, dimension order,
+// no contraction, self forced to 0 as in src/knn.rs:38-39), feeding the
+// (distance bits, index) keys to a warp top-k list.  Rows whose candidate list
+// overflowed, or that the screen cannot bound (zero vectors under cosine), are
+// appended to the overflow list for the exact plain path.
 #include <cuda_runtime.h>
 
 #include "hm_internal.cuh"
@@ -59,28 +66,23 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const JobDev *__r
         }
         return;
     }
-    // Threshold: the exact k-th smallest screened value of the row.  Every
-    // one of the row's k smallest screened values stays in the k-array of the
-    // list that saw it, so the k-th smallest of the union of the lists'
-    // arrays is exactly that value.
+    // Threshold: the exact k-th smallest screened value of the row, over the
+    // emitted candidates (they include the row's k smallest).
     WarpTopK<KPL> sel;
     sel.reset();
     for (uint32_t p = 0; p < lists; ++p) {
-        const float *kk = G.topk + J.topk0 + (l0 + p - J.slot0) * k;
-        for (uint32_t e0 = 0; e0 < k; e0 += 32) {
+        const uint32_t cnt = G.cand_cnt[l0 + p];
+        const unsigned long long *cand = G.cand + J.cand0 + (l0 + p - J.slot0) * J.cap;
+        for (uint32_t e0 = 0; e0 < cnt; e0 += 32) {
             uint64_t key = KEY_NONE;
-            if (e0 + lane < k) {
-                const uint32_t b = __float_as_uint(kk[e0 + lane]);
-                const uint32_t ord = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-                key = ((uint64_t)ord << 32) | (p * k + e0 + lane);
+            if (e0 + lane < cnt) {
+                const unsigned long long c = cand[e0 + lane];
+                key = ((uint64_t)ord32(__uint_as_float((uint32_t)(c >> 32))) << 32) | (uint32_t)c;
             }
-            if (!__any_sync(0xffffffffu, key < sel.tau)) break;  // arrays are ascending
             sel.offer(key, k, lane);
         }
     }
-    const uint32_t tord = (uint32_t)(sel.tau >> 32);
-    const float tau = sel.tau == KEY_NONE ? __int_as_float(0x7f800000)
-                                          : __uint_as_float((tord & 0x80000000u) ? (tord & 0x7fffffffu) : ~tord);
+    const float tau = sel.tau == KEY_NONE ? __int_as_float(0x7f800000) : unord32((uint32_t)(sel.tau >> 32));
     const float thr = __fadd_ru(tau, G.band[gr]);
 
     for (uint32_t t = lane; t < d; t += 32) xi[t] = (double)J.x[(size_t)row * d + t];
@@ -173,6 +175,49 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const JobDev *__r
         atomicAdd(&J.cnt->candidates, (unsigned long long)kept);
         atomicMax(&J.cnt->max_row, kept);
     }
+}
+
+// tau1 of every row: the k-th smallest of the union of its lists' k smallest
+// mini-chunk minima (an upper bound of the row's k-th screened value).
+template <int KPL>
+__global__ void __launch_bounds__(256) threshold_kernel(const JobDev *__restrict__ jobs,
+                                                       const GroupDev *__restrict__ Gp) {
+    const GroupDev &G = *Gp;
+    const int lane = threadIdx.x & 31;
+    const uint32_t gr = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (gr >= G.rows) return;
+    const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
+    const uint32_t row = gr - J.row0;
+    if (row < J.q0 || row >= J.q1) return;
+    const uint32_t k = J.k, lists = 2 * J.parts;
+    const size_t l0 = list_index(J, row, 0);
+    WarpTopK<KPL> sel;
+    sel.reset();
+    for (uint32_t p = 0; p < lists; ++p) {
+        const float *kk = G.topk + J.topk0 + (l0 + p - J.slot0) * k;
+        for (uint32_t e0 = 0; e0 < k; e0 += 32) {
+            const uint64_t key = (e0 + lane < k) ? (((uint64_t)ord32(kk[e0 + lane]) << 32) | (p * k + e0 + lane))
+                                                 : KEY_NONE;
+            if (!__any_sync(0xffffffffu, key < sel.tau)) break;  // arrays are ascending
+            sel.offer(key, k, lane);
+        }
+    }
+    if (lane == 0) G.rowthr[gr] = sel.tau == KEY_NONE ? ord32(__int_as_float(0x7f800000)) : (uint32_t)(sel.tau >> 32);
+}
+
+int launch_screen_threshold(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t kpl,
+                            cudaStream_t s) {
+    if (G.rows == 0) return HM_OK;
+    ScopedKernelTimer timer(HM_KCLASS_SELECT, s);
+    const int blocks = (int)((G.rows + 7) / 8);
+    switch (kpl) {
+    case 1: threshold_kernel<1><<<blocks, 256, 0, s>>>(jobs, Gd); break;
+    case 2: threshold_kernel<2><<<blocks, 256, 0, s>>>(jobs, Gd); break;
+    default: return set_error(HM_ERR_UNSUPPORTED, "threshold width %u", kpl);
+    }
+    HM_CUDA_TRY(cudaGetLastError());
+    count_launch();
+    return HM_OK;
 }
 
 template <int METRIC>

@@ -67,11 +67,21 @@ struct GroupDev {
     RowStat *rowstat;
     float *rowterm, *colterm, *band;  // colterm padded by SC_BN zeros
     uint8_t *force;               // rows the screen cannot bound (cosine zero vectors)
-    uint32_t *rowthr;             // per row: smallest list threshold so far (ordered key)
+    uint32_t *rowthr;             // per row, ordered key: pass 0 the smallest list k-th so
+                                  // far; pass 1 tau1, the k-th smallest mini-chunk minimum
     unsigned long long *cand;     // candidate lists, (c^ bits << 32) | job-local column
     uint32_t *cand_cnt;
-    float *topk;                  // each list's k smallest c^, ascending
+    float *topk;                  // each list's k smallest mini-chunk minima, ascending
 };
+
+// binary32 <-> unsigned key with the same order (for atomicMin)
+__device__ __forceinline__ uint32_t ord32(float f) {
+    const uint32_t b = __float_as_uint(f);
+    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float unord32(uint32_t o) {
+    return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
+}
 
 // Locations of row i's list s (s < 2 * parts) of job J.
 __device__ __forceinline__ size_t list_index(const JobDev &J, uint32_t i, uint32_t s) {
@@ -81,7 +91,10 @@ __device__ __forceinline__ size_t list_index(const JobDev &J, uint32_t i, uint32
 int launch_screen_prep(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, cudaStream_t s);
 int launch_screen_band(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, cudaStream_t s);
 int launch_screen_gemm(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t kp,
-                       const CUtensorMap &ta, const CUtensorMap &tb, float *dump, cudaStream_t s);
+                       const CUtensorMap &ta, const CUtensorMap &tb, float *dump, int pass,
+                       cudaStream_t s);
+int launch_screen_threshold(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t kpl,
+                            cudaStream_t s);
 int launch_rerank(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t kpl,
                   uint32_t dmax, int metric_mask, cudaStream_t s);
 

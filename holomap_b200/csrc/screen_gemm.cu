@@ -33,7 +33,11 @@ namespace hm {
 
 constexpr uint32_t SC_A_BYTES = SC_BM * SC_SLICE_BYTES;  // 16 KB
 constexpr uint32_t SC_B_BYTES = SC_BN * SC_SLICE_BYTES;  // 32 KB
-constexpr uint32_t SC_SMEM_BYTES = 1024 + SC_STAGES * (SC_A_BYTES + SC_B_BYTES) + 256;
+// A block kept in shared memory for a whole unit when its K slices fit
+// (96 KB: 6 slices of 128 B x 128 rows); otherwise A streams with B.
+constexpr uint32_t SC_ARES_STAGES = 6;
+constexpr uint32_t SC_OPND_BYTES = SC_ARES_STAGES * SC_A_BYTES + SC_STAGES * SC_B_BYTES;  // 224 KB
+constexpr uint32_t SC_SMEM_BYTES = 1024 + SC_OPND_BYTES + 256;
 constexpr uint32_t SC_TMEM_COLS = 512;
 constexpr uint64_t SC_WAIT_LIMIT_NS = 4000000000ull;  // 4 s
 constexpr uint64_t SC_DRAIN_LIMIT_NS = 200000000ull;  // 0.2 s for copies already in flight
@@ -179,14 +183,6 @@ __device__ __forceinline__ void tmem_ld_wait(uint32_t (&v)[32]) {
                  : "memory");
 }
 
-// binary32 <-> unsigned key with the same order (for atomicMin)
-__device__ __forceinline__ uint32_t ord32(float f) {
-    const uint32_t b = __float_as_uint(f);
-    return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
-}
-__device__ __forceinline__ float unord32(uint32_t o) {
-    return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
-}
 
 __device__ __forceinline__ void raise_error(volatile uint32_t *abort_flag, uint32_t *error_code,
                                             uint32_t code) {
@@ -198,7 +194,10 @@ struct UnitTiles {
     uint32_t job, rb, part, ct_begin, ct_end;
 };
 
-__device__ __forceinline__ UnitTiles unit_tiles(const JobDev *jobs, const GroupDev &G, uint32_t u) {
+// Pass 0 (the threshold pass) walks only the first seed_tiles tiles of each
+// part: a sample of the row's columns whose k-th smallest screened value
+// already bounds the row's k-th from above.
+__device__ __forceinline__ UnitTiles unit_tiles(const JobDev *jobs, const GroupDev &G, uint32_t u, int pass) {
     const uint32_t g = find_job(G.unit_starts, G.njobs, u);
     UnitTiles t;
     t.job = G.job_ids[g];
@@ -207,25 +206,30 @@ __device__ __forceinline__ UnitTiles unit_tiles(const JobDev *jobs, const GroupD
     t.rb = J.rb0 + lu / J.parts;
     t.part = lu % J.parts;
     t.ct_begin = t.part * J.part_tiles;
-    t.ct_end = min(J.col_tiles, t.ct_begin + J.part_tiles);
+    t.ct_end = min(J.col_tiles, t.ct_begin + (pass == 0 ? J.seed_tiles : J.part_tiles));
     return t;
 }
 
-template <int KIND, int KP>
+template <int KIND, int KP, int PASS>
 __global__ void __launch_bounds__(SC_THREADS, 1)
     screen_gemm_kernel(const __grid_constant__ CUtensorMap tma, const __grid_constant__ CUtensorMap tmb,
-                       const JobDev *__restrict__ jobs, const GroupDev G, float *dump, uint32_t idesc) {
+                       const JobDev *__restrict__ jobs, const GroupDev G, float *dump, uint32_t idesc,
+                       uint32_t a_res) {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                 ~(uintptr_t)1023);
+    // streaming: stage s holds A at sA + s * 16 KB and B at sB + s * 32 KB;
+    // resident A: the unit's A slices at smem + ks * 16 KB, B stages after them
     uint8_t *sA = smem;
-    uint8_t *sB = smem + SC_STAGES * SC_A_BYTES;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(sB + SC_STAGES * SC_B_BYTES);
+    uint8_t *sB = a_res ? smem + SC_ARES_STAGES * SC_A_BYTES : smem + SC_STAGES * SC_A_BYTES;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + SC_OPND_BYTES);
     uint64_t *full = bars;                  // [SC_STAGES]
     uint64_t *empty = bars + SC_STAGES;     // [SC_STAGES]
     uint64_t *accf = bars + 2 * SC_STAGES;  // [2]
     uint64_t *acce = accf + 2;              // [2]
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(acce + 2);
+    uint64_t *afull = acce + 2;             // resident A loaded
+    uint64_t *aempty = afull + 1;           // resident A consumed by the unit's MMAs
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(aempty + 1);
     volatile uint32_t *abort_flag = tmem_slot + 1;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -239,6 +243,8 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
             mbar_init(smem_u32(&accf[b]), 1);
             mbar_init(smem_u32(&acce[b]), SC_EPI_WARPS);
         }
+        mbar_init(smem_u32(afull), 1);
+        mbar_init(smem_u32(aempty), 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -256,11 +262,26 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
     if (warp == 0) {
         // ------------------------------------------------------ TMA producer
         if (lane == 0) {
-            uint32_t it = 0;
+            uint32_t it = 0, un = 0;
             bool ok = true;
+            constexpr uint32_t kelems = SC_SLICE_BYTES / (KIND == SCREEN_KIND_BF16 ? 2 : 4);
             for (uint32_t u = blockIdx.x; ok && u < G.units; u += gridDim.x) {
-                const UnitTiles ut = unit_tiles(jobs, G, u);
+                const UnitTiles ut = unit_tiles(jobs, G, u, PASS);
                 const JobDev &J = jobs[ut.job];
+                if (a_res) {
+                    // the previous unit's MMAs must be done with the A block
+                    if (un > 0 && !mbar_wait(smem_u32(aempty), (un - 1) & 1, abort_flag)) {
+                        raise_error(abort_flag, &J.cnt->error_code, SC_ERR_PRODUCER);
+                        ok = false;
+                        break;
+                    }
+                    const uint32_t fb = smem_u32(afull);
+                    mbar_arrive_expect_tx(fb, J.k_stages * SC_A_BYTES);
+                    for (uint32_t ks = 0; ks < J.k_stages; ++ks)
+                        tma_load_2d(smem_u32(sA + ks * SC_A_BYTES), &tma, fb, (int32_t)(ks * kelems),
+                                    (int32_t)(J.row0 + ut.rb * SC_BM));
+                    ++un;
+                }
                 for (uint32_t ct = ut.ct_begin; ok && ct < ut.ct_end; ++ct) {
                     for (uint32_t ks = 0; ks < J.k_stages; ++ks, ++it) {
                         const uint32_t s = it % SC_STAGES, r = it / SC_STAGES;
@@ -270,13 +291,20 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                             break;
                         }
                         const uint32_t fb = smem_u32(&full[s]);
-                        mbar_arrive_expect_tx(fb, SC_A_BYTES + SC_B_BYTES);
-                        const int32_t kx = (int32_t)(ks * (SC_SLICE_BYTES / (KIND == SCREEN_KIND_BF16 ? 2 : 4)));
-                        tma_load_2d(smem_u32(sA + s * SC_A_BYTES), &tma, fb, kx, (int32_t)(J.row0 + ut.rb * SC_BM));
+                        const int32_t kx = (int32_t)(ks * kelems);
+                        if (a_res) {
+                            mbar_arrive_expect_tx(fb, SC_B_BYTES);
+                        } else {
+                            mbar_arrive_expect_tx(fb, SC_A_BYTES + SC_B_BYTES);
+                            tma_load_2d(smem_u32(sA + s * SC_A_BYTES), &tma, fb, kx, (int32_t)(J.row0 + ut.rb * SC_BM));
+                        }
                         tma_load_2d(smem_u32(sB + s * SC_B_BYTES), &tmb, fb, kx, (int32_t)(J.row0 + ct * SC_BN));
                     }
                 }
             }
+            // drain: the last A block must have landed before the CTA exits
+            if (a_res && un > 0 && !mbar_wait(smem_u32(afull), (un - 1) & 1, abort_flag, true))
+                raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN);
             // drain: every issued stage must have landed before the CTA exits
             const uint32_t issued = it;
             for (uint32_t t = issued > SC_STAGES ? issued - SC_STAGES : 0; t < issued; ++t) {
@@ -291,11 +319,19 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
     } else if (warp == 1) {
         // ------------------------------------------------------- MMA issuer
         if (lane == 0) {
-            uint32_t it = 0, tile = 0;
+            uint32_t it = 0, tile = 0, un = 0;
             bool ok = true;
             for (uint32_t u = blockIdx.x; ok && u < G.units; u += gridDim.x) {
-                const UnitTiles ut = unit_tiles(jobs, G, u);
+                const UnitTiles ut = unit_tiles(jobs, G, u, PASS);
                 const JobDev &J = jobs[ut.job];
+                if (a_res) {
+                    if (!mbar_wait(smem_u32(afull), un & 1, abort_flag)) {
+                        raise_error(abort_flag, &J.cnt->error_code, SC_ERR_MMA_FULL);
+                        ok = false;
+                        break;
+                    }
+                    fence_after_sync();
+                }
                 for (uint32_t ct = ut.ct_begin; ok && ct < ut.ct_end; ++ct, ++tile) {
                     const uint32_t buf = tile & 1, use = tile >> 1;
                     if (!mbar_wait(smem_u32(&acce[buf]), (use & 1) ^ 1, abort_flag)) {
@@ -313,7 +349,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                             break;
                         }
                         fence_after_sync();
-                        const uint32_t a0 = smem_u32(sA + s * SC_A_BYTES);
+                        const uint32_t a0 = smem_u32(sA + (a_res ? ks : s) * SC_A_BYTES);
                         const uint32_t b0 = smem_u32(sB + s * SC_B_BYTES);
 #pragma unroll
                         for (uint32_t kk = 0; kk < SC_SLICE_BYTES / 32; ++kk)
@@ -324,13 +360,19 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                     if (!ok) break;
                     mma_commit(smem_u32(&accf[buf]));
                 }
+                if (ok && a_res) {
+                    mma_commit(smem_u32(aempty));  // the A block is free once these MMAs finish
+                    ++un;
+                }
             }
-            // drain: the last commit must have landed before TMEM is freed
+            // drain: the last commits must have landed before TMEM is freed
             if (it > 0) {
                 const uint32_t s = (it - 1) % SC_STAGES, r = (it - 1) / SC_STAGES;
                 if (!mbar_wait(smem_u32(&empty[s]), r & 1, abort_flag, true))
                     raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN);
             }
+            if (a_res && un > 0 && !mbar_wait(smem_u32(aempty), (un - 1) & 1, abort_flag, true))
+                raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN);
         }
         __syncwarp();
     } else {
@@ -344,7 +386,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         uint32_t tile = 0;
         bool ok = true;
         for (uint32_t u = blockIdx.x; ok && u < G.units; u += gridDim.x) {
-            const UnitTiles ut = unit_tiles(jobs, G, u);
+            const UnitTiles ut = unit_tiles(jobs, G, u, PASS);
             const JobDev &J = jobs[ut.job];
             const uint32_t n = J.n;
             const uint32_t row = ut.rb * SC_BM + row_in_tile;  // job-local
@@ -353,20 +395,25 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
             // cosine rows compare 1 - v directly (every column term is 1 when
             // the job has no zero vectors)
             const bool fast_cos = J.metric == HM_METRIC_COSINE && J.cnt->maxb[7] == 0;
-            // sorted k smallest screened values; arr[KP-1] is the running tau
-            float arr[KP];
-#pragma unroll
-            for (int q = 0; q < KP; ++q) arr[q] = (q < KP - (int)J.k) ? -INF : INF;
             const float band = valid ? G.band[gr] : 0.0f;
             const float rowterm = valid ? G.rowterm[gr] : 0.0f;
             const float scale = J.scale;
-            float thr = valid ? INF : -INF;  // invalid rows never emit
-            float tglob = INF;      // the row's shared threshold, last seen
-            float published = INF;  // this list's tau, last shared
-            uint32_t cnt = 0;
             const size_t list = list_index(J, valid ? row : 0, ut.part * 2 + half);
-            unsigned long long *cand = G.cand + J.cand0 + (list - J.slot0) * J.cap;
             const float *colterm = G.colterm + J.row0;
+            // pass 0: the k smallest mini-chunk minima seen (ascending;
+            // arr[KP-1] is the list's k-th) and the row's shared k-th
+            float arr[PASS == 0 ? KP : 1];
+#pragma unroll
+            for (int q = 0; q < (PASS == 0 ? KP : 1); ++q) arr[q] = (q < KP - (int)J.k) ? -INF : INF;
+            float tglob = INF, published = INF;
+            // pass 1: the row's fixed threshold tau1 + band
+            const float thr = (PASS == 1 && valid) ? __fadd_ru(unord32(G.rowthr[gr]), band) : -INF;
+            // cosine fast path of pass 1: every v with fl(1 - v) <= thr has
+            // v >= 1 - thr - ulp(thr)/2 >= vstar (2^-20 relative margin)
+            const float vstar = !(thr < INF) ? -INF
+                                             : __fsub_rd(__fsub_rd(1.0f, thr), fmaxf(fabsf(thr), 1.0f) * 0x1p-20f);
+            uint32_t cnt = 0;
+            unsigned long long *cand = G.cand + J.cand0 + (list - J.slot0) * J.cap;
 
             for (uint32_t ct = ut.ct_begin; ct < ut.ct_end; ++ct, ++tile) {
                 const uint32_t buf = tile & 1, use = tile >> 1;
@@ -376,84 +423,86 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                     break;
                 }
                 fence_after_sync();
-                if (valid) {  // the row's other lists may have tightened its threshold
-                    const float tg = unord32(*(volatile const uint32_t *)(G.rowthr + gr));
-                    if (tg < tglob) {
-                        tglob = tg;
-                        thr = __fadd_ru(fminf(arr[KP - 1], tglob), band);
-                    }
-                }
+                if (PASS == 0 && valid)  // the row's other lists may have tightened its k-th
+                    tglob = fminf(tglob, unord32(*(volatile const uint32_t *)(G.rowthr + gr)));
                 const uint32_t c_base = ct * SC_BN + half * (SC_BN / 2);
                 const bool diag = (ct * SC_BN < ut.rb * SC_BM + SC_BM) && (ut.rb * SC_BM < ct * SC_BN + SC_BN);
                 const uint32_t t_base = tmem_base + ((quad * 32) << 16) + buf * SC_BN + half * (SC_BN / 2);
-                // chunks of 32 columns, two accumulator register sets: the
-                // tcgen05.ld of the next chunk is in flight while this one is
-                // processed
+                // one chunk = 32 columns; the accumulator registers are
+                // overwritten in place by the screened values
                 auto process = [&](uint32_t (&v)[32], uint32_t ch) {
-                    // c overwrites the accumulator registers in place
                     float (&c)[32] = reinterpret_cast<float (&)[32]>(v);
                     const uint32_t j0 = c_base + ch * 32;  // job-local column
-                    // columns past n: never emitted
-                    const uint32_t vmask = (j0 + 32 <= n) ? 0xffffffffu
-                                           : (j0 >= n ? 0u : (0xffffffffu >> (32 - (n - j0))));
-                    if (fast_cos) {
+                    const bool full = j0 + 32 <= n;
+                    const bool self_here = diag && (row - j0 < 32u);
+                    // exact screened values of every column of the chunk
+                    // (columns past n: +inf; the row itself: 0)
+                    auto values = [&]() {
+                        if (fast_cos) {
 #pragma unroll
-                        for (int t = 0; t < 32; ++t) c[t] = __fsub_rn(1.0f, c[t]);
-                    } else {
-                        const float4 *ctp = reinterpret_cast<const float4 *>(colterm + j0);
+                            for (int t = 0; t < 32; ++t) c[t] = __fsub_rn(1.0f, c[t]);
+                        } else {
+                            const float4 *ctp = reinterpret_cast<const float4 *>(colterm + j0);
 #pragma unroll
-                        for (int q = 0; q < 8; ++q) {
-                            const float4 cq = __ldg(ctp + q);
-                            const float cs[4] = {cq.x, cq.y, cq.z, cq.w};
+                            for (int q = 0; q < 8; ++q) {
+                                const float4 cq = __ldg(ctp + q);
+                                const float cs[4] = {cq.x, cq.y, cq.z, cq.w};
 #pragma unroll
-                            for (int e = 0; e < 4; ++e)
-                                c[4 * q + e] = __fsub_rn(__fadd_rn(rowterm, cs[e]), __fmul_rn(scale, c[4 * q + e]));
-                        }
-                    }
-                    if (diag) {
-#pragma unroll
-                        for (int t = 0; t < 32; ++t)
-                            if (j0 + t == row) c[t] = 0.0f;
-                    }
-                    if (dump && valid) {
-                        for (int t = 0; t < 32; ++t)
-                            if (j0 + t < n) dump[(size_t)row * n + j0 + t] = c[t];
-                    }
-                    // columns within the threshold: one predicate word per
-                    // column (set.leu keeps a NaN), OR-reduced as a tree
-                    uint32_t pw[32];
-#pragma unroll
-                    for (int t = 0; t < 32; ++t) {
-                        uint32_t m;
-                        asm("set.leu.u32.f32 %0, %1, %2;" : "=r"(m) : "f"(c[t]), "f"(thr));
-                        pw[t] = m & (1u << t);
-                    }
-#pragma unroll
-                    for (int w = 16; w > 0; w >>= 1)
-#pragma unroll
-                        for (int t = 0; t < w; ++t) pw[t] |= pw[t + w];
-                    uint32_t pm = valid ? (pw[0] & vmask) : 0u;
-                    if (pm) {
-                        // emit each passing column and insert it into the
-                        // running k smallest when it improves them
-                        float cl[32];
-#pragma unroll
-                        for (int t = 0; t < 32; ++t) cl[t] = c[t];
-                        bool improved = false;
-                        while (pm) {
-                            const int t = __ffs(pm) - 1;
-                            pm &= pm - 1;
-                            const float x = cl[t];
-                            if (cnt < J.cap) cand[cnt] = ((unsigned long long)__float_as_uint(x) << 32) | (j0 + t);
-                            ++cnt;
-                            if (x < arr[KP - 1]) {
-#pragma unroll
-                                for (int q = KP - 1; q > 0; --q) arr[q] = fminf(arr[q], fmaxf(arr[q - 1], x));
-                                arr[0] = fminf(arr[0], x);
-                                improved = true;
+                                for (int e = 0; e < 4; ++e)
+                                    c[4 * q + e] =
+                                        __fsub_rn(__fadd_rn(rowterm, cs[e]), __fmul_rn(scale, c[4 * q + e]));
                             }
                         }
-                        if (improved) {
+                        if (!full) {
+#pragma unroll
+                            for (int t = 0; t < 32; ++t)
+                                if (j0 + t >= n) c[t] = INF;
+                        }
+                        if (self_here) {
+#pragma unroll
+                            for (int t = 0; t < 32; ++t)
+                                if (j0 + t == row) c[t] = 0.0f;
+                        }
+                    };
+                    // cosine fast path: c = 1 - v is monotone in v, so a
+                    // minimum of c is 1 - (the maximum of v), bit for bit
+                    const bool quick = fast_cos && full && !self_here && (PASS == 1 || !dump);
+                    if (PASS == 0) {
+                        // mini-chunk minima: columns {t, t+8, t+16, t+24}
+                        float m[8];
+                        if (quick) {
+#pragma unroll
+                            for (int t = 0; t < 8; ++t)
+                                m[t] = __fsub_rn(1.0f, fmaxf(fmaxf(c[t], c[t + 8]), fmaxf(c[t + 16], c[t + 24])));
+                        } else {
+                            values();
+                            if (dump && valid) {
+                                for (int t = 0; t < 32; ++t)
+                                    if (j0 + t < n) dump[(size_t)row * n + j0 + t] = c[t];
+                            }
+#pragma unroll
+                            for (int t = 0; t < 8; ++t)
+                                m[t] = fminf(fminf(c[t], c[t + 8]), fminf(c[t + 16], c[t + 24]));
+                        }
+                        // minima that can be among the row's k smallest
+                        uint32_t pm = 0;
+#pragma unroll
+                        for (int t = 0; t < 8; ++t)
+                            pm |= (m[t] < arr[KP - 1] && !(m[t] > tglob)) ? (1u << t) : 0u;
+                        if (!valid) pm = 0;
+                        if (pm) {
+                            while (pm) {
+                                const int t = __ffs(pm) - 1;
+                                pm &= pm - 1;
+                                float x = m[0];
+#pragma unroll
+                                for (int q = 1; q < 8; ++q) x = (t == q) ? m[q] : x;
+                                if (x < arr[KP - 1]) {
+#pragma unroll
+                                    for (int q = KP - 1; q > 0; --q) arr[q] = fminf(arr[q], fmaxf(arr[q - 1], x));
+                                    arr[0] = fminf(arr[0], x);
+                                }
+                            }
                             const float tl = arr[KP - 1];
                             if (tl < published) {  // share with the row's other lists
                                 const uint32_t o = ord32(tl);
@@ -461,7 +510,70 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                                 tglob = fminf(tglob, unord32(prev < o ? prev : o));
                                 published = tl;
                             }
-                            thr = __fadd_ru(fminf(tl, tglob), band);
+                        }
+                    } else {
+                        // emission: 8-column groups gate the per-column work,
+                        // which is divergent (the warp's lanes are 32 rows)
+                        auto emit_group = [&](uint32_t pm, int g, bool raw) {
+                            while (pm) {
+                                const int e = __ffs(pm) - 1;
+                                pm &= pm - 1;
+                                const float a0 = (e & 1) ? c[8 * g + 1] : c[8 * g];
+                                const float a1 = (e & 1) ? c[8 * g + 3] : c[8 * g + 2];
+                                const float a2 = (e & 1) ? c[8 * g + 5] : c[8 * g + 4];
+                                const float a3 = (e & 1) ? c[8 * g + 7] : c[8 * g + 6];
+                                const float b0 = (e & 2) ? a1 : a0, b1 = (e & 2) ? a3 : a2;
+                                float x = (e & 4) ? b1 : b0;
+                                if (raw) x = __fsub_rn(1.0f, x);
+                                if (cnt < J.cap)
+                                    cand[cnt] = ((unsigned long long)__float_as_uint(x) << 32) | (j0 + 8 * g + e);
+                                ++cnt;
+                            }
+                        };
+                        if (quick) {
+                            // c = 1 - v <= thr  <=>  v >= vstar (vstar a hair low:
+                            // a superset, the rerank filters exactly)
+                            float gm[4];
+#pragma unroll
+                            for (int g = 0; g < 4; ++g) {
+                                float x = c[8 * g];
+#pragma unroll
+                                for (int e = 1; e < 8; ++e) x = fmaxf(x, c[8 * g + e]);
+                                gm[g] = x;
+                            }
+                            if (valid && fmaxf(fmaxf(gm[0], gm[1]), fmaxf(gm[2], gm[3])) >= vstar) {
+#pragma unroll
+                                for (int g = 0; g < 4; ++g) {
+                                    if (gm[g] >= vstar) {
+                                        uint32_t pm = 0;
+#pragma unroll
+                                        for (int e = 0; e < 8; ++e) pm |= (c[8 * g + e] >= vstar) ? (1u << e) : 0u;
+                                        emit_group(pm, g, true);
+                                    }
+                                }
+                            }
+                        } else {
+                            values();
+                            float gm[4];
+#pragma unroll
+                            for (int g = 0; g < 4; ++g) {
+                                float x = c[8 * g];
+#pragma unroll
+                                for (int e = 1; e < 8; ++e) x = fminf(x, c[8 * g + e]);
+                                gm[g] = x;
+                            }
+                            if (valid && !(fminf(fminf(gm[0], gm[1]), fminf(gm[2], gm[3])) > thr)) {
+#pragma unroll
+                                for (int g = 0; g < 4; ++g) {
+                                    if (!(gm[g] > thr)) {
+                                        uint32_t pm = 0;
+#pragma unroll
+                                        for (int e = 0; e < 8; ++e)
+                                            pm |= (!(c[8 * g + e] > thr) && j0 + 8 * g + e < n) ? (1u << e) : 0u;
+                                        emit_group(pm, g, false);
+                                    }
+                                }
+                            }
                         }
                     }
                 };
@@ -482,14 +594,16 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                 if (lane == 0) mbar_arrive(smem_u32(&acce[buf]));
             }
             if (valid) {
-                // the list's k smallest screened values (ascending; the row's
-                // global k smallest are all among the union of these)
-                G.cand_cnt[list] = cnt;
-                float *kk = G.topk + J.topk0 + (list - J.slot0) * J.k;
+                if (PASS == 0) {
+                    // the list's k smallest mini-chunk minima (ascending)
+                    float *kk = G.topk + J.topk0 + (list - J.slot0) * J.k;
 #pragma unroll
-                for (int q = 0; q < KP; ++q)
-                    if (q >= KP - (int)J.k) kk[q - (KP - (int)J.k)] = arr[q];
-                atomicAdd(&J.cnt->emitted, (unsigned long long)cnt);
+                    for (int q = 0; q < KP; ++q)
+                        if (q >= KP - (int)J.k) kk[q - (KP - (int)J.k)] = arr[q];
+                } else {
+                    G.cand_cnt[list] = cnt;
+                    atomicAdd(&J.cnt->emitted, (unsigned long long)cnt);
+                }
             }
         }
     }
@@ -503,13 +617,16 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
     }
 }
 
-template <int KIND, int KP>
+template <int KIND, int KP, int PASS>
 static int launch_kind(const JobDev *jobs, const GroupDev &G, const CUtensorMap &ta,
                        const CUtensorMap &tb, float *dump, uint32_t idesc, cudaStream_t s) {
-    HM_TRY(ensure_dynamic_smem((const void *)screen_gemm_kernel<KIND, KP>, (int)SC_SMEM_BYTES));
+    HM_TRY(ensure_dynamic_smem((const void *)screen_gemm_kernel<KIND, KP, PASS>, (int)SC_SMEM_BYTES));
     const uint32_t sms = (uint32_t)device_sm_count();
     const uint32_t grid = G.units < sms ? G.units : sms;
-    screen_gemm_kernel<KIND, KP><<<grid, SC_THREADS, SC_SMEM_BYTES, s>>>(ta, tb, jobs, G, dump, idesc);
+    // every job's K slices fit the resident A block
+    const uint32_t a_res = (G.kpmax / G.kslice) <= SC_ARES_STAGES ? 1u : 0u;
+    screen_gemm_kernel<KIND, KP, PASS><<<grid, SC_THREADS, SC_SMEM_BYTES, s>>>(ta, tb, jobs, G, dump, idesc,
+                                                                               a_res);
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();
     return HM_OK;
@@ -523,19 +640,26 @@ static uint32_t make_idesc(int kind) {
            | ((uint32_t)(SC_BN >> 3) << 17) | ((uint32_t)(SC_BM >> 4) << 24);
 }
 
+template <int KIND>
+static int launch_pass(const JobDev *jobs, const GroupDev &G, uint32_t kp, const CUtensorMap &ta,
+                       const CUtensorMap &tb, float *dump, uint32_t idesc, int pass, cudaStream_t s) {
+    if (pass == 1) return launch_kind<KIND, 32, 1>(jobs, G, ta, tb, nullptr, idesc, s);
+    if (kp == 32) return launch_kind<KIND, 32, 0>(jobs, G, ta, tb, dump, idesc, s);
+    if (kp == 64) return launch_kind<KIND, 64, 0>(jobs, G, ta, tb, dump, idesc, s);
+    return set_error(HM_ERR_UNSUPPORTED, "screen top-k width %u", kp);
+}
+
+// pass 0: running k smallest mini-chunk minima per list (-> tau1 per row);
+// pass 1: emission of every column within tau1 + band
 int launch_screen_gemm(const JobDev *jobs, const GroupDev &G, const GroupDev *, uint32_t kp,
-                       const CUtensorMap &ta, const CUtensorMap &tb, float *dump, cudaStream_t s) {
+                       const CUtensorMap &ta, const CUtensorMap &tb, float *dump, int pass,
+                       cudaStream_t s) {
     if (G.units == 0) return HM_OK;
     ScopedKernelTimer timer(HM_KCLASS_BULK, s);
     const uint32_t idesc = make_idesc((int)G.kind);
-    if (G.kind == SCREEN_KIND_BF16) {
-        if (kp == 32) return launch_kind<SCREEN_KIND_BF16, 32>(jobs, G, ta, tb, dump, idesc, s);
-        if (kp == 64) return launch_kind<SCREEN_KIND_BF16, 64>(jobs, G, ta, tb, dump, idesc, s);
-    } else {
-        if (kp == 32) return launch_kind<SCREEN_KIND_TF32, 32>(jobs, G, ta, tb, dump, idesc, s);
-        if (kp == 64) return launch_kind<SCREEN_KIND_TF32, 64>(jobs, G, ta, tb, dump, idesc, s);
-    }
-    return set_error(HM_ERR_UNSUPPORTED, "screen top-k width %u", kp);
+    if (G.kind == SCREEN_KIND_BF16)
+        return launch_pass<SCREEN_KIND_BF16>(jobs, G, kp, ta, tb, dump, idesc, pass, s);
+    return launch_pass<SCREEN_KIND_TF32>(jobs, G, kp, ta, tb, dump, idesc, pass, s);
 }
 
 }  // namespace hm

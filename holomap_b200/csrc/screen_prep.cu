@@ -110,7 +110,17 @@ __global__ void __launch_bounds__(256) operand_kernel(const JobDev *__restrict__
     if (gr >= G.rows) return;
     const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
     const uint32_t row = gr - J.row0;
-    if (row >= J.n) return;  // padding between jobs (never read as a valid row)
+    if (row >= J.n) {  // padding between jobs: zero operands (read only as masked rows/columns)
+        for (uint32_t t = lane; t < G.kpmax; t += 32) {
+            if (G.elem_bytes == 4) {
+                reinterpret_cast<uint32_t *>(G.opa)[(size_t)gr * G.kpmax + t] = 0u;
+            } else {
+                reinterpret_cast<uint16_t *>(G.opa)[(size_t)gr * G.kpmax + t] = 0;
+                reinterpret_cast<uint16_t *>(G.opb)[(size_t)gr * G.kpmax + t] = 0;
+            }
+        }
+        return;
+    }
     unsigned long long *maxb = J.cnt->maxb;
 
     double scale = 1.0;
