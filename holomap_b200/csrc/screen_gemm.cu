@@ -406,6 +406,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
 #pragma unroll
             for (int q = 0; q < (PASS == 0 ? KP : 1); ++q) arr[q] = (q < KP - (int)J.k) ? -INF : INF;
             float tglob = INF, published = INF;
+            const bool chunk_min = J.seed_tiles < J.part_tiles;
             // pass 1: the row's fixed threshold tau1 + band
             const float thr = (PASS == 1 && valid) ? __fadd_ru(unord32(G.rowthr[gr]), band) : -INF;
             // cosine fast path of pass 1: every v with fl(1 - v) <= thr has
@@ -484,11 +485,18 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                             for (int t = 0; t < 8; ++t)
                                 m[t] = fminf(fminf(c[t], c[t + 8]), fminf(c[t + 16], c[t + 24]));
                         }
+                        // a sampled threshold pass keeps one minimum per 32-column
+                        // chunk (an eighth of the insertions; the sample's k smallest
+                        // rarely share a chunk), a full one the eight mini-chunk minima
+                        if (chunk_min) {
+#pragma unroll
+                            for (int t = 1; t < 8; ++t) m[0] = fminf(m[0], m[t]);
+                        }
                         // minima that can be among the row's k smallest
                         uint32_t pm = 0;
 #pragma unroll
                         for (int t = 0; t < 8; ++t)
-                            pm |= (m[t] < arr[KP - 1] && !(m[t] > tglob)) ? (1u << t) : 0u;
+                            pm |= (m[t] < arr[KP - 1] && !(m[t] > tglob) && (t == 0 || !chunk_min)) ? (1u << t) : 0u;
                         if (!valid) pm = 0;
                         if (pm) {
                             while (pm) {
