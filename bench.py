@@ -63,6 +63,8 @@ def parse_args():
     ap.add_argument("--batch-jobs", type=int, default=32, help="serving: requests per batch")
     ap.add_argument("--batch-work", type=float, default=4e11,
                     help="serving: a batch closes once its sum of n*n*d passes this")
+    ap.add_argument("--small-work", type=float, default=2e10,
+                    help="serving: requests with n*n*d at or below this run on high-priority streams")
     ap.add_argument("--rate-fracs", type=float, nargs="*", default=[0.5, 0.8, 1.0],
                     help="serving: open-loop arrival rates as fractions of saturation")
     ap.add_argument("--serial-seconds", type=float, default=20.0,
@@ -641,7 +643,7 @@ def serve_main(args) -> int:
         return lat, time.perf_counter() - t0
 
     srv = Server(max_inflight=args.inflight, max_batch_jobs=args.batch_jobs,
-                 max_batch_work=args.batch_work)
+                 max_batch_work=args.batch_work, small_work=args.small_work)
     # warm-up: the first requests once
     saved = reqs
     reqs = saved[: min(64, count)]
@@ -708,7 +710,7 @@ def serve_main(args) -> int:
                        "client": f"closed loop, {window} requests outstanding (saturation); "
                                  "open-loop Poisson arrivals for latency",
                        "max_inflight": args.inflight, "max_batch_jobs": args.batch_jobs,
-                       "max_batch_work": args.batch_work,
+                       "max_batch_work": args.batch_work, "small_work": args.small_work,
                        "l2": "every request copies its points in from host memory",
                        "parallelism": "replicas"},
             "path": "auto",

@@ -130,13 +130,16 @@ class HmJob(ctypes.Structure):
 
 class HmCtxConfig(ctypes.Structure):
     """``hm_ctx_config``: device arena bytes, batches in flight, requests per
-    batch, and the batch's work cap (sum of n*n*d); zeros take the defaults."""
+    batch, the batch's work cap (sum of n*n*d) and the small-request cut
+    (n*n*d) below which requests run on high-priority streams; zeros take the
+    defaults."""
 
     _fields_ = [
         ("memory_bytes", ctypes.c_uint64),
         ("max_inflight", ctypes.c_uint32),
         ("max_batch_jobs", ctypes.c_uint32),
         ("max_batch_work", ctypes.c_double),
+        ("small_work", ctypes.c_double),
     ]
 
 

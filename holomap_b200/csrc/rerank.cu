@@ -36,10 +36,11 @@ __device__ __forceinline__ double step(double acc, double x, double y) {
 
 constexpr int RR_WARPS = 8;
 constexpr int RR_LIST = 256;  // compacted candidates per warp between flushes
+constexpr int RR_CBUF = 256;  // emitted candidates a warp stages in shared memory
 
 // One warp per group row; candidates are evaluated 32 at a time, one per lane.
 template <int METRIC, int KPL>
-__global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const JobDev *__restrict__ jobs,
+__global__ void __launch_bounds__(RR_WARPS * 32, 3) rerank_kernel(const JobDev *__restrict__ jobs,
                                                                const GroupDev *__restrict__ Gp,
                                                                uint32_t dstride) {
     extern __shared__ double rr_smem[];
@@ -55,6 +56,9 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const JobDev *__r
     const size_t l0 = list_index(J, row, 0);
     double *xi = rr_smem + (size_t)warp * dstride;
     uint32_t *list = reinterpret_cast<uint32_t *>(rr_smem + (size_t)RR_WARPS * dstride) + warp * RR_LIST;
+    unsigned long long *cbuf = reinterpret_cast<unsigned long long *>(
+                                   reinterpret_cast<uint32_t *>(rr_smem + (size_t)RR_WARPS * dstride) +
+                                   RR_WARPS * RR_LIST) + warp * RR_CBUF;
 
     // overflow / unbounded rows go to the exact plain path
     bool ovf = G.force[gr] != 0;
@@ -67,22 +71,57 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const JobDev *__r
         return;
     }
     // Threshold: the exact k-th smallest screened value of the row, over the
-    // emitted candidates (they include the row's k smallest).
-    WarpTopK<KPL> sel;
-    sel.reset();
-    for (uint32_t p = 0; p < lists; ++p) {
-        const uint32_t cnt = G.cand_cnt[l0 + p];
-        const unsigned long long *cand = G.cand + J.cand0 + (l0 + p - J.slot0) * J.cap;
-        for (uint32_t e0 = 0; e0 < cnt; e0 += 32) {
-            uint64_t key = KEY_NONE;
-            if (e0 + lane < cnt) {
-                const unsigned long long c = cand[e0 + lane];
-                key = ((uint64_t)ord32(__uint_as_float((uint32_t)(c >> 32))) << 32) | (uint32_t)c;
-            }
-            sel.offer(key, k, lane);
+    // emitted candidates (they include the row's k smallest).  Up to RR_CBUF
+    // candidates are staged in shared memory and the k-th found by a bitwise
+    // search on the order-preserving keys; longer rows use a warp top-k.
+    uint32_t total = 0;
+    for (uint32_t p = 0; p < lists; ++p) total += G.cand_cnt[l0 + p];
+    const bool staged = total <= RR_CBUF;
+    float tau = __int_as_float(0x7f800000);
+    if (staged) {
+        uint32_t base = 0;
+        for (uint32_t p = 0; p < lists; ++p) {
+            const uint32_t cnt = G.cand_cnt[l0 + p];
+            const unsigned long long *cand = G.cand + J.cand0 + (l0 + p - J.slot0) * J.cap;
+            for (uint32_t e = lane; e < cnt; e += 32) cbuf[base + e] = cand[e];
+            base += cnt;
         }
+        __syncwarp();
+        uint32_t ov[RR_CBUF / 32];
+#pragma unroll
+        for (int q = 0; q < RR_CBUF / 32; ++q) {
+            const uint32_t e = q * 32 + lane;
+            ov[q] = e < total ? ord32(__uint_as_float((uint32_t)(cbuf[e] >> 32))) : 0xffffffffu;
+        }
+        if (total >= k) {
+            uint32_t r = 0;  // largest key with fewer than k keys below it = the k-th
+            for (int b = 31; b >= 0; --b) {
+                const uint32_t t = r | (1u << b);
+                uint32_t c = 0;
+#pragma unroll
+                for (int q = 0; q < RR_CBUF / 32; ++q) c += ov[q] < t ? 1u : 0u;
+                c = __reduce_add_sync(0xffffffffu, c);
+                if (c < k) r = t;
+            }
+            tau = unord32(r);
+        }
+    } else {
+        WarpTopK<KPL> sel;
+        sel.reset();
+        for (uint32_t p = 0; p < lists; ++p) {
+            const uint32_t cnt = G.cand_cnt[l0 + p];
+            const unsigned long long *cand = G.cand + J.cand0 + (l0 + p - J.slot0) * J.cap;
+            for (uint32_t e0 = 0; e0 < cnt; e0 += 32) {
+                uint64_t key = KEY_NONE;
+                if (e0 + lane < cnt) {
+                    const unsigned long long c = cand[e0 + lane];
+                    key = ((uint64_t)ord32(__uint_as_float((uint32_t)(c >> 32))) << 32) | (uint32_t)c;
+                }
+                sel.offer(key, k, lane);
+            }
+        }
+        if (sel.tau != KEY_NONE) tau = unord32((uint32_t)(sel.tau >> 32));
     }
-    const float tau = sel.tau == KEY_NONE ? __int_as_float(0x7f800000) : unord32((uint32_t)(sel.tau >> 32));
     const float thr = __fadd_ru(tau, G.band[gr]);
 
     for (uint32_t t = lane; t < d; t += 32) xi[t] = (double)J.x[(size_t)row * d + t];
@@ -138,14 +177,14 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const JobDev *__r
         __syncwarp();
     };
 
-    for (uint32_t p = 0; p < lists; ++p) {
-        const uint32_t cnt = G.cand_cnt[l0 + p];
-        const unsigned long long *cand = G.cand + J.cand0 + (l0 + p - J.slot0) * J.cap;
+    // compaction of the candidates within tau + band, from the staged copy or
+    // from the lists
+    auto compact = [&](const unsigned long long *src, uint32_t cnt) {
         for (uint32_t e0 = 0; e0 < cnt; e0 += 32) {
             bool pass = false;
             uint32_t j = 0;
             if (e0 + lane < cnt) {
-                const unsigned long long c = cand[e0 + lane];
+                const unsigned long long c = src[e0 + lane];
                 const float cv = __uint_as_float((uint32_t)(c >> 32));
                 j = (uint32_t)c;
                 pass = !(cv > thr);
@@ -160,6 +199,12 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const JobDev *__r
                 fill = 0;
             }
         }
+    };
+    if (staged) {
+        compact(cbuf, total);
+    } else {
+        for (uint32_t p = 0; p < lists; ++p)
+            compact(G.cand + J.cand0 + (l0 + p - J.slot0) * J.cap, G.cand_cnt[l0 + p]);
     }
     flush(fill);
 
@@ -224,7 +269,8 @@ template <int METRIC>
 static int launch_metric(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t kpl,
                          uint32_t dmax, cudaStream_t s) {
     const uint32_t dstride = (uint32_t)round_up(dmax, 4);
-    const size_t smem = (size_t)RR_WARPS * dstride * sizeof(double) + RR_WARPS * RR_LIST * sizeof(uint32_t);
+    const size_t smem = (size_t)RR_WARPS * dstride * sizeof(double) + RR_WARPS * RR_LIST * sizeof(uint32_t) +
+                        (size_t)RR_WARPS * RR_CBUF * sizeof(unsigned long long);
     const int blocks = (int)((G.rows + RR_WARPS - 1) / RR_WARPS);
 #define HM_RR_CASE(K)                                                                       \
     case K: {                                                                               \

@@ -4,9 +4,10 @@
 // A context owns one device arena.  hm_submit validates a request, sizes its
 // footprint (points + outputs + the pipeline scratch hm_workspace_bytes
 // plans for it) and queues it.  A scheduler thread forms batches: whenever a
-// batch slot (a stream) is free it takes queued requests in arrival order
-// while their footprints fit the arena's largest free block and the batch's
-// work cap, reserves one block for them, and enqueues on the slot's stream
+// batch slot (a stream) is free it takes queued requests of one size class in
+// arrival order while their footprints fit the arena's largest free block and
+// the batch's work cap (small requests go to high-priority streams and never
+// wait behind a large request's batch), reserves one block for them, and enqueues on the slot's stream
 // the copies in, the whole pipeline (hm_batch_bind + hm_batch_run), the copies
 // out and a host callback.  The callback only marks the slot finished; the
 // scheduler then reads each request's counters (copied with the results),
@@ -86,6 +87,7 @@ struct Request {
     size_t io_bytes = 0;     // device copies of points and outputs
     size_t ws_bytes = 0;     // pipeline scratch of the request alone
     double work = 0;         // n * n * d
+    bool small = true;       // work <= small_work: high-priority batches
     double submit_ms = 0, admit_ms = 0, done_ms = 0;
     int status = HM_ERR_NOT_READY;
     std::string message;
@@ -101,6 +103,7 @@ struct Slot {
     hm_ctx *ctx = nullptr;
     cudaStream_t stream = nullptr;
     JobCounters *counters = nullptr;  // page-locked, max_batch_jobs entries
+    bool high = false;                // high-priority stream: small requests
     bool busy = false, done = false;
     double done_ms = 0;
     hm_batch *batch = nullptr;
@@ -245,38 +248,62 @@ static int launch(hm_ctx *C, Slot &s, std::vector<Request *> &take, size_t off, 
 // Form and enqueue at most one batch.  Called with the lock held; drops it
 // around the CUDA calls.  Returns true when a batch was launched.
 static bool try_launch(hm_ctx *C, std::unique_lock<std::mutex> &lk) {
-    Slot *slot = nullptr;
-    for (Slot &s : C->slots)
-        if (!s.busy) {
-            slot = &s;
-            break;
-        }
-    if (!slot || C->pending.empty()) return false;
-    const size_t avail = C->arena.largest();
-    std::vector<uint64_t> tickets;
-    std::vector<Request *> take;
-    size_t need = 0;
-    double work = 0;
-    while (!C->pending.empty()) {
-        const uint64_t t = C->pending.front();
-        Request &r = C->reqs[t];
+    // a free high-priority slot serves small requests; a free low-priority
+    // one large requests first, then small ones
+    Slot *slot_hi = nullptr, *slot_lo = nullptr;
+    for (Slot &s : C->slots) {
+        if (s.busy) continue;
+        if (s.high && !slot_hi) slot_hi = &s;
+        if (!s.high && !slot_lo) slot_lo = &s;
+    }
+    if (C->pending.empty() || (!slot_hi && !slot_lo)) return false;
+    bool any_small = false, any_large = false;
+    for (auto it = C->pending.begin(); it != C->pending.end();) {
+        Request &r = C->reqs.at(*it);
         if (r.footprint() > C->arena.capacity) {
-            C->pending.pop_front();
             char msg[160];
             snprintf(msg, sizeof msg, "request needs %zu bytes of device memory; the context holds %zu",
                      r.footprint(), C->arena.capacity);
             finish(C, r, HM_ERR_ADMISSION, msg, C->now_ms());
             C->cv_done.notify_all();
+            it = C->pending.erase(it);
+            continue;
+        }
+        (r.small ? any_small : any_large) = true;
+        ++it;
+    }
+    Slot *slot = nullptr;
+    bool want_small = true;
+    if (slot_hi && any_small) {
+        slot = slot_hi;
+    } else if (slot_lo && any_large) {
+        slot = slot_lo;
+        want_small = false;
+    } else if (slot_lo && any_small) {
+        slot = slot_lo;
+    } else {
+        return false;
+    }
+    // requests of that class in arrival order, while they fit
+    const size_t avail = C->arena.largest();
+    std::vector<uint64_t> tickets;
+    std::vector<Request *> take;
+    size_t need = 0;
+    double work = 0;
+    for (auto it = C->pending.begin(); it != C->pending.end();) {
+        Request &r = C->reqs.at(*it);
+        if (r.small != want_small) {
+            ++it;
             continue;
         }
         if (!take.empty() && (take.size() >= C->cfg.max_batch_jobs || work + r.work > C->cfg.max_batch_work))
             break;
-        if (need + r.footprint() > avail) break;  // arrival order: later requests wait too
-        C->pending.pop_front();
+        if (need + r.footprint() > avail) break;  // arrival order: later requests of the class wait too
         take.push_back(&r);
-        tickets.push_back(t);
+        tickets.push_back(*it);
         need += r.footprint();
         work += r.work;
+        it = C->pending.erase(it);
     }
     if (take.empty()) return false;
     size_t off = 0;
@@ -378,6 +405,7 @@ int hm_ctx_create(const hm_ctx_config *config, hm_ctx **out) {
     if (cfg.max_inflight == 0) cfg.max_inflight = 4;
     if (cfg.max_batch_jobs == 0) cfg.max_batch_jobs = 64;
     if (cfg.max_batch_work <= 0) cfg.max_batch_work = 4e11;
+    if (cfg.small_work <= 0) cfg.small_work = 2e10;
     if (cfg.max_inflight > 64) return set_error(HM_ERR_INVALID, "max_inflight above 64");
     int dev = 0;
     HM_CUDA_TRY(cudaGetDevice(&dev));
@@ -400,9 +428,13 @@ int hm_ctx_create(const hm_ctx_config *config, hm_ctx **out) {
     C->arena.init(C->arena_mem, cfg.memory_bytes);
     C->totals.arena_bytes = cfg.memory_bytes;
     C->slots.resize(cfg.max_inflight);
-    for (Slot &s : C->slots) {
+    int prio_lo = 0, prio_hi = 0;
+    e = cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi);
+    for (size_t i = 0; e == cudaSuccess && i < C->slots.size(); ++i) {
+        Slot &s = C->slots[i];
         s.ctx = C;
-        e = cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking);
+        s.high = cfg.max_inflight > 1 && i < (cfg.max_inflight + 1) / 2;  // at least one low slot
+        e = cudaStreamCreateWithPriority(&s.stream, cudaStreamNonBlocking, s.high ? prio_hi : prio_lo);
         if (e == cudaSuccess)
             e = cudaMallocHost(reinterpret_cast<void **>(&s.counters), cfg.max_batch_jobs * sizeof(JobCounters));
         if (e != cudaSuccess) break;
@@ -452,6 +484,7 @@ int hm_submit(hm_ctx *C, const hm_job *r, uint64_t *ticket) {
     q.io_bytes = io_bytes_of(*r);
     q.ws_bytes = ws;
     q.work = (double)r->n * (double)r->n * (double)r->d;
+    q.small = q.work <= C->cfg.small_work;
     {
         std::lock_guard<std::mutex> lk(C->mu);
         if (C->stop) return set_error(HM_ERR_INVALID, "context is shutting down");

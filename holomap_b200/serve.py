@@ -53,8 +53,8 @@ class Server:
     """One serving context on the current CUDA device."""
 
     def __init__(self, memory_bytes: int = 0, max_inflight: int = 0, max_batch_jobs: int = 0,
-                 max_batch_work: float = 0.0, pinned: bool = True):
-        cfg = HmCtxConfig(memory_bytes, max_inflight, max_batch_jobs, max_batch_work)
+                 max_batch_work: float = 0.0, small_work: float = 0.0, pinned: bool = True):
+        cfg = HmCtxConfig(memory_bytes, max_inflight, max_batch_jobs, max_batch_work, small_work)
         self._ctx = ctypes.c_void_p()
         check(lib().hm_ctx_create(ctypes.byref(cfg), ctypes.byref(self._ctx)))
         self.pinned = pinned

@@ -214,6 +214,8 @@ typedef struct hm_ctx_config {
     uint32_t max_inflight;   /* batches on the device at once; 0 = 4 */
     uint32_t max_batch_jobs; /* requests per batch; 0 = 64 */
     double max_batch_work;   /* a batch closes once its sum of n*n*d passes this; 0 = 4e11 */
+    double small_work;       /* requests with n*n*d at or below this are batched apart and run
+                                on high-priority streams; 0 = 2e10 */
 } hm_ctx_config;
 
 /* What a finished (or pending) request reports. */
