@@ -236,10 +236,32 @@ __global__ void __launch_bounds__(256) threshold_kernel(const JobDev *__restrict
     if (row < J.q0 || row >= J.q1) return;
     const uint32_t k = J.k, lists = 2 * J.parts;
     const size_t l0 = list_index(J, row, 0);
+    // the row's lists' arrays are contiguous: lists x k values
+    const float *base = G.topk + J.topk0 + (l0 - J.slot0) * k;
+    const uint32_t total = lists * k;
+    if (total <= 256) {
+        uint32_t ov[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const uint32_t e = q * 32 + lane;
+            ov[q] = e < total ? ord32(base[e]) : 0xffffffffu;
+        }
+        uint32_t r = 0;  // largest key with fewer than k keys below it = the k-th
+        for (int b = 31; b >= 0; --b) {
+            const uint32_t t = r | (1u << b);
+            uint32_t c = 0;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) c += ov[q] < t ? 1u : 0u;
+            c = __reduce_add_sync(0xffffffffu, c);
+            if (c < k) r = t;
+        }
+        if (lane == 0) G.rowthr[gr] = r;
+        return;
+    }
     WarpTopK<KPL> sel;
     sel.reset();
     for (uint32_t p = 0; p < lists; ++p) {
-        const float *kk = G.topk + J.topk0 + (l0 + p - J.slot0) * k;
+        const float *kk = base + p * k;
         for (uint32_t e0 = 0; e0 < k; e0 += 32) {
             const uint64_t key = (e0 + lane < k) ? (((uint64_t)ord32(kk[e0 + lane]) << 32) | (p * k + e0 + lane))
                                                  : KEY_NONE;

@@ -59,22 +59,32 @@ __global__ void colmean_kernel(const JobDev *__restrict__ jobs, const GroupDev *
 }
 
 // Largest ||x_i - mu||^2 of each euclidean job, for its power-of-two scale.
-__global__ void centred_norm_max_kernel(const JobDev *__restrict__ jobs, const GroupDev *__restrict__ G) {
-    const int lane = threadIdx.x & 31;
-    const uint32_t gr = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (gr >= G->rows) return;
-    const uint32_t g = find_job(G->row_starts, G->njobs, gr);
-    const JobDev &J = jobs[G->job_ids[g]];
-    if (J.metric != HM_METRIC_EUCLIDEAN) return;
-    const uint32_t row = gr - J.row0;
-    if (row >= J.n) return;  // padding between jobs
-    double s = 0.0;
-    for (uint32_t t = lane; t < J.d; t += 32) {
-        const double v = (double)J.x[(size_t)row * J.d + t] - J.mu[t];
-        s += v * v;
+// A block covers 32 group rows (one job: a job's rows start 32-aligned), a
+// warp 4 of them; one atomic per block.
+__global__ void __launch_bounds__(256) centred_norm_max_kernel(const JobDev *__restrict__ jobs,
+                                                              const GroupDev *__restrict__ G) {
+    __shared__ double s_max[8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t gr0 = blockIdx.x * 32;
+    const JobDev &J = jobs[G->job_ids[find_job(G->row_starts, G->njobs, gr0)]];
+    if (J.metric != HM_METRIC_EUCLIDEAN) return;  // uniform over the block
+    double m = 0.0;
+    for (uint32_t r = 0; r < 4; ++r) {
+        const uint32_t row = gr0 + warp * 4 + r - J.row0;
+        if (row >= J.n) break;  // padding between jobs
+        double s = 0.0;
+        for (uint32_t t = lane; t < J.d; t += 32) {
+            const double v = (double)J.x[(size_t)row * J.d + t] - J.mu[t];
+            s += v * v;
+        }
+        m = fmax(m, warp_sum(s));
     }
-    s = warp_sum(s);
-    if (lane == 0) atomic_max_pos(&J.cnt->maxb[6], s);
+    if (lane == 0) s_max[warp] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < 8; ++w) m = fmax(m, s_max[w]);
+        atomic_max_pos(&J.cnt->maxb[6], m);
+    }
 }
 
 __device__ __forceinline__ uint16_t to_bf16_bits(double v, double *rounded) {
@@ -100,114 +110,136 @@ __device__ __forceinline__ uint32_t to_tf32_bits(double v, double *rounded) {
     return b;
 }
 
-// One warp per group row: operand row(s), binary64 error statistics,
-// additive terms of the screen epilogue, and the row's shared threshold.
+// Operand row(s), binary64 error statistics, additive terms of the screen
+// epilogue, and the row's shared threshold.  A block covers 32 group rows of
+// one job (a job's rows start 32-aligned), a warp 4 of them; the job's maxima
+// take one atomic per block.
 __global__ void __launch_bounds__(256) operand_kernel(const JobDev *__restrict__ jobs,
                                                      const GroupDev *__restrict__ Gp) {
+    __shared__ double s_max[8][6];
+    __shared__ unsigned long long s_zero[8];
     const GroupDev &G = *Gp;
-    const int lane = threadIdx.x & 31;
-    const uint32_t gr = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (gr >= G.rows) return;
-    const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
-    const uint32_t row = gr - J.row0;
-    if (row >= J.n) {  // padding between jobs: zero operands (read only as masked rows/columns)
-        for (uint32_t t = lane; t < G.kpmax; t += 32) {
-            if (G.elem_bytes == 4) {
-                reinterpret_cast<uint32_t *>(G.opa)[(size_t)gr * G.kpmax + t] = 0u;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t gr0 = blockIdx.x * 32;
+    const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr0)]];
+    unsigned long long *maxb = J.cnt->maxb;
+    double wmax[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    unsigned long long wzero = 0;
+    for (uint32_t wr = 0; wr < 4; ++wr) {
+        const uint32_t gr = gr0 + warp * 4 + wr;
+        const uint32_t row = gr - J.row0;
+        if (row >= J.n) {  // padding between jobs: zero operands (read only as masked rows/columns)
+            for (uint32_t t = lane; t < G.kpmax; t += 32) {
+                if (G.elem_bytes == 4) {
+                    reinterpret_cast<uint32_t *>(G.opa)[(size_t)gr * G.kpmax + t] = 0u;
+                } else {
+                    reinterpret_cast<uint16_t *>(G.opa)[(size_t)gr * G.kpmax + t] = 0;
+                    reinterpret_cast<uint16_t *>(G.opb)[(size_t)gr * G.kpmax + t] = 0;
+                }
+            }
+            continue;
+        }
+
+        double scale = 1.0;
+        bool zero_row = false;
+        if (J.metric == HM_METRIC_EUCLIDEAN) {
+            const double m = sqrt(__longlong_as_double((long long)maxb[6]));
+            if (m > 0.0) {
+                int e;
+                frexp(m, &e);  // m = f * 2^e, f in [0.5, 1)
+                scale = ldexp(1.0, -e);
+            }
+        } else {
+            const double rn = J.rnorm[row];
+            zero_row = !(rn > 0.0);
+            scale = zero_row ? 0.0 : 1.0 / rn;
+        }
+
+        const size_t kp = G.kpmax;
+        double uu = 0.0, ee = 0.0, rr = 0.0, aa = 0.0;
+        const float *xr = J.x + (size_t)row * J.d;
+        for (uint32_t t = lane; t < J.kp1; t += 32) {
+            double u = 0.0;
+            if (t < J.d) {
+                u = (J.metric == HM_METRIC_EUCLIDEAN) ? ((double)xr[t] - J.mu[t]) * scale
+                                                      : (zero_row ? 0.0 : (double)xr[t] / J.rnorm[row]);
+            }
+            uu += u * u;
+            if (G.kind == SCREEN_KIND_TF32) {
+                double r;
+                const uint32_t b = to_tf32_bits(u, &r);
+                reinterpret_cast<uint32_t *>(G.opa)[(size_t)gr * kp + t] = b;
+                ee += (r - u) * (r - u);
+                aa += r * r;
+            } else if (!G.split) {
+                double r;
+                const uint16_t b = to_bf16_bits(u, &r);
+                reinterpret_cast<uint16_t *>(G.opa)[(size_t)gr * kp + t] = b;
+                ee += (r - u) * (r - u);
+                aa += r * r;
             } else {
-                reinterpret_cast<uint16_t *>(G.opa)[(size_t)gr * G.kpmax + t] = 0;
-                reinterpret_cast<uint16_t *>(G.opb)[(size_t)gr * G.kpmax + t] = 0;
+                double hi, lo;
+                const uint16_t bh = to_bf16_bits(u, &hi);
+                const uint16_t bl = to_bf16_bits(u - hi, &lo);
+                const double res = (u - hi) - lo;
+                uint16_t *A = reinterpret_cast<uint16_t *>(G.opa) + (size_t)gr * kp;
+                uint16_t *B = reinterpret_cast<uint16_t *>(G.opb) + (size_t)gr * kp;
+                A[t] = bh;
+                A[J.kp1 + t] = bh;
+                A[2 * J.kp1 + t] = bl;
+                B[t] = bh;
+                B[J.kp1 + t] = bl;
+                B[2 * J.kp1 + t] = bh;
+                ee += lo * lo;
+                rr += res * res;
+                aa += 2.0 * hi * hi + lo * lo;
             }
         }
-        return;
-    }
-    unsigned long long *maxb = J.cnt->maxb;
-
-    double scale = 1.0;
-    bool zero_row = false;
-    if (J.metric == HM_METRIC_EUCLIDEAN) {
-        const double m = sqrt(__longlong_as_double((long long)maxb[6]));
-        if (m > 0.0) {
-            int e;
-            frexp(m, &e);  // m = f * 2^e, f in [0.5, 1)
-            scale = ldexp(1.0, -e);
-        }
-    } else {
-        const double rn = J.rnorm[row];
-        zero_row = !(rn > 0.0);
-        scale = zero_row ? 0.0 : 1.0 / rn;
-    }
-
-    const size_t kp = G.kpmax;
-    double uu = 0.0, ee = 0.0, rr = 0.0, aa = 0.0;
-    const float *xr = J.x + (size_t)row * J.d;
-    for (uint32_t t = lane; t < J.kp1; t += 32) {
-        double u = 0.0;
-        if (t < J.d) {
-            u = (J.metric == HM_METRIC_EUCLIDEAN) ? ((double)xr[t] - J.mu[t]) * scale
-                                                  : (zero_row ? 0.0 : (double)xr[t] / J.rnorm[row]);
-        }
-        uu += u * u;
-        if (G.kind == SCREEN_KIND_TF32) {
-            double r;
-            const uint32_t b = to_tf32_bits(u, &r);
-            reinterpret_cast<uint32_t *>(G.opa)[(size_t)gr * kp + t] = b;
-            ee += (r - u) * (r - u);
-            aa += r * r;
-        } else if (!G.split) {
-            double r;
-            const uint16_t b = to_bf16_bits(u, &r);
-            reinterpret_cast<uint16_t *>(G.opa)[(size_t)gr * kp + t] = b;
-            ee += (r - u) * (r - u);
-            aa += r * r;
-        } else {
-            double hi, lo;
-            const uint16_t bh = to_bf16_bits(u, &hi);
-            const uint16_t bl = to_bf16_bits(u - hi, &lo);
-            const double res = (u - hi) - lo;
-            uint16_t *A = reinterpret_cast<uint16_t *>(G.opa) + (size_t)gr * kp;
-            uint16_t *B = reinterpret_cast<uint16_t *>(G.opb) + (size_t)gr * kp;
-            A[t] = bh;
-            A[J.kp1 + t] = bh;
-            A[2 * J.kp1 + t] = bl;
-            B[t] = bh;
-            B[J.kp1 + t] = bl;
-            B[2 * J.kp1 + t] = bh;
-            ee += lo * lo;
-            rr += res * res;
-            aa += 2.0 * hi * hi + lo * lo;
+        uu = warp_sum(uu);
+        ee = warp_sum(ee);
+        rr = warp_sum(rr);
+        aa = warp_sum(aa);
+        if (lane == 0) {
+            RowStat st;
+            st.unorm = sqrt(uu);
+            st.enorm = sqrt(ee);
+            st.rnorm = sqrt(rr);
+            st.anorm = sqrt(aa);
+            st.bnorm = st.anorm;  // both operand layouts have the same row norm
+            st.sqnorm = uu;
+            G.rowstat[gr] = st;
+            wmax[0] = fmax(wmax[0], st.unorm);
+            wmax[1] = fmax(wmax[1], st.enorm);
+            wmax[2] = fmax(wmax[2], st.rnorm);
+            wmax[3] = fmax(wmax[3], st.anorm);
+            wmax[4] = fmax(wmax[4], st.bnorm);
+            wmax[5] = fmax(wmax[5], st.sqnorm);
+            if (J.metric == HM_METRIC_EUCLIDEAN) {
+                const float nsq = __double2float_rn(uu);
+                G.rowterm[gr] = nsq;
+                G.colterm[gr] = nsq;
+            } else {
+                G.rowterm[gr] = 0.0f;
+                G.colterm[gr] = zero_row ? 0.0f : 1.0f;
+            }
+            G.force[gr] = zero_row ? 1 : 0;
+            if (zero_row) ++wzero;
+            G.rowthr[gr] = 0xff800000u;  // the row's shared threshold starts at +inf
         }
     }
-    uu = warp_sum(uu);
-    ee = warp_sum(ee);
-    rr = warp_sum(rr);
-    aa = warp_sum(aa);
     if (lane == 0) {
-        RowStat st;
-        st.unorm = sqrt(uu);
-        st.enorm = sqrt(ee);
-        st.rnorm = sqrt(rr);
-        st.anorm = sqrt(aa);
-        st.bnorm = st.anorm;  // both operand layouts have the same row norm
-        st.sqnorm = uu;
-        G.rowstat[gr] = st;
-        atomic_max_pos(&maxb[0], st.unorm);
-        atomic_max_pos(&maxb[1], st.enorm);
-        atomic_max_pos(&maxb[2], st.rnorm);
-        atomic_max_pos(&maxb[3], st.anorm);
-        atomic_max_pos(&maxb[4], st.bnorm);
-        atomic_max_pos(&maxb[5], st.sqnorm);
-        if (J.metric == HM_METRIC_EUCLIDEAN) {
-            const float nsq = __double2float_rn(uu);
-            G.rowterm[gr] = nsq;
-            G.colterm[gr] = nsq;
-        } else {
-            G.rowterm[gr] = 0.0f;
-            G.colterm[gr] = zero_row ? 0.0f : 1.0f;
-        }
-        G.force[gr] = zero_row ? 1 : 0;
-        if (zero_row) atomicAdd(&maxb[7], 1ull);
-        G.rowthr[gr] = 0xff800000u;  // the row's shared threshold starts at +inf
+        for (int q = 0; q < 6; ++q) s_max[warp][q] = wmax[q];
+        s_zero[warp] = wzero;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        double m = s_max[0][threadIdx.x];
+        for (int w = 1; w < 8; ++w) m = fmax(m, s_max[w][threadIdx.x]);
+        atomic_max_pos(&maxb[threadIdx.x], m);
+    } else if (threadIdx.x == 6) {
+        unsigned long long z = 0;
+        for (int w = 0; w < 8; ++w) z += s_zero[w];
+        if (z) atomicAdd(&maxb[7], z);
     }
 }
 
@@ -251,8 +283,9 @@ int launch_screen_prep(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd
     HM_CUDA_TRY(cudaMemsetAsync(G.colterm, 0, round_up(G.rows, SC_BN) * sizeof(float) + SC_BN * sizeof(float), s));
     colsum_partial_kernel<<<G.njobs * CSUM_BLOCKS, 128, 0, s>>>(jobs, Gd);
     colmean_kernel<<<G.njobs, 128, 0, s>>>(jobs, Gd);
-    centred_norm_max_kernel<<<(G.rows + 7) / 8, 256, 0, s>>>(jobs, Gd);
-    operand_kernel<<<(G.rows + 7) / 8, 256, 0, s>>>(jobs, Gd);
+    // G.rows is a multiple of 32: 32 group rows per block
+    centred_norm_max_kernel<<<G.rows / 32, 256, 0, s>>>(jobs, Gd);
+    operand_kernel<<<G.rows / 32, 256, 0, s>>>(jobs, Gd);
     HM_CUDA_TRY(cudaGetLastError());
     count_launch(4);
     return HM_OK;
