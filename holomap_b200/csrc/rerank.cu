@@ -40,9 +40,8 @@ constexpr int RR_CBUF = 256;  // emitted candidates a warp stages in shared memo
 
 // One warp per group row; candidates are evaluated 32 at a time, one per lane.
 template <int METRIC, int KPL>
-__global__ void __launch_bounds__(RR_WARPS * 32, 3) rerank_kernel(const JobDev *__restrict__ jobs,
-                                                               const GroupDev *__restrict__ Gp,
-                                                               uint32_t dstride) {
+__device__ __forceinline__ void rerank_row(const JobDev *__restrict__ jobs, const GroupDev *__restrict__ Gp,
+                                           uint32_t dstride) {
     extern __shared__ double rr_smem[];
     const GroupDev &G = *Gp;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -287,7 +286,17 @@ int launch_screen_threshold(const JobDev *jobs, const GroupDev &G, const GroupDe
     return HM_OK;
 }
 
-template <int METRIC>
+// One launch covers both metrics of a group: each warp's row runs the
+// instantiation of its job's metric.
+template <int MASK, int KPL>
+__global__ void __launch_bounds__(RR_WARPS * 32, 3) rerank_kernel(const JobDev *__restrict__ jobs,
+                                                               const GroupDev *__restrict__ Gp,
+                                                               uint32_t dstride) {
+    if (MASK & (1 << HM_METRIC_EUCLIDEAN)) rerank_row<HM_METRIC_EUCLIDEAN, KPL>(jobs, Gp, dstride);
+    if (MASK & (1 << HM_METRIC_COSINE)) rerank_row<HM_METRIC_COSINE, KPL>(jobs, Gp, dstride);
+}
+
+template <int MASK>
 static int launch_metric(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t kpl,
                          uint32_t dmax, cudaStream_t s) {
     const uint32_t dstride = (uint32_t)round_up(dmax, 4);
@@ -296,8 +305,8 @@ static int launch_metric(const JobDev *jobs, const GroupDev &G, const GroupDev *
     const int blocks = (int)((G.rows + RR_WARPS - 1) / RR_WARPS);
 #define HM_RR_CASE(K)                                                                       \
     case K: {                                                                               \
-        HM_TRY(ensure_dynamic_smem((const void *)rerank_kernel<METRIC, K>, (int)smem));     \
-        rerank_kernel<METRIC, K><<<blocks, RR_WARPS * 32, smem, s>>>(jobs, Gd, dstride);    \
+        HM_TRY(ensure_dynamic_smem((const void *)rerank_kernel<MASK, K>, (int)smem));       \
+        rerank_kernel<MASK, K><<<blocks, RR_WARPS * 32, smem, s>>>(jobs, Gd, dstride);      \
         break;                                                                              \
     }
     switch (kpl) {
@@ -311,15 +320,15 @@ static int launch_metric(const JobDev *jobs, const GroupDev &G, const GroupDev *
     return HM_OK;
 }
 
-// one launch per metric present in the group
+// one launch for the metrics present in the group
 int launch_rerank(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t kpl,
                   uint32_t dmax, int metric_mask, cudaStream_t s) {
     if (G.rows == 0) return HM_OK;
     ScopedKernelTimer timer(HM_KCLASS_SELECT, s);
-    if (metric_mask & (1 << HM_METRIC_EUCLIDEAN))
-        HM_TRY(launch_metric<HM_METRIC_EUCLIDEAN>(jobs, G, Gd, kpl, dmax, s));
-    if (metric_mask & (1 << HM_METRIC_COSINE))
-        HM_TRY(launch_metric<HM_METRIC_COSINE>(jobs, G, Gd, kpl, dmax, s));
+    const int mask = metric_mask & ((1 << HM_METRIC_EUCLIDEAN) | (1 << HM_METRIC_COSINE));
+    if (mask == 1) return launch_metric<1>(jobs, G, Gd, kpl, dmax, s);
+    if (mask == 2) return launch_metric<2>(jobs, G, Gd, kpl, dmax, s);
+    if (mask == 3) return launch_metric<3>(jobs, G, Gd, kpl, dmax, s);
     return HM_OK;
 }
 
