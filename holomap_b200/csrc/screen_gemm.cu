@@ -406,6 +406,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
 #pragma unroll
             for (int q = 0; q < (PASS == 0 ? KP : 1); ++q) arr[q] = (q < KP - (int)J.k) ? -INF : INF;
             float tglob = INF, published = INF;
+            uint32_t tnext = 0xff800000u;  // ordered key of +inf
             const bool chunk_min = J.seed_tiles < J.part_tiles;
             // pass 1: the row's fixed threshold tau1 + band
             const float thr = (PASS == 1 && valid) ? __fadd_ru(unord32(G.rowthr[gr]), band) : -INF;
@@ -424,8 +425,12 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                     break;
                 }
                 fence_after_sync();
-                if (PASS == 0 && valid)  // the row's other lists may have tightened its k-th
-                    tglob = fminf(tglob, unord32(*(volatile const uint32_t *)(G.rowthr + gr)));
+                if (PASS == 0 && valid) {
+                    // the row's other lists may have tightened its k-th: use the
+                    // value loaded during the previous tile, load the next one
+                    tglob = fminf(tglob, unord32(tnext));
+                    tnext = *(volatile const uint32_t *)(G.rowthr + gr);
+                }
                 const uint32_t c_base = ct * SC_BN + half * (SC_BN / 2);
                 const bool diag = (ct * SC_BN < ut.rb * SC_BM + SC_BM) && (ut.rb * SC_BM < ct * SC_BN + SC_BN);
                 const uint32_t t_base = tmem_base + ((quad * 32) << 16) + buf * SC_BN + half * (SC_BN / 2);
