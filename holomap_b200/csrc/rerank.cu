@@ -34,6 +34,56 @@ __device__ __forceinline__ double step(double acc, double x, double y) {
     return __dadd_rn(acc, __dmul_rn(x, y));
 }
 
+// k-th smallest of a warp's `total` keys (at most 32 * NQ; lane l holds keys
+// l, l + 32, ...; absent keys are ~0): the largest r with fewer than k keys
+// below it, found bit by bit from the highest bit where the keys differ.
+template <int NQ>
+__device__ __forceinline__ uint32_t kth_key(const uint32_t (&ov)[NQ], uint32_t total, uint32_t k, int lane) {
+    uint32_t mn = 0xffffffffu, mx = 0u;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+        if ((uint32_t)(q * 32 + lane) < total) {
+            mn = min(mn, ov[q]);
+            mx = max(mx, ov[q]);
+        }
+    }
+    mn = __reduce_min_sync(0xffffffffu, mn);
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if (mn == mx) return mn;
+    const int top = 31 - __clz(mn ^ mx);
+    uint32_t r = top == 31 ? 0u : (mn & ~((2u << top) - 1u));  // the keys' common high bits
+    for (int b = top; b >= 0; --b) {
+        const uint32_t t = r | (1u << b);
+        uint32_t c = 0;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) c += ov[q] < t ? 1u : 0u;
+        c = __reduce_add_sync(0xffffffffu, c);
+        if (c < k) r = t;
+    }
+    return r;
+}
+
+// kth_key over keys key(e), e < total <= 256, with the register count
+// chosen by the total
+template <int NQ, typename KeyFn>
+__device__ __forceinline__ uint32_t kth_load(KeyFn key, uint32_t total, uint32_t k, int lane) {
+    uint32_t ov[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+        const uint32_t e = q * 32 + lane;
+        ov[q] = e < total ? key(e) : 0xffffffffu;
+    }
+    return kth_key<NQ>(ov, total, k, lane);
+}
+
+template <typename KeyFn>
+__device__ __forceinline__ uint32_t kth_of(KeyFn key, uint32_t total, uint32_t k, int lane) {
+    if (total <= 32) return kth_load<1>(key, total, k, lane);
+    if (total <= 64) return kth_load<2>(key, total, k, lane);
+    if (total <= 128) return kth_load<4>(key, total, k, lane);
+    return kth_load<8>(key, total, k, lane);
+}
+
 constexpr int RR_WARPS = 8;
 constexpr int RR_LIST = 256;  // compacted candidates per warp between flushes
 constexpr int RR_CBUF = 256;  // emitted candidates a warp stages in shared memory
@@ -86,24 +136,9 @@ __device__ __forceinline__ void rerank_row(const JobDev *__restrict__ jobs, cons
             base += cnt;
         }
         __syncwarp();
-        uint32_t ov[RR_CBUF / 32];
-#pragma unroll
-        for (int q = 0; q < RR_CBUF / 32; ++q) {
-            const uint32_t e = q * 32 + lane;
-            ov[q] = e < total ? ord32(__uint_as_float((uint32_t)(cbuf[e] >> 32))) : 0xffffffffu;
-        }
-        if (total >= k) {
-            uint32_t r = 0;  // largest key with fewer than k keys below it = the k-th
-            for (int b = 31; b >= 0; --b) {
-                const uint32_t t = r | (1u << b);
-                uint32_t c = 0;
-#pragma unroll
-                for (int q = 0; q < RR_CBUF / 32; ++q) c += ov[q] < t ? 1u : 0u;
-                c = __reduce_add_sync(0xffffffffu, c);
-                if (c < k) r = t;
-            }
-            tau = unord32(r);
-        }
+        if (total >= k)
+            tau = unord32(kth_of([&](uint32_t e) { return ord32(__uint_as_float((uint32_t)(cbuf[e] >> 32))); },
+                                 total, k, lane));
     } else {
         WarpTopK<KPL> sel;
         sel.reset();
@@ -239,21 +274,7 @@ __global__ void __launch_bounds__(256) threshold_kernel(const JobDev *__restrict
     const float *base = G.topk + J.topk0 + (l0 - J.slot0) * k;
     const uint32_t total = lists * k;
     if (total <= 256) {
-        uint32_t ov[8];
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const uint32_t e = q * 32 + lane;
-            ov[q] = e < total ? ord32(base[e]) : 0xffffffffu;
-        }
-        uint32_t r = 0;  // largest key with fewer than k keys below it = the k-th
-        for (int b = 31; b >= 0; --b) {
-            const uint32_t t = r | (1u << b);
-            uint32_t c = 0;
-#pragma unroll
-            for (int q = 0; q < 8; ++q) c += ov[q] < t ? 1u : 0u;
-            c = __reduce_add_sync(0xffffffffu, c);
-            if (c < k) r = t;
-        }
+        const uint32_t r = kth_of([&](uint32_t e) { return ord32(base[e]); }, total, k, lane);
         if (lane == 0) G.rowthr[gr] = r;
         return;
     }
