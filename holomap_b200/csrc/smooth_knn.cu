@@ -4,8 +4,10 @@
 // MIN_K_DIST_SCALE floors), mean at :82-84, and libm::expf reached through
 // src/fmath.rs:119-122.
 //
-// Rows of jobs with k <= 32 take one thread each (smooth_knn_row_kernel: the
-// row in registers, the reference's loop as written).  Larger k: one warp per
+// Rows of jobs with k <= 32 take four lanes each (smooth_knn_quad_kernel: the
+// row in registers, exp terms in parallel, the adds in the reference's order),
+// or one thread each when the rows alone fill the device
+// (smooth_knn_row_kernel).  Larger k: one warp per
 // row (of any job).  Lanes evaluate the row's exp terms in parallel; the
 // binary32 partial sum is then formed in the reference's order (j = 1, 2, ...,
 // k-1, each add rounded) by broadcasting the terms, so every lane holds the
@@ -103,7 +105,7 @@ __global__ void __launch_bounds__(256) smooth_knn_kernel(const JobDev *__restric
     const uint32_t ar = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (ar >= rows) return;
     const JobDev &J = jobs[row_starts ? find_job(row_starts, njobs, ar) : 0];
-    if (!J.sigma || !J.rho || J.k <= 32) return;  // k <= 32: smooth_knn_row_kernel
+    if (!J.sigma || !J.rho || J.k <= 32) return;  // k <= 32: the row kernels
     const uint32_t row = ar - J.arow0, k = J.k;
     const double target = J.target;
     const float *v = J.dist + (size_t)row * k;
@@ -180,6 +182,8 @@ __global__ void __launch_bounds__(256) smooth_knn_kernel(const JobDev *__restric
 // One thread per row for k <= KC: the row stays in registers and the whole
 // calibration is the reference's sequential loop, with no shuffles.  Rows of
 // jobs with k > KC are left to smooth_knn_kernel.
+// k <= KC (16 or 32), many rows: one thread per row, the row in registers and
+// the reference's loop as written.
 template <int KC>
 __global__ void __launch_bounds__(128) smooth_knn_row_kernel(const JobDev *__restrict__ jobs, uint32_t njobs,
                                                              const uint32_t *__restrict__ row_starts,
@@ -248,14 +252,110 @@ __global__ void __launch_bounds__(128) smooth_knn_row_kernel(const JobDev *__res
     J.rho[row] = rh;
 }
 
+// k <= KC (16 or 32): four lanes per row.  Lane q of a row holds the row's
+// values j = 4 i + q and evaluates their exp terms; every lane then forms the
+// binary32 partial sum in the reference's order (j = 1, ..., k - 1, each add
+// rounded) from the four lanes' terms, so the four lanes hold the same psum
+// and take the same branches (shuffles stay within the row's lanes).
+template <int KC>
+__global__ void __launch_bounds__(128) smooth_knn_quad_kernel(const JobDev *__restrict__ jobs, uint32_t njobs,
+                                                              const uint32_t *__restrict__ row_starts,
+                                                              uint32_t rows) {
+    constexpr int NV = KC / 4;
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t ar = tid >> 2, q = tid & 3;
+    if (ar >= rows) return;  // the row's four lanes leave together
+    const JobDev &J = jobs[row_starts ? find_job(row_starts, njobs, ar) : 0];
+    if (!J.sigma || !J.rho || J.k > KC) return;
+    const unsigned gmask = 0xfu << (threadIdx.x & 28u);
+    const uint32_t row = ar - J.arow0, k = J.k;
+    const double target = J.target;
+    const float *src = J.dist + (size_t)row * k;
+    float v[NV];
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+        const uint32_t j = 4 * i + q;
+        v[i] = j < k ? src[j] : 0.0f;
+    }
+    // value j of the row, from the lane that holds it
+    auto at = [&](int j) { return __shfl_sync(gmask, v[j >> 2], j & 3, 4); };
+
+    // rho: first positive distance in row order, else 0 (src/smooth_knn.rs:35)
+    float rh = 0.0f;
+#pragma unroll
+    for (int j = 0; j < KC; ++j) {
+        const float x = at(j);
+        if (rh == 0.0f && j < (int)k && x > 0.0f) rh = x;
+    }
+    // bisection, binary32 state, hi seeded at f32::MAX (src/smooth_knn.rs:39-65)
+    const float f32max = __uint_as_float(0x7f7fffffu);
+    float lo = 0.0f, hi = f32max, mid = 1.0f;
+    for (int it = 0; it < 64; ++it) {
+        float term[NV];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            const float dd = __fsub_rn(v[i], rh);
+            term[i] = (dd > 0.0f) ? expf_libm(-__fdiv_rn(dd, mid)) : 1.0f;
+        }
+        float psum = 0.0f;
+#pragma unroll
+        for (int j = 1; j < KC; ++j) {
+            const float t = __shfl_sync(gmask, term[j >> 2], j & 3, 4);
+            if (j < (int)k) psum = __fadd_rn(psum, t);
+        }
+        const double ps = (double)psum;
+        if (fabs(__dsub_rn(ps, target)) < 1e-5) break;
+        if (ps > target) {
+            hi = mid;
+            mid = __fdiv_rn(__fadd_rn(lo, hi), 2.0f);
+        } else {
+            lo = mid;
+            if (hi >= f32max)
+                mid = __fmul_rn(mid, 2.0f);
+            else
+                mid = __fdiv_rn(__fadd_rn(lo, hi), 2.0f);
+        }
+    }
+    float sg = mid;
+    if (rh > 0.0f) {
+        // floor = 1e-3 * mean(row), mean = f32(sequential f64 sum / k)
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < KC; ++j) {
+            const float x = at(j);
+            if (j < (int)k) s = __dadd_rn(s, (double)x);
+        }
+        const float floor_v = __fmul_rn(1e-3f, __double2float_rn(__ddiv_rn(s, (double)k)));
+        if (sg < floor_v) sg = floor_v;
+    } else if (q == 0) {
+        // floored later with the job's global mean (mean_all_floor_kernel)
+        const uint32_t slot = atomicAdd(&J.cnt->zero_count, 1u);
+        J.zero_rows[slot] = row;
+    }
+    if (q == 0) {
+        J.sigma[row] = sg;
+        J.rho[row] = rh;
+    }
+}
+
 int launch_smooth(const JobDev *jobs, uint32_t njobs, const uint32_t *row_starts, uint32_t rows,
                   uint32_t kmax, cudaStream_t s) {
     ScopedKernelTimer timer(HM_KCLASS_SMOOTH, s);
     // every job with k <= 32 (the kernel returns for rows of larger k)
-    if (kmax <= 16)
-        smooth_knn_row_kernel<16><<<(rows + 127) / 128, 128, 0, s>>>(jobs, njobs, row_starts, rows);
-    else
-        smooth_knn_row_kernel<32><<<(rows + 127) / 128, 128, 0, s>>>(jobs, njobs, row_starts, rows);
+    // four lanes per row unless the rows alone fill the device (then the
+    // extra lanes' shuffles cost more than the shorter exp chains save)
+    const bool quad = rows < (1u << 17);
+    if (kmax <= 16) {
+        if (quad)
+            smooth_knn_quad_kernel<16><<<(rows + 31) / 32, 128, 0, s>>>(jobs, njobs, row_starts, rows);
+        else
+            smooth_knn_row_kernel<16><<<(rows + 127) / 128, 128, 0, s>>>(jobs, njobs, row_starts, rows);
+    } else {
+        if (quad)
+            smooth_knn_quad_kernel<32><<<(rows + 31) / 32, 128, 0, s>>>(jobs, njobs, row_starts, rows);
+        else
+            smooth_knn_row_kernel<32><<<(rows + 127) / 128, 128, 0, s>>>(jobs, njobs, row_starts, rows);
+    }
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();
     if (kmax > 32) {  // rows of jobs with k > 32, one warp per row
