@@ -1,21 +1,24 @@
 // screen_gemm.cu -- the tensor-core screen: U U^T on tcgen05 with TMEM
-// accumulators, fused with a per-row running top-k threshold and candidate
-// emission, so the N x N similarity matrix never leaves the SM.
+// accumulators, fused with the per-row thresholds and the candidate emission,
+// so the N x N similarity matrix never leaves the SM.
 //
 // One CTA per SM (persistent), 10 warps:
-//   warp 0     TMA producer: 128-row A slice + 256-row B slice per stage
-//              (128-byte K slices, 128B swizzle, 4-stage mbarrier ring; no
-//              cluster multicast),
+//   warp 0     TMA producer: the unit's 128-row A block stays resident in
+//              shared memory when its K slices fit 96 KB (else it streams
+//              with B), 256-row B slices per stage (128-byte K slices, 128B
+//              swizzle, 4-stage mbarrier ring; every CTA loads its own tiles),
 //   warp 1     allocates 512 TMEM columns (two 128 x 256 fp32 accumulators)
 //              and issues tcgen05.mma (one thread) + tcgen05.commit,
 //   warps 2-9  epilogue: each thread owns one query row (its TMEM lane) and
-//              one half of every tile's 256 columns.  Per 32-column chunk it
-//              forms the screened values c^ in binary32 and their minimum
-//              (branch-free); only when that minimum passes the row's
-//              threshold does it emit the chunk's columns with
-//              c^ <= tau + band into the row's candidate list and insert
-//              them into a sorted register array of the k smallest c^ seen,
-//              whose largest entry is tau.
+//              one half of every tile's 256 columns, read 32 columns at a time.
+// Two launches per group (template PASS):
+//   0  threshold pass over a sample of each part's columns: per list, the k
+//      smallest minima of column chunks, sorted in registers and shared
+//      between the row's lists (atomicMin); threshold_kernel then takes the
+//      k-th of the union, tau1, an upper bound of the row's k-th screened value;
+//   1  emission pass over all columns with the fixed limit tau1 + band: 8-column
+//      group minima gate the per-column test, which writes every column within
+//      the limit into the row's list.
 // Work units are (row block of 128, column part); the columns of a unit are
 // walked in 256-wide tiles with the two accumulators double buffered, so the
 // epilogue of one tile overlaps the MMAs of the next.
