@@ -4,7 +4,9 @@
 // The screened pipeline of one group of jobs is (see api.cu for the order):
 //   screen prep   operands + binary64 error statistics (screen_prep.cu)
 //   band          keep band 2E_i per row
-//   screen gemm   tcgen05 U U^T + running top-k + candidate emission
+//   screen gemm   tcgen05 U U^T, threshold pass over a column sample
+//   threshold     tau1 per row (rerank.cu)
+//   screen gemm   tcgen05 U U^T, emission pass within tau1 + band
 //   rerank        exact distances of the survivors + select (rerank.cu)
 //   fallback      plain exact kernel over the rows the screen could not bound
 #include <cuda.h>

@@ -665,7 +665,7 @@ static int launch_pass(const JobDev *jobs, const GroupDev &G, uint32_t kp, const
     return set_error(HM_ERR_UNSUPPORTED, "screen top-k width %u", kp);
 }
 
-// pass 0: running k smallest mini-chunk minima per list (-> tau1 per row);
+// pass 0: each list's k smallest chunk minima over the column sample (-> tau1);
 // pass 1: emission of every column within tau1 + band
 int launch_screen_gemm(const JobDev *jobs, const GroupDev &G, const GroupDev *, uint32_t kp,
                        const CUtensorMap &ta, const CUtensorMap &tb, float *dump, int pass,
