@@ -811,7 +811,7 @@ def roofline(runner, kern, clk, workload_name) -> dict:
         src = "MEASURED_PEAKS.json bf16_tflops_sustained (of measured)" if peaks else \
             "fallback 1.4 PFLOP/s sustained (of fallback)"
         # the screen of one step is two launches: the threshold pass (over
-        # a quarter of the columns) and the emission pass (all columns);
+        # an eighth of the columns) and the emission pass (all columns);
         # achieved counts the useful product 2 n^2 d once per step
         step_s = ms / max(launches // 2, 1) / 1e3
         return {"bound": "tensor", "kernel": "screen_gemm_kernel (threshold + emission launches)",

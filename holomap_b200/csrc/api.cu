@@ -265,9 +265,9 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
                 P.part_tiles = (P.col_tiles + parts - 1) / parts;
                 P.parts = (P.col_tiles + P.part_tiles - 1) / P.part_tiles;
             }
-            // threshold-pass sample: a quarter of the columns, at least 2048
+            // threshold-pass sample: an eighth of the columns, at least 2048
             // (all of them for small jobs), spread over the parts
-            const uint64_t seed_cols = std::max<uint64_t>(P.spec.n / 4, 2048);
+            const uint64_t seed_cols = std::max<uint64_t>(P.spec.n / 8, 2048);
             P.seed_tiles = std::min<uint32_t>(
                 P.part_tiles, (uint32_t)((seed_cols + (uint64_t)SC_BN * P.parts - 1) / ((uint64_t)SC_BN * P.parts)));
             P.seed_tiles = std::max<uint32_t>(P.seed_tiles, 1);

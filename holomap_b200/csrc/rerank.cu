@@ -63,7 +63,7 @@ __device__ __forceinline__ uint32_t kth_key(const uint32_t (&ov)[NQ], uint32_t t
     return r;
 }
 
-// kth_key over keys key(e), e < total <= 256, with the register count
+// kth_key over keys key(e), e < total <= 512, with the register count
 // chosen by the total
 template <int NQ, typename KeyFn>
 __device__ __forceinline__ uint32_t kth_load(KeyFn key, uint32_t total, uint32_t k, int lane) {
@@ -81,12 +81,13 @@ __device__ __forceinline__ uint32_t kth_of(KeyFn key, uint32_t total, uint32_t k
     if (total <= 32) return kth_load<1>(key, total, k, lane);
     if (total <= 64) return kth_load<2>(key, total, k, lane);
     if (total <= 128) return kth_load<4>(key, total, k, lane);
-    return kth_load<8>(key, total, k, lane);
+    if (total <= 256) return kth_load<8>(key, total, k, lane);
+    return kth_load<16>(key, total, k, lane);
 }
 
 constexpr int RR_WARPS = 8;
 constexpr int RR_LIST = 256;  // compacted candidates per warp between flushes
-constexpr int RR_CBUF = 256;  // emitted candidates a warp stages in shared memory
+constexpr int RR_CBUF = 512;  // emitted candidates a warp stages in shared memory
 
 // One warp per group row; candidates are evaluated 32 at a time, one per lane.
 template <int METRIC, int KPL>
