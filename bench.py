@@ -243,6 +243,45 @@ def batch_config(wls) -> dict:
             "l2": "flushed before every timed step (256 MiB write)", "parallelism": "replicas"}
 
 
+def screen_error(wl, path: str, rows: int = 2048) -> dict | None:
+    """The screen's observed error against binary64 on the first `rows`
+    points of the workload (the screened values are dumped by the library's
+    test hook; the threshold pass sees every column at this size): max
+    |c^ - c| over all pairs, next to the largest keep band 2E the library
+    derived for that problem.  The keep rule needs |c^ - c| <= E."""
+    import torch
+
+    import holomap_b200 as hm
+    x = np.ascontiguousarray(wl.data[:rows])
+    n, d = x.shape
+    st = hm.HmStats()
+    buf = torch.full((n * n,), float("nan"), dtype=torch.float32, device="cuda")
+    hm.lib().hm_debug_set_screen_dump(buf.data_ptr())
+    try:
+        hm.exact_knn(x, d, wl.k, wl.metric, path, stats=st)
+    finally:
+        hm.lib().hm_debug_set_screen_dump(None)
+    if st.path_used == hm.KnnPath.PLAIN:
+        return None
+    c = buf.cpu().numpy().reshape(n, n).astype(np.float64)
+    xd = x.astype(np.float64)
+    if wl.metric == "cosine":
+        u = xd / np.linalg.norm(xd, axis=1, keepdims=True)
+        exact = 1.0 - u @ u.T
+    else:
+        u = xd - xd.mean(0)
+        m = np.sqrt((u * u).sum(1).max())
+        u = u * 2.0 ** -np.frexp(m)[1]
+        sq = (u * u).sum(1)
+        exact = sq[:, None] + sq[None, :] - 2 * u @ u.T
+    np.fill_diagonal(exact, 0.0)
+    err = float(np.abs(c - exact).max())
+    return {"rows": n, "path": hm.KnnPath(int(st.path_used)).name.lower(),
+            "max_abs_error": err, "band_max": float(st.screen_band),
+            "error_over_half_band": err / (float(st.screen_band) / 2) if st.screen_band else None,
+            "value_space": "1 - cos" if wl.metric == "cosine" else "squared distance of centred, scaled rows"}
+
+
 def lib_workspace(wl, path) -> int:
     from holomap_b200 import _lib
     return int(_lib.lib().hm_workspace_bytes(wl.n, wl.d, wl.k, int(_lib.Metric.parse(wl.metric)),
@@ -589,6 +628,8 @@ def main():
                         "max": max(step_ms)},
             "stats": stats,
         }
+        if hasattr(runner, "wl") and not runner.plain:
+            line["screen_error"] = screen_error(runner.wl, runner.path)
         if world == 1 and not args.no_cpu_baseline:
             cb = runner.cpu_baseline(args.cpu_seconds)
             cb.pop("seconds", None)
