@@ -282,6 +282,11 @@ def screen_error(wl, path: str, rows: int = 2048) -> dict | None:
             "value_space": "1 - cos" if wl.metric == "cosine" else "squared distance of centred, scaled rows"}
 
 
+def torch_equal(host, dev_t) -> bool:
+    """Byte equality of a host tensor and a device tensor."""
+    return bool(np.array_equal(host.numpy().view(np.uint32), dev_t.cpu().numpy().view(np.uint32)))
+
+
 def lib_workspace(wl, path) -> int:
     from holomap_b200 import _lib
     return int(_lib.lib().hm_workspace_bytes(wl.n, wl.d, wl.k, int(_lib.Metric.parse(wl.metric)),
@@ -403,7 +408,16 @@ class BatchRunner:
 
         from holomap_b200.device import DeviceBatch
         self.wls, self.dev = wls, dev
-        self.x_dev = [torch.from_numpy(w.data).to(dev) for w in wls]
+        # all datasets in one device buffer (one host-to-device copy per step),
+        # each starting 256-byte aligned
+        self.offs, off = [], 0
+        for w in wls:
+            self.offs.append(off)
+            off += (w.n * w.d + 63) // 64 * 64
+        self.host_in = np.zeros(off, dtype=np.float32)
+        for w, o in zip(wls, self.offs):
+            self.host_in[o:o + w.n * w.d] = w.data.reshape(-1)
+        self.x_all, self.x_dev = self._views(torch.from_numpy(self.host_in).to(dev))
         self.batch = DeviceBatch([(x, w.k, w.metric) for x, w in zip(self.x_dev, wls)], device=dev)
         self.graphs_per_step = len(wls)
         self.paths = [self.batch.path(j) for j in range(len(wls))]
@@ -412,26 +426,66 @@ class BatchRunner:
     def step(self, stream, graph=True):
         self.batch.run(stream, graph=graph)
 
+    def _views(self, flat):
+        return flat, [flat[o:o + w.n * w.d].view(w.n, w.d) for w, o in zip(self.wls, self.offs)]
+
     def e2e_prepare(self):
         import torch
-        self.pin_x = [torch.from_numpy(w.data).pin_memory() for w in self.wls]
-        self.pin_out = [[torch.empty_like(t, device="cpu").pin_memory() for t in prob[1:5]]
-                        for prob in self.batch.problems]
+        self.pin_in = torch.from_numpy(self.host_in).pin_memory()
+        self.pin_out = torch.empty_like(self.batch.out, device="cpu").pin_memory()
 
     def e2e_step(self):
+        """One batch, one call at a time: one copy in, the graph, one copy out."""
         import torch
         s = torch.cuda.current_stream(self.dev)
-        for x, p in zip(self.x_dev, self.pin_x):
-            x.copy_(p, non_blocking=True)
+        self.x_all.copy_(self.pin_in, non_blocking=True)
         self.batch.run(s, graph=True)
-        for prob, outs in zip(self.batch.problems, self.pin_out):
-            for t, o in zip(prob[1:5], outs):
-                o.copy_(t, non_blocking=True)
+        self.pin_out.copy_(self.batch.out, non_blocking=True)
         s.synchronize()
 
     def e2e_matches(self) -> bool:
-        return all(np.array_equal(o[0].numpy(), prob[1].cpu().numpy())
-                   for prob, o in zip(self.batch.problems, self.pin_out))
+        return bool(torch_equal(self.pin_out, self.batch.out))
+
+    def e2e_pipelined(self, steps: int) -> tuple[float, bool]:
+        """``steps`` batches with two sets of buffers: the copy in of one
+        batch and the copy out of the previous one overlap the graph of the
+        other set (separate copy streams, event-ordered)."""
+        import torch
+
+        from holomap_b200.device import DeviceBatch
+        dev = self.dev
+        sets = [(self.x_all, self.batch)]
+        x2, v2 = self._views(torch.empty_like(self.x_all))
+        sets.append((x2, DeviceBatch([(x, w.k, w.metric) for x, w in zip(v2, self.wls)], device=dev)))
+        outs = [torch.empty_like(self.batch.out, device="cpu").pin_memory() for _ in sets]
+        s_in, s_run, s_out = (torch.cuda.Stream(dev) for _ in range(3))
+        ev_in = [torch.cuda.Event() for _ in sets]
+        ev_run = [torch.cuda.Event() for _ in sets]
+        ev_out = [torch.cuda.Event() for _ in sets]
+        for b, (_, batch) in enumerate(sets):  # capture both graphs before timing
+            batch.run(s_run, graph=True)
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for i in range(steps):
+            b = i % 2
+            x, batch = sets[b]
+            if i >= 2:
+                s_in.wait_event(ev_run[b])    # the set's previous graph read its inputs
+                s_run.wait_event(ev_out[b])   # and its previous outputs were copied out
+            with torch.cuda.stream(s_in):
+                x.copy_(self.pin_in, non_blocking=True)
+                ev_in[b].record(s_in)
+            s_run.wait_event(ev_in[b])
+            batch.run(s_run, graph=True)
+            ev_run[b].record(s_run)
+            s_out.wait_event(ev_run[b])
+            with torch.cuda.stream(s_out):
+                outs[b].copy_(batch.out, non_blocking=True)
+                ev_out[b].record(s_out)
+        torch.cuda.synchronize(dev)
+        elapsed = time.perf_counter() - t0
+        same = all(torch_equal(o, self.batch.out) for o in outs)
+        return elapsed, same
 
     def io_bytes(self):
         h2d = sum(int(w.n * w.d * 4) for w in self.wls)
@@ -595,6 +649,7 @@ def main():
     e2e_value = world * e2e_steps * runner.graphs_per_step / e2e_s
     same = runner.e2e_matches()
     e2e_sync = e2e_value
+    pipelined, p_value = False, None
     if hasattr(runner, "e2e_pipelined"):
         # the public asynchronous API with two requests in flight
         barrier()
@@ -603,8 +658,10 @@ def main():
             t = torch.tensor([p_s], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             p_s = float(t.item())
-        e2e_value = world * e2e_steps * runner.graphs_per_step / p_s
+        p_value = world * e2e_steps * runner.graphs_per_step / p_s
         same = same and p_same
+        pipelined = p_value >= e2e_sync  # report the faster public-API method
+        e2e_value = max(p_value, e2e_sync)
 
     if rank == 0:
         h2d, d2h = runner.io_bytes()
@@ -617,9 +674,12 @@ def main():
             "path": str(getattr(runner, "path", "auto")).split(".")[-1].lower(),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps, "matches_device_run": same,
-                    "api": ("hm_submit/hm_wait, 2 requests in flight"
-                            if hasattr(runner, "e2e_pipelined") else "hm_batch_* from pinned buffers"),
-                    "one_call_at_a_time": e2e_sync},
+                    "api": (("hm_submit/hm_wait, 2 requests in flight" if hasattr(runner, "wl") else
+                             "hm_batch_graph_launch, two buffer sets: one copy in and one copy out "
+                             "per batch overlapping the other set's graph") if pipelined else
+                            ("hm_knn_smooth, one call at a time" if hasattr(runner, "wl") else
+                             "hm_batch_graph_launch, one batch at a time")),
+                    "one_call_at_a_time": e2e_sync, "pipelined": p_value},
             "gpu_launches": int(launches_per_step * args.steps),
             "roofline": roofline(runner, kern, clk, args.workload),
             "kernels_ms_per_step": {c: kern[c][0] / max(args.steps, 1) for c in kern},

@@ -178,7 +178,9 @@ __device__ __forceinline__ void rerank_row(const JobDev *__restrict__ jobs, cons
             const float *xj = J.x + (size_t)j * d;
             double acc = 0.0;
             uint32_t t = 0;
-            if ((d & 3u) == 0) {
+            // 16-byte loads when every row starts 16-byte aligned (the caller's
+            // pointer need only be 4-byte aligned)
+            if ((d & 3u) == 0 && (reinterpret_cast<uintptr_t>(J.x) & 15u) == 0) {
                 const float4 *xj4 = reinterpret_cast<const float4 *>(xj);
                 const double2 *xi2 = reinterpret_cast<const double2 *>(xi);
 #pragma unroll 4

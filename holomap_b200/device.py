@@ -65,15 +65,27 @@ class DeviceBatch:
         self.device = torch.device("cuda", device) if isinstance(device, int) else device
         self.problems = []
         jobs = (HmJob * len(problems))()
+        # every job's outputs (indices, distances, sigmas, rhos) live in one
+        # 4-byte-element buffer, so a batch's results come back in one copy
+        sizes = [int(p[0].shape[0]) * int(p[1]) * 2 + (2 * int(p[0].shape[0]) if smooth else 0)
+                 for p in problems]
+        self.out = torch.empty(sum(sizes), dtype=torch.float32, device=self.device)
+        off = 0
         for i, prob in enumerate(problems):
             data, k, metric = prob[0], int(prob[1]), Metric.parse(prob[2])
             path = KnnPath.parse(prob[3]) if len(prob) > 3 else KnnPath.AUTO
             assert data.is_cuda and data.dtype == torch.float32 and data.is_contiguous()
             n, d = data.shape
-            idx = torch.empty(n * k, dtype=torch.int32, device=self.device)
-            dist = torch.empty(n * k, dtype=torch.float32, device=self.device)
-            sig = torch.empty(n, dtype=torch.float32, device=self.device) if smooth else None
-            rho = torch.empty(n, dtype=torch.float32, device=self.device) if smooth else None
+
+            def take(m):
+                nonlocal off
+                t = self.out[off:off + m]
+                off += m
+                return t
+            idx = take(n * k).view(torch.int32)
+            dist = take(n * k)
+            sig = take(n) if smooth else None
+            rho = take(n) if smooth else None
             self.problems.append((data, idx, dist, sig, rho, k))
             jobs[i] = HmJob(data.data_ptr(), n, d, k, int(metric), int(path), idx.data_ptr(),
                             dist.data_ptr(), sig.data_ptr() if smooth else None,

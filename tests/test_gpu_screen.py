@@ -105,3 +105,25 @@ def test_screened_equals_plain_on_clustered_duplicates():
         assert_same_bytes(b.indices, a.indices, f"{path} indices")
         assert_same_bytes(b.dists, a.dists, f"{path} dists")
         assert rows_sorted_by_key(b.indices.reshape(-1, wl.k), b.dists.reshape(-1, wl.k))
+
+
+@pytest.mark.parametrize("path", PATHS)
+def test_device_data_at_a_4_byte_offset(oracle, path):
+    """The C ABI takes any 4-byte-aligned device pointer: points given at an
+    odd float offset inside a larger buffer (d a multiple of 4, so the
+    rerank's 16-byte row loads must not be used) return the oracle's bytes."""
+    import torch
+    from holomap_b200.device import DeviceKnnProblem
+    n, d, k = 1500, 32, 15
+    x = edge_case("gauss", n, d, seed=41)
+    big = torch.zeros(n * d + 1, dtype=torch.float32, device="cuda")
+    big[1:] = torch.from_numpy(x.reshape(-1)).cuda()
+    view = big[1:].view(n, d)
+    assert view.data_ptr() % 16 != 0
+    p = DeviceKnnProblem(n, d, k, "euclidean", path)
+    p.run(view)
+    torch.cuda.synchronize()
+    oi, od = oracle.exact_knn(x, k, "euclidean")
+    assert_same_bytes(p.idx.cpu().numpy().view(np.uint32), oi, "indices")
+    assert_same_bytes(p.dist.cpu().numpy(), od, "dists")
+    assert p.stats().path_used == hm.KnnPath.parse(path)
