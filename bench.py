@@ -52,6 +52,8 @@ def parse_args():
                     help="use only the first ROWS points of the workload (a smaller case "
                          "of the same kernels, e.g. for profiling)")
     ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--e2e-window", type=int, default=2,
+                    help="requests in flight in the pipelined end-to-end measurement")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the oracle baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -653,7 +655,8 @@ def main():
     if hasattr(runner, "e2e_pipelined"):
         # the public asynchronous API with two requests in flight
         barrier()
-        p_s, p_same = runner.e2e_pipelined(e2e_steps)
+        p_s, p_same = (runner.e2e_pipelined(e2e_steps, args.e2e_window) if hasattr(runner, "wl")
+                       else runner.e2e_pipelined(e2e_steps))
         if world > 1:
             t = torch.tensor([p_s], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -674,7 +677,7 @@ def main():
             "path": str(getattr(runner, "path", "auto")).split(".")[-1].lower(),
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": e2e_steps, "matches_device_run": same,
-                    "api": (("hm_submit/hm_wait, 2 requests in flight" if hasattr(runner, "wl") else
+                    "api": ((f"hm_submit/hm_wait, {args.e2e_window} requests in flight" if hasattr(runner, "wl") else
                              "hm_batch_graph_launch, two buffer sets: one copy in and one copy out "
                              "per batch overlapping the other set's graph") if pipelined else
                             ("hm_knn_smooth, one call at a time" if hasattr(runner, "wl") else
