@@ -98,3 +98,25 @@ def test_row_shard_ranges_are_validated_on_cpu():
     for b, e in [(0, 0), (10, 5), (0, 1001)]:
         assert lib.hm_knn_rows_workspace_bytes(1000, 8, 5, 0, 1, b, e) == 0
         assert "query rows" in lib.hm_last_error().decode()
+
+
+def test_autotune_table():
+    """The autotuner's table (hm_autotune_path): plain where no screen
+    applies or pays, split-bf16 up to d = 256, then bf16 (cosine) / tf32."""
+    at = hm.autotune_path
+    P = hm.KnnPath
+    assert at(50000, 300, 15, "manhattan") == P.PLAIN      # no inner-product form
+    assert at(50000, 384, 65, "cosine") == P.PLAIN         # k above the screen's 64
+    assert at(50000, 4096, 15, "euclidean") == P.PLAIN     # d above 2048
+    assert at(511, 50, 15, "euclidean") == P.PLAIN         # too small to pay
+    assert at(1000, 50, 15, "euclidean") == P.SCREEN_BF16X3
+    assert at(20000, 256, 15, "cosine") == P.SCREEN_BF16X3
+    assert at(50000, 384, 30, "cosine") == P.SCREEN_BF16
+    assert at(50000, 300, 15, "euclidean") == P.SCREEN_TF32
+
+
+def test_every_screened_path_plans_for_the_benchmark_shapes():
+    for n, d, k, metric in [(1000, 50, 15, "euclidean"), (20000, 128, 15, "euclidean"),
+                            (50000, 384, 30, "cosine")]:
+        for path in ("auto", "plain", "screen_bf16", "screen_tf32", "screen_bf16x3"):
+            assert hm.workspace_bytes(n, d, k, metric, path) > 0
