@@ -9,6 +9,7 @@ collective is on the data path).
 
     python bench.py [--gpus N --steps K --warmup W] [--workload W] [--path P]
     python bench.py --impl reference ...   # the reference algorithm on host cores
+    python bench.py --workload fuzzy_50k   # the fuzzy simplicial set of that graph
 
 Prints one JSON line (rank 0).
 """
@@ -46,7 +47,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="embed_50k",
-                    choices=["embed_50k", "dups_20k", "blobs_1k", "batch_256", "serve_2000"])
+                    choices=["embed_50k", "dups_20k", "blobs_1k", "batch_256", "serve_2000",
+                             "fuzzy_50k"])
     ap.add_argument("--path", default="auto")
     ap.add_argument("--rows", type=int, default=None,
                     help="use only the first ROWS points of the workload (a smaller case "
@@ -167,6 +169,8 @@ def reference_arm(args):
     import holomap_oracle
     holomap_oracle.build()
     threads = os.cpu_count() or 1
+    if args.workload == "fuzzy_50k":
+        return fuzzy_reference_arm(args)
     if args.workload in ("batch_256", "serve_2000"):
         if args.workload == "batch_256":
             from holomap_b200.synth import batch_256
@@ -559,6 +563,8 @@ def main():
         return reference_arm(args)
     if args.workload == "serve_2000":
         return serve_main(args)
+    if args.workload == "fuzzy_50k":
+        return fuzzy_main(args)
 
     import torch
     import torch.distributed as dist
@@ -701,6 +707,170 @@ def main():
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+    return 0
+
+
+# ------------------------------------------------------------ fuzzy graph
+FUZZY_METRIC = "fuzzy simplicial sets/s (src/fuzzy.rs, bit-exact)"
+FUZZY_UNIT = "graphs/s"
+
+
+def fuzzy_input(wl):
+    """The kNN graph and calibration the fuzzy stage consumes, for workload
+    ``wl``: computed once on the device by this library (bit-exact to the
+    reference) and returned as host arrays (idx, dist, sigma, rho)."""
+    import holomap_b200 as hm
+    knn, sm = hm.knn_smooth(wl.data, wl.d, wl.k, wl.metric)
+    return knn.indices, knn.dists, sm.sigmas, sm.rhos
+
+
+def fuzzy_config(wl, nnz=None) -> dict:
+    cfg = {"workload": "fuzzy_50k", "input": f"kNN graph + calibration of {wl.name} "
+           f"(n={wl.n}, d={wl.d}, k={wl.k}, {wl.metric})", "n": wl.n, "k": wl.k,
+           "l2": "flushed before every timed step (256 MiB write)", "parallelism": "replicas"}
+    if nnz is not None:
+        cfg["nnz"] = nnz
+    return cfg
+
+
+def fuzzy_reference_arm(args) -> int:
+    """The reference's fuzzy_simplicial_set (as its C restatement) on one host
+    thread: the algorithm is a sequential sort, binary searches and a scan."""
+    import holomap_oracle
+    wl = workload("embed_50k", args.rows)
+    idx, dist, sig, rho = fuzzy_input(wl)
+
+    def once():
+        t0 = time.perf_counter()
+        holomap_oracle.fuzzy_graph(idx, dist, sig, rho, wl.k)
+        return time.perf_counter() - t0
+
+    for _ in range(args.warmup):
+        once()
+    times = [once() for _ in range(args.steps)]
+    per = sum(times) / len(times)
+    value = 1.0 / per
+    line = {
+        "metric": FUZZY_METRIC, "value": value, "unit": FUZZY_UNIT, "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": fuzzy_config(wl), "path": "reference (host cores)",
+        "cpu_baseline": {"value": value, "unit": FUZZY_UNIT, "cores": 1, "kind": "port",
+                         "sample": "the whole graph per step; C restatement of src/fuzzy.rs:25-91"},
+        "e2e": {"value": value, "unit": FUZZY_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def fuzzy_main(args) -> int:
+    """fuzzy_50k: one step = the fuzzy simplicial set (hm_fuzzy_graph_device)
+    of the embed_50k kNN graph, inputs resident in HBM.  e2e = the host entry
+    point hm_fuzzy_graph (host arrays in, COO out)."""
+    import ctypes
+
+    import torch
+
+    import holomap_b200 as hm
+    from holomap_b200 import _lib
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1 and int(os.environ.get("RANK", "0")) != 0:
+        return 0  # one replica; the stage has no multi-GPU form
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    wl = workload("embed_50k", args.rows)
+    idx, dist, sig, rho = fuzzy_input(wl)
+    n, k = wl.n, wl.k
+    lib = hm.lib()
+    t = lambda a: torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a).to(dev)
+    d_idx, d_dist, d_sig, d_rho = t(idx), t(dist), t(sig), t(rho)
+    cap = 2 * n * k
+    rows = torch.empty(cap, dtype=torch.int32, device=dev)
+    cols = torch.empty(cap, dtype=torch.int32, device=dev)
+    vals = torch.empty(cap, dtype=torch.float32, device=dev)
+    nnz = torch.zeros(1, dtype=torch.int64, device=dev)
+    ws_bytes = lib.hm_fuzzy_workspace_bytes(n, k)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        _lib.check(lib.hm_fuzzy_graph_device(
+            d_idx.data_ptr(), d_dist.data_ptr(), d_sig.data_ptr(), d_rho.data_ptr(), n, k,
+            rows.data_ptr(), cols.data_ptr(), vals.data_ptr(), nnz.data_ptr(), ws.data_ptr(),
+            ws_bytes, ctypes.c_void_p(stream.cuda_stream)))
+
+    l0 = _lib.launch_count()
+    step()
+    torch.cuda.synchronize(dev)
+    launches = _lib.launch_count() - l0
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    m = int(nnz.item())
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    evs = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(step_ms)
+    value = args.steps / (total_ms / 1e3)
+
+    # end to end: the host entry point, host arrays in and the COO out
+    e2e_steps = args.e2e_steps or max(3, min(args.steps, 10))
+    g = hm.fuzzy_simplicial_set(hm.Knn(k, idx, dist), hm.SmoothKnn(sig, rho))  # warm
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        g = hm.fuzzy_simplicial_set(hm.Knn(k, idx, dist), hm.SmoothKnn(sig, rho))
+    e2e_s = time.perf_counter() - t0
+    same = (g.rows.size == m and np.array_equal(g.rows, rows[:m].cpu().numpy().view(np.uint32))
+            and np.array_equal(g.cols, cols[:m].cpu().numpy().view(np.uint32))
+            and np.array_equal(g.vals.view(np.uint32), vals[:m].cpu().numpy().view(np.uint32)))
+
+    # algorithmic bytes of one graph: the kNN graph and calibration read once,
+    # the COO written once
+    alg = n * k * 8 + n * 8 + m * 12 + 8
+    avg_s = total_ms / args.steps / 1e3
+    peaks = measured_peaks()
+    peak = peaks.get("hbm_gbs", 6650.0)
+    line = {
+        "metric": FUZZY_METRIC, "value": value, "unit": FUZZY_UNIT, "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic", "config": fuzzy_config(wl, m),
+        "e2e": {"value": e2e_steps / e2e_s, "unit": FUZZY_UNIT,
+                "h2d_bytes_per_step": int(n * k * 8 + n * 8), "d2h_bytes_per_step": int(m * 12 + 8),
+                "steps": e2e_steps, "matches_device_run": bool(same),
+                "api": "hm_fuzzy_graph (host arrays, one call at a time)"},
+        "gpu_launches": int(launches * args.steps),
+        "roofline": {"bound": "hbm", "kernel": "fuzzy stage (directed, radix sort, fuse, scan, scatter)",
+                     "achieved": alg / avg_s / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / avg_s / 1e9 / peak, "traffic": None,
+                     "algorithmic": f"8 n k + 8 n + 12 nnz = {alg} bytes per graph",
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else
+                                    "fallback 6.65 TB/s (of fallback)"},
+        "clocks": clk,
+        "step_ms": {"min": min(step_ms), "median": statistics.median(step_ms), "max": max(step_ms)},
+    }
+    if not args.no_cpu_baseline:
+        import holomap_oracle
+        t0 = time.perf_counter()
+        r, c, v = holomap_oracle.fuzzy_graph(idx, dist, sig, rho, k)
+        cpu_s = time.perf_counter() - t0
+        line["cpu_baseline"] = {
+            "value": 1.0 / cpu_s, "unit": FUZZY_UNIT, "cores": 1, "kind": "port",
+            "sample": "the whole graph once; C restatement of src/fuzzy.rs:25-91",
+            "same_graph": bool(r.size == m and np.array_equal(r, g.rows) and np.array_equal(c, g.cols)
+                               and np.array_equal(v.view(np.uint32), g.vals.view(np.uint32)))}
+    print(json.dumps(line), flush=True)
     return 0
 
 

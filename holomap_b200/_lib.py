@@ -188,6 +188,10 @@ SIGNATURES = {
     "hm_stats_from_workspace": (_i32, [_vp, _u64, _u32, _u32, _i32, _i32, _vp]),
     "hm_smooth_workspace_bytes": (_sz, [_u64]),
     "hm_smooth_knn_device": (_i32, [_vp, _u64, _u32, _vp, _vp, _vp, _vp]),
+    "hm_fuzzy_workspace_bytes": (_sz, [_u64, _u32]),
+    "hm_fuzzy_graph_device": (_i32, [_vp, _vp, _vp, _vp, _u64, _u32, _vp, _vp, _vp, _vp, _vp, _sz,
+                                     _vp]),
+    "hm_fuzzy_graph": (_i32, [_vp, _vp, _vp, _vp, _u64, _u32, _vp, _vp, _vp, _vp]),
     "hm_last_error": (ctypes.c_char_p, []),
     "hm_abi_version": (_i32, []),
     "hm_autotune_path": (_i32, [_u64, _u32, _u32, _i32]),
@@ -341,6 +345,41 @@ def knn_smooth(data, n_features: int, k: int, metric="euclidean", path="auto",
                               int(KnnPath.parse(path)), _ptr(idx), _ptr(dist), _ptr(sig),
                               _ptr(rho), ctypes.byref(stats) if stats is not None else None))
     return Knn(k, idx, dist), SmoothKnn(sig, rho)
+
+
+@dataclass
+class FuzzyGraph:
+    """Symmetric membership graph as COO sorted by (row, col) (src/fuzzy.rs:16-22)."""
+    n: int
+    rows: np.ndarray  # uint32
+    cols: np.ndarray  # uint32
+    vals: np.ndarray  # float32
+
+
+def fuzzy_simplicial_set(knn: Knn, calib: SmoothKnn) -> FuzzyGraph:
+    """The fuzzy simplicial set on the GPU; same entries and bits as
+    src/fuzzy.rs:25-91 (each row's kNN indices must be distinct, as
+    exact_knn returns them)."""
+    k = knn.k
+    idx = np.ascontiguousarray(np.asarray(knn.indices, dtype=np.uint32)).reshape(-1)
+    dist = np.ascontiguousarray(np.asarray(knn.dists, dtype=np.float32)).reshape(-1)
+    sig = np.ascontiguousarray(np.asarray(calib.sigmas, dtype=np.float32)).reshape(-1)
+    rho = np.ascontiguousarray(np.asarray(calib.rhos, dtype=np.float32)).reshape(-1)
+    if k <= 0 or idx.size == 0 or idx.size % k or dist.size != idx.size:
+        raise HolomapInvalidInput(HM_ERR_INVALID, "knn is not a non-empty n x k graph")
+    n = idx.size // k
+    if sig.size != n or rho.size != n:
+        raise HolomapInvalidInput(HM_ERR_INVALID, "calibration length differs from n")
+    if int(idx.max()) >= n:
+        raise HolomapInvalidInput(HM_ERR_INVALID, "a kNN index is not below n")
+    rows = np.empty(2 * n * k, dtype=np.uint32)
+    cols = np.empty(2 * n * k, dtype=np.uint32)
+    vals = np.empty(2 * n * k, dtype=np.float32)
+    nnz = ctypes.c_uint64(0)
+    check(lib().hm_fuzzy_graph(_ptr(idx), _ptr(dist), _ptr(sig), _ptr(rho), n, k, _ptr(rows),
+                               _ptr(cols), _ptr(vals), ctypes.byref(nnz)))
+    m = nnz.value
+    return FuzzyGraph(n, rows[:m].copy(), cols[:m].copy(), vals[:m].copy())
 
 
 def workspace_bytes(n: int, d: int, k: int, metric="euclidean", path="auto") -> int:

@@ -149,6 +149,28 @@ HM_API size_t hm_smooth_workspace_bytes(uint64_t n);
 HM_API int hm_smooth_knn_device(const float *d_dists, uint64_t n, uint32_t k, float *d_sigma,
                          float *d_rho, void *d_workspace, void *stream);
 
+/* The fuzzy simplicial set (replaces fuzzy_simplicial_set, src/fuzzy.rs:25-91):
+ * the kNN graph (n x k indices and distances, each row's indices distinct, as
+ * exact_knn returns them) and its calibration (sigma, rho) fused into the
+ * symmetric membership graph W = A + A^T - A o A^T in binary32, as COO sorted
+ * by (row, col) with zeros dropped; the same entries, in the same order, with
+ * the same bits as the reference.  Capacity of rows / cols / vals: 2 n k
+ * entries; *nnz receives the count.  Bits [32 + bits(n)) of a 64-bit sort key
+ * hold (row, col, direction), so 2 n k must stay below 2^31.
+ *
+ * hm_fuzzy_graph: host buffers in and out (one allocation, synchronous).
+ * hm_fuzzy_graph_device: device pointers; d_nnz is a device uint64; the
+ * workspace (hm_fuzzy_workspace_bytes, 256-byte aligned) holds the sort's
+ * buffers; ordered on `stream`, nothing synchronised. */
+HM_API size_t hm_fuzzy_workspace_bytes(uint64_t n, uint32_t k);
+HM_API int hm_fuzzy_graph_device(const uint32_t *d_idx, const float *d_dist, const float *d_sigma,
+                                 const float *d_rho, uint64_t n, uint32_t k, uint32_t *d_rows,
+                                 uint32_t *d_cols, float *d_vals, uint64_t *d_nnz, void *d_workspace,
+                                 size_t workspace_bytes, void *stream);
+HM_API int hm_fuzzy_graph(const uint32_t *idx, const float *dist, const float *sigma, const float *rho,
+                          uint64_t n, uint32_t k, uint32_t *rows_out, uint32_t *cols_out,
+                          float *vals_out, uint64_t *nnz_out);
+
 /* ----------------------------------------------------------------------------
  * Batches: many independent problems of uneven n, d, k and metric in one
  * pass of the device pipeline (every kernel works on the whole batch; the

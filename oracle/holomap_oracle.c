@@ -1,5 +1,6 @@
 /*
- * holomap_oracle.c -- CPU restatement of holomap's exact kNN + smooth-kNN path.
+ * holomap_oracle.c -- CPU restatement of holomap's exact kNN + smooth-kNN path
+ * and of the fuzzy simplicial set that consumes it.
  *
  * TEST INFRASTRUCTURE ONLY.  This file is the checker that the CUDA product is
  * compared against; it is never linked into libholomap_cuda.so and the product
@@ -18,12 +19,15 @@
  *   oracle_smooth_knn    src/smooth_knn.rs:23-80, mean :82-84
  *   oracle_expf          libm crate 0.2.16 `expf`, reached from
  *                        src/smooth_knn.rs:46 via src/fmath.rs:119-122
+ *   oracle_fuzzy_graph   src/fuzzy.rs:25-91 (t-conorm :67-75)
  *
  * Parity pins: kNN indices and distances are checked against the reference's
  * own known-answer tests (src/knn.rs:64-105, src/metric.rs:92-102) and the
  * umap-learn golden fixtures tests/fixtures/stage2_*.json (indices exact,
  * values 1e-5).  rho/sigma are pinned to 1e-5 by src/smooth_knn.rs:104-124 and
- * the same fixtures.  The libm crate's source is not available here, so
+ * the same fixtures.  The fuzzy graph is pinned by src/fuzzy.rs:97-155 and
+ * the fixtures' graph_rows / graph_cols (exact) and graph_vals (1e-5,
+ * src/fixture_parity.rs:101-117).  The libm crate's source is not available here, so
  * oracle_expf restates its published algorithm (see the comment there); the
  * bit-level identity of sigma with the Rust binary is therefore unpinned
  * beyond those 1e-5 checks.
@@ -426,4 +430,101 @@ double oracle_log2(double x) { return log2(x); }
 void oracle_expf_array(const float *x, float *y, size_t n)
 {
     for (size_t t = 0; t < n; ++t) y[t] = oracle_expf(x[t]);
+}
+
+/* -------------------------------------------------------------- fuzzy graph */
+
+typedef struct {
+    uint32_t r, c;
+    float v;
+} coo_t;
+
+static int cmp_coo(const void *x, const void *y)
+{
+    const coo_t *a = (const coo_t *)x, *b = (const coo_t *)y;
+    if (a->r != b->r) return a->r < b->r ? -1 : 1;
+    if (a->c != b->c) return a->c < b->c ? -1 : 1;
+    return 0;
+}
+
+/* Value of directed entry (r, c), 0 when absent (src/fuzzy.rs:52-57: a binary
+ * search over the (row, col)-sorted directed list). */
+static float lookup(const coo_t *dir, size_t m, uint32_t r, uint32_t c)
+{
+    size_t lo = 0, hi = m;
+    while (lo < hi) {
+        size_t mid = lo + (hi - lo) / 2;
+        if (dir[mid].r < r || (dir[mid].r == r && dir[mid].c < c)) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < m && dir[lo].r == r && dir[lo].c == c) ? dir[lo].v : 0.0f;
+}
+
+/* src/fuzzy.rs:25-91.  Directed strengths (self edges skipped,
+ * w = 1 when d - rho <= 0 or sigma == 0, else expf(-(d / sigma)), zeros
+ * dropped), sorted by (row, col); the support is the union of (r, c) and
+ * (c, r) over them, deduplicated and sorted; each support entry gets the
+ * binary32 t-conorm (v + vt) - v * vt and is kept when nonzero.  Outputs hold
+ * up to 2 n k entries; returns the entry count, or -1 on allocation failure. */
+long long oracle_fuzzy_graph(const uint32_t *idx, const float *dist, const float *sigma,
+                             const float *rho, size_t n, size_t k, uint32_t *rows_out,
+                             uint32_t *cols_out, float *vals_out)
+{
+    coo_t *dir = (coo_t *)malloc(sizeof(coo_t) * (n * k + 1));
+    coo_t *sup = (coo_t *)malloc(sizeof(coo_t) * (2 * n * k + 1));
+    if (!dir || !sup) {
+        free(dir);
+        free(sup);
+        return -1;
+    }
+    size_t m = 0;
+    for (size_t i = 0; i < n; ++i) {
+        for (size_t j = 0; j < k; ++j) {
+            uint32_t col = idx[i * k + j];
+            if ((size_t)col == i) continue;
+            volatile float d = dist[i * k + j] - rho[i];
+            float val;
+            if (d <= 0.0f || sigma[i] == 0.0f) {
+                val = 1.0f;
+            } else {
+                volatile float q = d / sigma[i];
+                val = oracle_expf(-q);
+            }
+            if (val != 0.0f) {
+                dir[m].r = (uint32_t)i;
+                dir[m].c = col;
+                dir[m].v = val;
+                ++m;
+            }
+        }
+    }
+    qsort(dir, m, sizeof(coo_t), cmp_coo);
+    size_t s = 0;
+    for (size_t e = 0; e < m; ++e) {
+        sup[s].r = dir[e].r;
+        sup[s].c = dir[e].c;
+        ++s;
+        sup[s].r = dir[e].c;
+        sup[s].c = dir[e].r;
+        ++s;
+    }
+    qsort(sup, s, sizeof(coo_t), cmp_coo);
+    long long out = 0;
+    for (size_t e = 0; e < s; ++e) {
+        if (e > 0 && sup[e].r == sup[e - 1].r && sup[e].c == sup[e - 1].c) continue;  /* dedup */
+        float v = lookup(dir, m, sup[e].r, sup[e].c);
+        float vt = lookup(dir, m, sup[e].c, sup[e].r);
+        volatile float sum = v + vt;
+        volatile float prod = v * vt;
+        float w = sum - prod;
+        if (w != 0.0f) {
+            rows_out[out] = sup[e].r;
+            cols_out[out] = sup[e].c;
+            vals_out[out] = w;
+            ++out;
+        }
+    }
+    free(dir);
+    free(sup);
+    return out;
 }

@@ -70,6 +70,8 @@ def lib() -> ctypes.CDLL:
         L.oracle_mean.restype = ctypes.c_float
         L.oracle_expf_array.argtypes = [fp, fp, sz]
         L.oracle_expf_array.restype = None
+        L.oracle_fuzzy_graph.argtypes = [u32p, fp, fp, fp, sz, sz, u32p, u32p, fp]
+        L.oracle_fuzzy_graph.restype = ctypes.c_longlong
         L.oracle_log2.argtypes = [ctypes.c_double]
         L.oracle_log2.restype = ctypes.c_double
         _lib = L
@@ -144,3 +146,23 @@ def expf(x) -> np.ndarray:
     y = np.empty_like(x)
     lib().oracle_expf_array(_ptr(x), _ptr(y), x.size)
     return y
+
+
+def fuzzy_graph(indices: np.ndarray, dists: np.ndarray, sigmas: np.ndarray, rhos: np.ndarray,
+                k: int):
+    """src/fuzzy.rs:25-91: (rows uint32, cols uint32, vals float32), COO sorted
+    by (row, col)."""
+    idx = np.ascontiguousarray(indices, dtype=np.uint32).reshape(-1)
+    dd = np.ascontiguousarray(dists, dtype=np.float32).reshape(-1)
+    sg = np.ascontiguousarray(sigmas, dtype=np.float32).reshape(-1)
+    rh = np.ascontiguousarray(rhos, dtype=np.float32).reshape(-1)
+    n = idx.size // k
+    cap = 2 * n * k
+    rows = np.empty(cap, dtype=np.uint32)
+    cols = np.empty(cap, dtype=np.uint32)
+    vals = np.empty(cap, dtype=np.float32)
+    m = lib().oracle_fuzzy_graph(_ptr(idx), _ptr(dd), _ptr(sg), _ptr(rh), n, k, _ptr(rows),
+                                 _ptr(cols), _ptr(vals))
+    if m < 0:
+        raise MemoryError("oracle_fuzzy_graph")
+    return rows[:m].copy(), cols[:m].copy(), vals[:m].copy()

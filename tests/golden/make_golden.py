@@ -4,9 +4,11 @@ The reference (mnmal-ai/holomap) pins its kNN and smooth-kNN stages against
 umap-learn 0.5.12 fixtures, tests/fixtures/stage2_{blobs_euclidean,cosine,
 duplicates_euclidean}.json, produced by its dev/export_stage2_fixtures.py and
 asserted in src/fixture_parity.rs:42-99 (kNN indices exact; distances, rho and
-sigma within 1e-5 * (1 + |expected|)).  This script copies the keys that the
-kNN + smooth-kNN path consumes or produces (data, knn_indices, knn_dists,
-rhos, sigmas and the shape/metric header) so the tests can run where the
+sigma within 1e-5 * (1 + |expected|)) and its fuzzy graph at :101-117
+(support exact, weights within the same tolerance).  This script copies the
+keys that the kNN + smooth-kNN path and the fuzzy graph consume or produce
+(data, knn_indices, knn_dists, rhos, sigmas, graph_rows, graph_cols,
+graph_vals and the shape/metric header) so the tests can run where the
 reference checkout is absent.  Run it from the repository root with the
 reference checkout path as its only argument:
 
@@ -18,7 +20,7 @@ from pathlib import Path
 
 NAMES = ("blobs_euclidean", "cosine", "duplicates_euclidean")
 KEYS = ("name", "metric", "n_neighbors", "n_samples", "n_features", "data",
-        "knn_indices", "knn_dists", "rhos", "sigmas")
+        "knn_indices", "knn_dists", "rhos", "sigmas", "graph_rows", "graph_cols", "graph_vals")
 
 
 def main(ref_root: str) -> None:

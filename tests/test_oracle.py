@@ -1,8 +1,10 @@
-"""The oracle (C restatement of the reference's kNN + smooth-kNN path) pinned
-against the reference's own known-answer tests and golden fixtures.
+"""The oracle (C restatement of the reference's kNN, smooth-kNN and fuzzy graph
+path) pinned against the reference's own known-answer tests and golden
+fixtures.
 
 Ports the *assertions* of src/knn.rs:64-105, src/metric.rs:92-102,
-src/smooth_knn.rs:104-124 and src/fixture_parity.rs:42-99."""
+src/smooth_knn.rs:104-124, src/fuzzy.rs:97-155 and
+src/fixture_parity.rs:42-117."""
 import json
 import math
 from pathlib import Path
@@ -106,7 +108,34 @@ def test_all_zero_distances_yield_unit_sigma(oracle):
     assert sig.tolist() == [1.0, 1.0]
 
 
-# --- golden fixtures (src/fixture_parity.rs:42-99) --------------------------
+# --- src/fuzzy.rs tests -----------------------------------------------------
+
+def test_fuzzy_line_points_symmetrized_sorted_no_self_edges(oracle):
+    # src/fuzzy.rs:97-129: 3 line points, k = 3
+    idx = np.array([0, 1, 2, 1, 0, 2, 2, 1, 0], dtype=np.uint32)
+    dists = f32([0.0, 1.0, 3.0, 0.0, 1.0, 2.0, 0.0, 2.0, 3.0])
+    sig = f32([3.72998046875, 1.864990234375, 1.864990234375])
+    rho = f32([1.0, 1.0, 2.0])
+    rows, cols, vals = oracle.fuzzy_graph(idx, dists, sig, rho, 3)
+    w = oracle.expf(f32([-2.0 / 3.72998046875]))[0]
+    fused = np.float32(np.float32(w + w) - np.float32(w * w))
+    assert rows.tolist() == [0, 0, 1, 1, 2, 2]
+    assert cols.tolist() == [1, 2, 0, 2, 0, 1]
+    np.testing.assert_allclose(vals, [1.0, fused, 1.0, 1.0, fused, 1.0], atol=1e-6, rtol=0)
+
+
+def test_fuzzy_one_directional_edge_becomes_symmetric(oracle):
+    # src/fuzzy.rs:131-155
+    idx = np.array([0, 1, 1, 2, 2, 1], dtype=np.uint32)
+    dists = f32([0.0, 1.0, 0.0, 0.1, 0.0, 0.1])
+    rows, cols, vals = oracle.fuzzy_graph(idx, dists, f32([1.0, 1.0, 1.0]), f32([0.5, 0.1, 0.1]), 2)
+    w = oracle.expf(f32([-0.5]))[0]
+    assert rows.tolist() == [0, 1, 1, 2]
+    assert cols.tolist() == [1, 0, 2, 1]
+    assert vals.tolist() == [w, w, 1.0, 1.0]
+
+
+# --- golden fixtures (src/fixture_parity.rs:42-117) -------------------------
 
 def close(actual, expected):
     expected = np.asarray(expected, dtype=np.float64)
@@ -125,6 +154,11 @@ def test_oracle_matches_golden_fixture(oracle, name):
     sig, rho = oracle.smooth_knn(dist, k)
     assert close(rho, fx["rhos"]).all()
     assert close(sig, fx["sigmas"]).all()
+    # src/fixture_parity.rs:101-117: graph support exact, weights to tolerance
+    rows, cols, vals = oracle.fuzzy_graph(idx, dist, sig, rho, k)
+    assert rows.tolist() == fx["graph_rows"]
+    assert cols.tolist() == fx["graph_cols"]
+    assert close(vals, fx["graph_vals"]).all()
 
 
 # --- expf restatement -------------------------------------------------------
