@@ -2,20 +2,37 @@
 // the symmetrized membership graph that consumes the kNN graph and its
 // calibration, as COO sorted by (row, col).
 //
-// Directed strengths A[i][col] (self edges skipped; 1 when d - rho <= 0 or
-// sigma == 0, else libm expf(-(d / sigma)); zeros dropped) are written twice:
-// the forward entry (i, col) into the first half of one key array and the
-// reverse entry (col, i) into the second half, keyed row << b | col with b
-// the bit width of n - 1 (32-bit keys while 2b <= 32, that is n <= 65536,
-// else 64-bit).  The weight's bits are the value, its sign bit (free: a
-// weight is in (0, 1]) marking the reverse entry; absent entries carry the
-// all-ones key, which no off-diagonal coordinate can equal.  One stable radix
-// sort over the 2b key bits orders the entries by (row, col); a coordinate
-// holds at most one forward and one reverse entry (each row's indices are
-// distinct).  The first entry of every coordinate forms the binary32
-// t-conorm (v + vt) - v * vt as the reference does (src/fuzzy.rs:67-75), and
-// a scan compacts the nonzero results.  Every step is a function of the
-// inputs alone: the output is the reference's, entry for entry.
+// Row r of the output is the sorted union of two lists: F_r, the columns of
+// row r's own kNN list with a nonzero directed strength A[r][c], and R_r,
+// the rows s whose lists hold r with A[s][r] nonzero.  Each is a set (the
+// indices of a row are distinct), so
+//
+//   1. fuzzy_rows_kernel (one warp per row) computes the strengths (self
+//      skipped; 1 when d - rho <= 0 or sigma == 0, else libm expf(-(d /
+//      sigma)); zeros dropped), orders F_r by rank (the count of smaller
+//      columns), and writes each entry's reverse copy as (key col, value e)
+//      with e its position in the kNN arrays; dropped entries get the key n.
+//   2. A stable radix sort of the reverse copies over the bits of n groups
+//      them by column with ascending e, so each R_r comes out sorted by
+//      source row (CUB onesweep).
+//   3. fuzzy_merge_kernel (one warp per row) binary-searches every element
+//      of F_r in R_r: it finds the partner strength A[c][r], forms the
+//      binary32 t-conorm (v + vt) - v * vt in the reference's order
+//      (src/fuzzy.rs:67-75), and places the element at j + lb - dups_below
+//      (F elements below it, R elements below it, minus those counted in
+//      both).  The row's entry count |F_r| + |R_r| - |F_r and R_r| goes
+//      through an exclusive scan (CUB) to row offsets.
+//   4. fuzzy_write_kernel writes the F elements at their places and every R
+//      element without an F partner at u + lb_F - dups_below (the same rule
+//      seen from the other list), with strength (0 + vt) - 0 * vt.
+//
+// Strengths lie in [0, 1] (or are NaN) when every sigma is non-negative, and
+// then no fused value of a union coordinate is zero: fl(v * vt) <= min(v,
+// vt) <= max(v, vt) <= fl(v + vt) with one of the inequalities strict, so
+// the difference is positive.  The reference's zero filter after the fusion
+// therefore drops nothing and the union size is the entry count.  Every
+// step is a function of the inputs alone: the output is the reference's,
+// entry for entry.
 #include <cub/cub.cuh>
 #include <cuda_runtime.h>
 
@@ -24,163 +41,205 @@
 
 namespace hm {
 
-constexpr uint32_t FZ_REVERSE = 0x80000000u;
+constexpr unsigned FZ_FULL = 0xffffffffu;
 
-template <typename Key>
-__global__ void fuzzy_directed_kernel(const uint32_t *__restrict__ idx, const float *__restrict__ dist,
-                                      const float *__restrict__ sigma, const float *__restrict__ rho,
-                                      uint64_t n, uint32_t k, uint32_t b, Key *__restrict__ keys,
-                                      uint32_t *__restrict__ vals) {
-    const uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t entries = n * k;
-    if (e >= entries) return;
-    const uint64_t i = e / k;
-    const uint32_t col = idx[e];
-    Key fk = ~Key(0), rk = ~Key(0);
-    uint32_t vb = 0;
-    if ((uint64_t)col != i) {
-        const float d = __fsub_rn(dist[e], rho[i]);
-        const float s = sigma[i];
-        const float w = (d <= 0.0f || s == 0.0f) ? 1.0f : expf_libm(-__fdiv_rn(d, s));
-        if (w != 0.0f) {
-            fk = (Key(i) << b) | Key(col);
-            rk = (Key(col) << b) | Key(i);
-            vb = __float_as_uint(w);
-        }
-    }
-    keys[e] = fk;
-    keys[entries + e] = rk;
-    vals[e] = vb;
-    vals[entries + e] = vb | FZ_REVERSE;
+__device__ __forceinline__ float tconorm(float v, float vt) {
+    return __fsub_rn(__fadd_rn(v, vt), __fmul_rn(v, vt));
 }
 
-// flag[p] = 1 for the first entry of each coordinate whose t-conorm is
-// nonzero; its weight goes to w[p]
-template <typename Key>
-__global__ void fuzzy_fuse_kernel(const Key *__restrict__ keys, const uint32_t *__restrict__ vals, uint64_t total,
-                                  uint32_t *__restrict__ flag, float *__restrict__ w) {
-    const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= total) return;
-    const Key key = keys[p];
-    uint32_t keep = 0;
-    float out = 0.0f;
-    if (key != ~Key(0) && (p == 0 || keys[p - 1] != key)) {
+__global__ void __launch_bounds__(256) fuzzy_rows_kernel(
+    const uint32_t *__restrict__ idx, const float *__restrict__ dist, const float *__restrict__ sigma,
+    const float *__restrict__ rho, uint32_t n, uint32_t k, float *__restrict__ wdir, uint32_t *__restrict__ rkey,
+    uint32_t *__restrict__ rval, uint32_t *__restrict__ fcol, float *__restrict__ fw,
+    uint32_t *__restrict__ fcount) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (r >= n) return;  // whole warps
+    const uint64_t base = r * k;
+    const float rh = rho[r], sg = sigma[r];
+    uint32_t cnt = 0;
+    for (uint32_t j0 = 0; j0 < k; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        bool valid = false;
+        if (j < k) {
+            const uint32_t col = idx[base + j];
+            float w = 0.0f;
+            if ((uint64_t)col != r) {
+                const float d = __fsub_rn(dist[base + j], rh);
+                w = (d <= 0.0f || sg == 0.0f) ? 1.0f : expf_libm(-__fdiv_rn(d, sg));
+                valid = w != 0.0f;
+            }
+            wdir[base + j] = w;
+            rkey[base + j] = valid ? col : n;
+            rval[base + j] = (uint32_t)(base + j);
+        }
+        cnt += __popc(__ballot_sync(FZ_FULL, valid));
+    }
+    __syncwarp();
+    // rank of each valid column among the row's valid columns (dropped
+    // entries carry the key n, above every column)
+    for (uint32_t j0 = 0; j0 < k; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        const uint32_t mine = j < k ? rkey[base + j] : n;
+        uint32_t rank = 0;
+        for (uint32_t c0 = 0; c0 < k; c0 += 32) {
+            const uint32_t other = c0 + lane < k ? rkey[base + c0 + lane] : n;
+#pragma unroll
+            for (int s = 0; s < 32; ++s) rank += __shfl_sync(FZ_FULL, other, s) < mine ? 1u : 0u;
+        }
+        if (mine < n) {
+            fcol[base + rank] = mine;
+            fw[base + rank] = wdir[base + j];
+        }
+    }
+    if (lane == 0) fcount[r] = cnt;
+}
+
+// first position in [lo, hi) of the sorted array a whose value is >= x
+__device__ __forceinline__ uint32_t lower_bound_u32(const uint32_t *__restrict__ a, uint32_t lo, uint32_t hi,
+                                                    uint32_t x) {
+    while (lo < hi) {
+        const uint32_t mid = lo + ((hi - lo) >> 1);
+        if (a[mid] < x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(256) fuzzy_merge_kernel(
+    const uint32_t *__restrict__ skey, const uint32_t *__restrict__ sval, const float *__restrict__ wdir,
+    uint32_t entries, uint32_t n, uint32_t k, const uint32_t *__restrict__ fcol, float *__restrict__ fw,
+    const uint32_t *__restrict__ fcount, uint32_t *__restrict__ fpos, uint32_t *__restrict__ dpre,
+    uint32_t *__restrict__ rstart, uint32_t *__restrict__ rdups, uint32_t *__restrict__ count) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (r >= n) return;  // whole warps
+    const uint64_t base = r * k;
+    uint32_t b = 0;
+    if (lane < 2) b = lower_bound_u32(skey, 0, entries, (uint32_t)r + lane);
+    const uint32_t start = __shfl_sync(FZ_FULL, b, 0), end = __shfl_sync(FZ_FULL, b, 1);
+    const uint32_t fc = fcount[r];
+    uint32_t dups = 0;
+    for (uint32_t j0 = 0; j0 < fc; j0 += 32) {
+        const uint32_t j = j0 + lane;
+        bool found = false;
+        uint32_t lb = 0;
         float v = 0.0f, vt = 0.0f;
-        const uint32_t a = vals[p];
-        (a & FZ_REVERSE ? vt : v) = __uint_as_float(a & ~FZ_REVERSE);
-        if (p + 1 < total && keys[p + 1] == key) {
-            const uint32_t c = vals[p + 1];
-            (c & FZ_REVERSE ? vt : v) = __uint_as_float(c & ~FZ_REVERSE);
+        if (j < fc) {
+            const uint32_t f = fcol[base + j];
+            // R_r is sorted by source row sval / k
+            uint32_t lo = start, hi = end;
+            while (lo < hi) {
+                const uint32_t mid = lo + ((hi - lo) >> 1);
+                if (sval[mid] / k < f) lo = mid + 1;
+                else hi = mid;
+            }
+            found = lo < end && sval[lo] / k == f;
+            lb = lo - start;
+            v = fw[base + j];
+            if (found) vt = wdir[sval[lo]];
         }
-        out = __fsub_rn(__fadd_rn(v, vt), __fmul_rn(v, vt));
-        keep = out != 0.0f ? 1u : 0u;
+        const unsigned ball = __ballot_sync(FZ_FULL, found);
+        const uint32_t before = dups + __popc(ball & ((1u << lane) - 1u));
+        if (j < fc) {
+            fpos[base + j] = j + lb - before;
+            dpre[base + j] = before;
+            fw[base + j] = tconorm(v, vt);
+        }
+        dups += __popc(ball);
     }
-    flag[p] = keep;
-    w[p] = out;
+    if (lane == 0) {
+        rstart[r] = start;
+        rdups[r] = dups;
+        count[r] = fc + (end - start) - dups;
+    }
 }
 
-template <typename Key>
-__global__ void fuzzy_scatter_kernel(const Key *__restrict__ keys, const uint32_t *__restrict__ flag,
-                                     const uint32_t *__restrict__ pos, const float *__restrict__ w, uint64_t total,
-                                     uint32_t b, uint32_t *__restrict__ rows, uint32_t *__restrict__ cols,
-                                     float *__restrict__ outv, unsigned long long *__restrict__ nnz) {
+__global__ void __launch_bounds__(256) fuzzy_write_kernel(
+    const uint32_t *__restrict__ skey, const uint32_t *__restrict__ sval, const float *__restrict__ wdir,
+    uint32_t n, uint32_t k, const uint32_t *__restrict__ fcol, const float *__restrict__ fval,
+    const uint32_t *__restrict__ fcount, const uint32_t *__restrict__ fpos, const uint32_t *__restrict__ dpre,
+    const uint32_t *__restrict__ rstart, const uint32_t *__restrict__ rdups, const uint32_t *__restrict__ count,
+    const uint32_t *__restrict__ off, uint32_t *__restrict__ rows, uint32_t *__restrict__ cols,
+    float *__restrict__ vals, unsigned long long *__restrict__ nnz) {
+    const uint64_t entries = (uint64_t)n * k;
     const uint64_t p = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (p >= total) return;
-    if (flag[p]) {
-        const Key key = keys[p];
-        const uint32_t q = pos[p];
-        rows[q] = (uint32_t)(key >> b);
-        cols[q] = (uint32_t)(key & ((Key(1) << b) - 1));
-        outv[q] = w[p];
+    if (p == 0) *nnz = (unsigned long long)off[n - 1] + count[n - 1];
+    if (p < entries) {  // F element j of row r
+        const uint32_t r = (uint32_t)(p / k), j = (uint32_t)(p - (uint64_t)r * k);
+        if (j < fcount[r]) {
+            const uint32_t q = off[r] + fpos[p];
+            rows[q] = r;
+            cols[q] = fcol[p];
+            vals[q] = fval[p];
+        }
+    } else if (p < 2 * entries) {  // reverse copy t, an element of R_r
+        const uint32_t t = (uint32_t)(p - entries);
+        const uint32_t r = skey[t];
+        if (r >= n) return;  // dropped entry
+        const uint32_t e = sval[t];
+        const uint32_t s = e / k;
+        const uint64_t base = (uint64_t)r * k;
+        const uint32_t fc = fcount[r];
+        const uint32_t lbf = lower_bound_u32(fcol + base, 0, fc, s);
+        if (lbf < fc && fcol[base + lbf] == s) return;  // written with its F partner
+        // F elements below s that also lie in R_r
+        const uint32_t dup_below = lbf < fc ? dpre[base + lbf] : rdups[r];
+        const uint32_t q = off[r] + (t - rstart[r]) + lbf - dup_below;
+        rows[q] = r;
+        cols[q] = s;
+        vals[q] = tconorm(0.0f, wdir[e]);
     }
-    if (p == total - 1) *nnz = (unsigned long long)pos[p] + flag[p];
 }
 
-// bit width of the largest index n - 1 (at least 1)
-static uint32_t index_bits(uint64_t n) {
-    uint32_t b = 1;
-    while (b < 63 && (1ull << b) < n) ++b;
+// bits that hold every value 0..n (the key n marks a dropped entry)
+static int key_bits(uint64_t n) {
+    int b = 1;
+    while (b < 32 && (1ull << b) <= n) ++b;
     return b;
 }
 
-// Workspace: keys and values (double-buffered for the sort), flags,
-// positions, fused weights, and CUB's temporary storage.
+// Workspace: the directed strengths, the reverse copies (double-buffered
+// for the sort), the ordered F lists and their merge results, per-row
+// counters, and CUB's temporary storage.
 struct FuzzyLayout {
-    size_t keys0, keys1, vals0, vals1, flag, pos, w, temp, temp_bytes, total;
-    uint32_t b;
-    bool wide;  // 64-bit keys
+    size_t wdir, rk0, rk1, rv0, rv1, fcol, fw, fpos, dpre, fcount, rstart, rdups, count, off, temp, temp_bytes,
+        total;
 };
 
-template <typename Key>
-static int fuzzy_temp_bytes(uint64_t total, size_t *bytes) {
-    size_t sort_bytes = 0, scan_bytes = 0;
-    cub::DoubleBuffer<Key> kb(nullptr, nullptr);
-    cub::DoubleBuffer<uint32_t> vb(nullptr, nullptr);
-    HM_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, kb, vb, (int)total));
-    HM_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (uint32_t *)nullptr, (uint32_t *)nullptr,
-                                              (int)total));
-    *bytes = std::max(sort_bytes, scan_bytes);
-    return HM_OK;
-}
-
 static int fuzzy_layout(uint64_t n, uint32_t k, FuzzyLayout *L) {
-    const uint64_t total = 2 * n * k;
-    if (n > 0x7fffffffull || total >= 0x7fffffffull) return set_error(HM_ERR_UNSUPPORTED, "2 n k above 2^31 entries");
-    L->b = index_bits(n);
-    L->wide = 2 * L->b > 32;
-    const size_t kbytes = L->wide ? 8 : 4;
-    HM_TRY(L->wide ? fuzzy_temp_bytes<unsigned long long>(total, &L->temp_bytes)
-                   : fuzzy_temp_bytes<uint32_t>(total, &L->temp_bytes));
-    size_t off = 0;
+    const uint64_t entries = n * k;
+    if (n >= 0x7fffffffull || entries > 0x7fffffffull)
+        return set_error(HM_ERR_UNSUPPORTED, "n k above 2^31 - 1 entries");
+    size_t sort_bytes = 0, scan_bytes = 0;
+    cub::DoubleBuffer<uint32_t> kb(nullptr, nullptr), vb(nullptr, nullptr);
+    HM_CUDA_TRY(cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, kb, vb, (int)entries));
+    HM_CUDA_TRY(cub::DeviceScan::ExclusiveSum(nullptr, scan_bytes, (uint32_t *)nullptr, (uint32_t *)nullptr,
+                                              (int)n));
+    size_t at = 0;
     auto take = [&](size_t bytes) {
-        const size_t at = off;
-        off = round_up(off + std::max<size_t>(bytes, 1), 256);
-        return at;
+        const size_t here = at;
+        at = round_up(at + std::max<size_t>(bytes, 1), 256);
+        return here;
     };
-    L->keys0 = take(total * kbytes);
-    L->keys1 = take(total * kbytes);
-    L->vals0 = take(total * 4);
-    L->vals1 = take(total * 4);
-    L->flag = take(total * 4);
-    L->pos = take(total * 4);
-    L->w = take(total * 4);
+    const size_t e4 = entries * 4, n4 = n * 4;
+    L->wdir = take(e4);
+    L->rk0 = take(e4);
+    L->rk1 = take(e4);
+    L->rv0 = take(e4);
+    L->rv1 = take(e4);
+    L->fcol = take(e4);
+    L->fw = take(e4);
+    L->fpos = take(e4);
+    L->dpre = take(e4);
+    L->fcount = take(n4);
+    L->rstart = take(n4);
+    L->rdups = take(n4);
+    L->count = take(n4);
+    L->off = take(n4);
+    L->temp_bytes = std::max(sort_bytes, scan_bytes);
     L->temp = take(L->temp_bytes);
-    L->total = off;
-    return HM_OK;
-}
-
-template <typename Key>
-static int fuzzy_run(const FuzzyLayout &L, const uint32_t *d_idx, const float *d_dist, const float *d_sigma,
-                     const float *d_rho, uint64_t n, uint32_t k, uint32_t *d_rows, uint32_t *d_cols, float *d_vals,
-                     unsigned long long *d_nnz, char *ws, cudaStream_t s) {
-    auto *k0 = reinterpret_cast<Key *>(ws + L.keys0);
-    auto *k1 = reinterpret_cast<Key *>(ws + L.keys1);
-    auto *v0 = reinterpret_cast<uint32_t *>(ws + L.vals0);
-    auto *v1 = reinterpret_cast<uint32_t *>(ws + L.vals1);
-    auto *flag = reinterpret_cast<uint32_t *>(ws + L.flag);
-    auto *pos = reinterpret_cast<uint32_t *>(ws + L.pos);
-    auto *w = reinterpret_cast<float *>(ws + L.w);
-    const uint64_t entries = n * k, total = 2 * entries;
-    fuzzy_directed_kernel<Key><<<(unsigned)((entries + 255) / 256), 256, 0, s>>>(d_idx, d_dist, d_sigma, d_rho, n,
-                                                                                 k, L.b, k0, v0);
-    HM_CUDA_TRY(cudaGetLastError());
-    count_launch();
-    cub::DoubleBuffer<Key> kb(k0, k1);
-    cub::DoubleBuffer<uint32_t> vb(v0, v1);
-    size_t temp_bytes = L.temp_bytes;
-    HM_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ws + L.temp, temp_bytes, kb, vb, (int)total, 0, (int)(2 * L.b), s));
-    count_launch();
-    fuzzy_fuse_kernel<Key><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(kb.Current(), vb.Current(), total, flag,
-                                                                            w);
-    HM_CUDA_TRY(cudaGetLastError());
-    count_launch();
-    temp_bytes = L.temp_bytes;
-    HM_CUDA_TRY(cub::DeviceScan::ExclusiveSum(ws + L.temp, temp_bytes, flag, pos, (int)total, s));
-    count_launch();
-    fuzzy_scatter_kernel<Key><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(kb.Current(), flag, pos, w, total, L.b,
-                                                                               d_rows, d_cols, d_vals, d_nnz);
-    HM_CUDA_TRY(cudaGetLastError());
-    count_launch();
+    L->total = at;
     return HM_OK;
 }
 
@@ -216,10 +275,33 @@ int hm_fuzzy_graph_device(const uint32_t *d_idx, const float *d_dist, const floa
         return set_error(HM_ERR_INVALID, "workspace must be 256-byte aligned");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     char *ws = static_cast<char *>(d_workspace);
-    auto *nnz = reinterpret_cast<unsigned long long *>(d_nnz);
-    return L.wide ? fuzzy_run<unsigned long long>(L, d_idx, d_dist, d_sigma, d_rho, n, k, d_rows, d_cols, d_vals,
-                                                  nnz, ws, s)
-                  : fuzzy_run<uint32_t>(L, d_idx, d_dist, d_sigma, d_rho, n, k, d_rows, d_cols, d_vals, nnz, ws, s);
+    auto u32 = [&](size_t o) { return reinterpret_cast<uint32_t *>(ws + o); };
+    auto f32 = [&](size_t o) { return reinterpret_cast<float *>(ws + o); };
+    const uint32_t nn = (uint32_t)n, entries = (uint32_t)(n * k);
+    const unsigned warp_blocks = (unsigned)((n * 32 + 255) / 256);
+    fuzzy_rows_kernel<<<warp_blocks, 256, 0, s>>>(d_idx, d_dist, d_sigma, d_rho, nn, k, f32(L.wdir), u32(L.rk0),
+                                                  u32(L.rv0), u32(L.fcol), f32(L.fw), u32(L.fcount));
+    HM_CUDA_TRY(cudaGetLastError());
+    count_launch();
+    cub::DoubleBuffer<uint32_t> kb(u32(L.rk0), u32(L.rk1)), vb(u32(L.rv0), u32(L.rv1));
+    size_t temp_bytes = L.temp_bytes;
+    HM_CUDA_TRY(cub::DeviceRadixSort::SortPairs(ws + L.temp, temp_bytes, kb, vb, (int)entries, 0, key_bits(n), s));
+    count_launch();
+    fuzzy_merge_kernel<<<warp_blocks, 256, 0, s>>>(kb.Current(), vb.Current(), f32(L.wdir), entries, nn, k,
+                                                   u32(L.fcol), f32(L.fw), u32(L.fcount), u32(L.fpos), u32(L.dpre),
+                                                   u32(L.rstart), u32(L.rdups), u32(L.count));
+    HM_CUDA_TRY(cudaGetLastError());
+    count_launch();
+    temp_bytes = L.temp_bytes;
+    HM_CUDA_TRY(cub::DeviceScan::ExclusiveSum(ws + L.temp, temp_bytes, u32(L.count), u32(L.off), (int)n, s));
+    count_launch();
+    fuzzy_write_kernel<<<(unsigned)((2ull * entries + 255) / 256), 256, 0, s>>>(
+        kb.Current(), vb.Current(), f32(L.wdir), nn, k, u32(L.fcol), f32(L.fw), u32(L.fcount), u32(L.fpos),
+        u32(L.dpre), u32(L.rstart), u32(L.rdups), u32(L.count), u32(L.off), d_rows, d_cols, d_vals,
+        reinterpret_cast<unsigned long long *>(d_nnz));
+    HM_CUDA_TRY(cudaGetLastError());
+    count_launch();
+    return HM_OK;
 }
 
 int hm_fuzzy_graph(const uint32_t *idx, const float *dist, const float *sigma, const float *rho, uint64_t n,
@@ -232,6 +314,8 @@ int hm_fuzzy_graph(const uint32_t *idx, const float *dist, const float *sigma, c
     for (uint64_t j = 0; j < e; ++j)
         if (idx[j] >= n) return set_error(HM_ERR_INVALID, "kNN index %u at entry %llu is not below n", idx[j],
                                           (unsigned long long)j);
+    for (uint64_t i = 0; i < n; ++i)
+        if (sigma[i] < 0.0f) return set_error(HM_ERR_INVALID, "sigma[%llu] is negative", (unsigned long long)i);
     FuzzyLayout L;
     HM_TRY(fuzzy_layout(n, k, &L));
     const size_t ws = L.total;

@@ -1,6 +1,7 @@
 /*
  * holomap_cuda.h -- C ABI of libholomap_cuda.so, the B200 (sm_100a) exact kNN +
- * smooth-kNN engine for holomap.
+ * smooth-kNN engine for holomap, with the fuzzy simplicial set that follows
+ * them (hm_fuzzy_graph*, src/fuzzy.rs:25-91, called at src/api.rs:149).
  *
  * The reference has no FFI on this path: its "operator API" is two
  * crate-private Rust calls made back to back by Holomap::fit_transform,
@@ -154,9 +155,10 @@ HM_API int hm_smooth_knn_device(const float *d_dists, uint64_t n, uint32_t k, fl
  * exact_knn returns them) and its calibration (sigma, rho) fused into the
  * symmetric membership graph W = A + A^T - A o A^T in binary32, as COO sorted
  * by (row, col) with zeros dropped; the same entries, in the same order, with
- * the same bits as the reference.  Capacity of rows / cols / vals: 2 n k
- * entries; *nnz receives the count.  Bits [32 + bits(n)) of a 64-bit sort key
- * hold (row, col, direction), so 2 n k must stay below 2^31.
+ * the same bits as the reference.  Every sigma must be non-negative, as
+ * smooth-kNN returns it (the host entry point checks this and the index
+ * bound).  Capacity of rows / cols / vals: 2 n k entries; *nnz receives the
+ * count.  n k must stay below 2^31.
  *
  * hm_fuzzy_graph: host buffers in and out (one allocation, synchronous).
  * hm_fuzzy_graph_device: device pointers; d_nnz is a device uint64; the

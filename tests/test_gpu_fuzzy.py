@@ -84,11 +84,11 @@ def test_after_knn_edge_cases(oracle, kind, metric):
     check(oracle, knn.indices, knn.dists, sm.sigmas, sm.rhos, 15)
 
 
-@pytest.mark.parametrize("n,k", [(1, 1), (2, 2), (5, 5), (300, 1), (3000, 7), (65536, 4),
-                                 (65537, 4), (200000, 15)])
+@pytest.mark.parametrize("n,k", [(1, 1), (2, 2), (5, 5), (300, 1), (3000, 7), (65535, 4),
+                                 (65536, 4), (200000, 15)])
 def test_random_graphs(oracle, n, k):
-    # 65536 is the last size with 32-bit sort keys, 65537 the first with
-    # 64-bit ones
+    # the reverse copies are sorted on the bits of n: 16 up to n = 65535, 17
+    # (a third radix pass) from n = 65536
     if k > n:
         pytest.skip("k above n")
     idx, dist = random_knn(n, k, seed=n + k) if k > 1 else (np.arange(n, dtype=np.uint32),
@@ -117,6 +117,22 @@ def test_special_calibrations(oracle):
     d2[5::17, 1:] = rho[5::17, None] + np.float32(95.0) * sig[5::17, None]
     d2[3::19, k - 1] = np.inf
     check(oracle, idx, dist, sig, rho, k)
+
+
+def test_hub_rows(oracle):
+    """Every row lists the same first points, so their reverse lists hold all
+    n rows (in-degree n), next to rows of in-degree 0."""
+    n, k = 5000, 6
+    idx = np.empty((n, k), dtype=np.uint32)
+    idx[:, 0] = np.arange(n)
+    for r in range(n):
+        others = [c for c in range(k + 1) if c != r][: k - 1]
+        idx[r, 1:] = others
+    dist = np.zeros((n, k), dtype=np.float32)
+    dist[:, 1:] = np.linspace(0.5, 2.0, k - 1, dtype=np.float32)
+    sm = hm.smooth_knn(dist.reshape(-1), k)
+    g = check(oracle, idx.reshape(-1), dist.reshape(-1), sm.sigmas, sm.rhos, k)
+    assert (g.rows == 0).sum() == n - 1
 
 
 def test_device_entry_point_on_a_stream(oracle):
