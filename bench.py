@@ -10,12 +10,14 @@ collective is on the data path).
     python bench.py [--gpus N --steps K --warmup W] [--workload W] [--path P]
     python bench.py --impl reference ...   # the reference algorithm on host cores
     python bench.py --workload fuzzy_50k   # the fuzzy simplicial set of that graph
+    python bench.py --workload spectral_50k   # Laplacian + Lanczos eigenpairs of it
 
 Prints one JSON line (rank 0).
 """
 from __future__ import annotations
 
 import argparse
+import ctypes
 import csv
 import datetime
 import io
@@ -48,7 +50,7 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="embed_50k",
                     choices=["embed_50k", "dups_20k", "blobs_1k", "batch_256", "serve_2000",
-                             "fuzzy_50k"])
+                             "fuzzy_50k", "spectral_50k"])
     ap.add_argument("--path", default="auto")
     ap.add_argument("--rows", type=int, default=None,
                     help="use only the first ROWS points of the workload (a smaller case "
@@ -171,6 +173,8 @@ def reference_arm(args):
     threads = os.cpu_count() or 1
     if args.workload == "fuzzy_50k":
         return fuzzy_reference_arm(args)
+    if args.workload == "spectral_50k":
+        return spectral_reference_arm(args)
     if args.workload in ("batch_256", "serve_2000"):
         if args.workload == "batch_256":
             from holomap_b200.synth import batch_256
@@ -565,6 +569,8 @@ def main():
         return serve_main(args)
     if args.workload == "fuzzy_50k":
         return fuzzy_main(args)
+    if args.workload == "spectral_50k":
+        return spectral_main(args)
 
     import torch
     import torch.distributed as dist
@@ -870,6 +876,189 @@ def fuzzy_main(args) -> int:
             "sample": "the whole graph once; C restatement of src/fuzzy.rs:25-91",
             "same_graph": bool(r.size == m and np.array_equal(r, g.rows) and np.array_equal(c, g.cols)
                                and np.array_equal(v.view(np.uint32), g.vals.view(np.uint32)))}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------- spectral stage
+SPECTRAL_METRIC = "spectral eigenpair solves/s (Laplacian + Lanczos, src/sparse.rs + src/eigen.rs)"
+SPECTRAL_UNIT = "solves/s"
+SPECTRAL_K = 3  # dim + 1 for a 2-d embedding (src/spectral.rs:72-73)
+
+
+def spectral_input(wl):
+    """The fuzzy graph of ``wl``'s kNN graph, computed on the device by this
+    library: (rows, cols, vals) host arrays."""
+    import holomap_b200 as hm
+    knn, sm = hm.knn_smooth(wl.data, wl.d, wl.k, wl.metric)
+    g = hm.fuzzy_simplicial_set(knn, sm)
+    return g.rows, g.cols, g.vals
+
+
+def spectral_config(wl, nnz, cycles=None) -> dict:
+    cfg = {"workload": "spectral_50k", "input": f"fuzzy graph of the {wl.name} kNN graph "
+           f"(n={wl.n}, d={wl.d}, k={wl.k}, {wl.metric})", "n": wl.n, "nnz": int(nnz),
+           "eigenpairs": SPECTRAL_K, "parallelism": "replicas"}
+    if cycles is not None:
+        cfg["lanczos_cycles"] = int(cycles)
+    return cfg
+
+
+def spectral_cpu_sample(wl, rows, cols, vals, cycles: int) -> tuple[float, str]:
+    """Seconds for the oracle's restatement of the reference's Laplacian +
+    Lanczos: one restart cycle timed, scaled to ``cycles`` cycles."""
+    import holomap_oracle
+    t0 = time.perf_counter()
+    ip, sv, _ = holomap_oracle.laplacian(rows, cols, vals, wl.n)
+    t_lap = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    holomap_oracle.lanczos(ip, cols, sv, wl.n, SPECTRAL_K, max_cycles=1)
+    t_cycle = time.perf_counter() - t0
+    total = t_lap + t_cycle * max(cycles, 1)
+    return total, (f"Laplacian::new once + one Lanczos cycle, the cycle scaled by the "
+                   f"{cycles} cycles the device run took; C restatement of src/sparse.rs:21-84 "
+                   f"and src/eigen.rs:95-238 (modified Gram-Schmidt, sequential dots), 1 thread")
+
+
+def spectral_reference_arm(args) -> int:
+    wl = workload("embed_50k", args.rows)
+    rows, cols, vals = spectral_input(wl)
+    import holomap_b200 as hm
+    cycles = hm.smallest_eigenpairs(hm.FuzzyGraph(wl.n, rows, cols, vals), SPECTRAL_K).cycles
+    per, sample = spectral_cpu_sample(wl, rows, cols, vals, cycles)
+    value = 1.0 / per
+    line = {
+        "metric": SPECTRAL_METRIC, "value": value, "unit": SPECTRAL_UNIT, "impl": "reference",
+        "n_gpus": args.gpus, "steps": 1, "warmup": 0, "ms_per_step": per * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": spectral_config(wl, rows.size, cycles),
+        "path": "reference (host cores)",
+        "cpu_baseline": {"value": value, "unit": SPECTRAL_UNIT, "cores": 1, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": SPECTRAL_UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def spectral_main(args) -> int:
+    """spectral_50k: one step = hm_laplacian_device + hm_eigenpairs_device (3
+    smallest eigenpairs) on the fuzzy graph of the embed_50k kNN graph, the
+    graph resident in HBM.  e2e = hm_spectral_eigenpairs (host COO in, host
+    eigenpairs out).  The roofline is the Laplacian matvec's, the kernel the
+    iteration is built on."""
+    import torch
+
+    import holomap_b200 as hm
+    from holomap_b200 import _lib
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1 and int(os.environ.get("RANK", "0")) != 0:
+        return 0  # one replica; the stage has no multi-GPU form
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    wl = workload("embed_50k", args.rows)
+    rows, cols, vals = spectral_input(wl)
+    n, nnz = wl.n, rows.size
+    lib = hm.lib()
+    t = lambda a: torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a).to(dev)
+    d_r, d_c, d_v = t(rows), t(cols), t(vals)
+    ip = torch.empty(n + 1, dtype=torch.int64, device=dev)
+    sv = torch.empty(nnz, dtype=torch.float64, device=dev)
+    deg = torch.empty(n, dtype=torch.float64, device=dev)
+    ws_bytes = lib.hm_eigenpairs_workspace_bytes(n, SPECTRAL_K)
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    out_v = np.empty(SPECTRAL_K)
+    out_x = np.empty(SPECTRAL_K * n)
+    found, cycles = ctypes.c_uint32(0), ctypes.c_uint32(0)
+    stream = torch.cuda.current_stream(dev)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def step():
+        _lib.check(lib.hm_laplacian_device(d_r.data_ptr(), d_c.data_ptr(), d_v.data_ptr(), n, nnz,
+                                           ip.data_ptr(), sv.data_ptr(), deg.data_ptr(), sp))
+        _lib.check(lib.hm_eigenpairs_device(ip.data_ptr(), d_c.data_ptr(), sv.data_ptr(), n, SPECTRAL_K,
+                                            ws.data_ptr(), ws_bytes, sp, out_v.ctypes.data,
+                                            out_x.ctypes.data, ctypes.byref(found), ctypes.byref(cycles)))
+
+    l0 = _lib.launch_count()
+    step()
+    launches = _lib.launch_count() - l0
+    first = out_v.copy(), out_x.copy()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    clocks = ClockSampler(dev.index)
+    clocks.start()
+    evs = []
+    for _ in range(args.steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize(dev)
+    clk = clocks.stop()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    total_ms = sum(step_ms)
+    same_runs = bool(np.array_equal(first[0], out_v) and np.array_equal(first[1], out_x))
+
+    # the matvec kernel alone: L x over the resident Laplacian, many launches
+    x = torch.randn(n, dtype=torch.float64, device=dev)
+    y = torch.empty_like(x)
+    reps = 200
+    for _ in range(5):
+        _lib.check(lib.hm_laplacian_matvec_device(ip.data_ptr(), d_c.data_ptr(), sv.data_ptr(), n,
+                                                  x.data_ptr(), y.data_ptr(), sp))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        _lib.check(lib.hm_laplacian_matvec_device(ip.data_ptr(), d_c.data_ptr(), sv.data_ptr(), n,
+                                                  x.data_ptr(), y.data_ptr(), sp))
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    mv_s = e0.elapsed_time(e1) / reps / 1e3
+    # algorithmic bytes of one L x: the CSR (offsets, columns, weights), x
+    # gathered once per entry, x and y streamed once
+    alg = (n + 1) * 8 + nnz * (4 + 8) + nnz * 8 + n * 16
+    peaks = measured_peaks()
+    peak = peaks.get("hbm_gbs", 6650.0)
+
+    # end to end through the host entry point
+    e2e_steps = args.e2e_steps or max(2, min(args.steps, 5))
+    g = hm.FuzzyGraph(n, rows, cols, vals)
+    hm.smallest_eigenpairs(g, SPECTRAL_K)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        pairs = hm.smallest_eigenpairs(g, SPECTRAL_K)
+    e2e_s = time.perf_counter() - t0
+    same_e2e = bool(np.array_equal(pairs.values, out_v[: pairs.values.size]))
+    line = {
+        "metric": SPECTRAL_METRIC, "value": args.steps / (total_ms / 1e3), "unit": SPECTRAL_UNIT,
+        "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": spectral_config(wl, nnz, cycles.value),
+        "found": int(found.value), "eigenvalues": [float(v) for v in out_v[: found.value]],
+        "identical_across_runs": same_runs,
+        "e2e": {"value": e2e_steps / e2e_s, "unit": SPECTRAL_UNIT,
+                "h2d_bytes_per_step": int(nnz * 12), "d2h_bytes_per_step": int(SPECTRAL_K * (n + 1) * 8),
+                "steps": e2e_steps, "matches_device_run": same_e2e,
+                "api": "hm_spectral_eigenpairs (host COO in, host eigenpairs out)"},
+        "gpu_launches": int(launches * args.steps),
+        "roofline": {"bound": "hbm", "kernel": "lap_matvec_kernel (L x, binary64, row order kept)",
+                     "achieved": alg / mv_s / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / mv_s / 1e9 / peak, "traffic": None,
+                     "algorithmic": f"8 (n + 1) + 20 nnz + 16 n = {alg} bytes per L x",
+                     "avg_launch_us": mv_s * 1e6,
+                     "peak_source": "MEASURED_PEAKS.json hbm_gbs (of measured)" if peaks else
+                                    "fallback 6.65 TB/s (of fallback)"},
+        "clocks": clk,
+        "step_ms": {"min": min(step_ms), "median": statistics.median(step_ms), "max": max(step_ms)},
+    }
+    if not args.no_cpu_baseline:
+        per, sample = spectral_cpu_sample(wl, rows, cols, vals, cycles.value)
+        line["cpu_baseline"] = {"value": 1.0 / per, "unit": SPECTRAL_UNIT, "cores": 1, "kind": "port",
+                                "sample": sample}
     print(json.dumps(line), flush=True)
     return 0
 

@@ -8,12 +8,12 @@ hand-written CUDA kernels behind the C ABI in include/holomap_cuda.h.
 from ._lib import (  # noqa: F401
     HM_ERR_ADMISSION, HM_ERR_CUDA, HM_ERR_INVALID, HM_ERR_NOT_READY, HM_ERR_OOM,
     HM_ERR_TIMEOUT, HM_ERR_UNSUPPORTED, HM_OK, HmStats, HolomapCudaError, HolomapInvalidInput,
-    FuzzyGraph, Knn, KnnPath, Metric, SmoothKnn, autotune_path, exact_knn, fuzzy_simplicial_set,
-    knn_smooth, lib, smooth_knn, workspace_bytes,
+    EigenPairs, FuzzyGraph, Knn, KnnPath, Metric, SmoothKnn, autotune_path, exact_knn, fuzzy_simplicial_set,
+    knn_smooth, lib, smallest_eigenpairs, smooth_knn, workspace_bytes,
 )
 
 __all__ = [
-    "FuzzyGraph", "HmStats", "HolomapCudaError", "HolomapInvalidInput", "Knn", "KnnPath", "Metric",
+    "EigenPairs", "FuzzyGraph", "HmStats", "HolomapCudaError", "HolomapInvalidInput", "Knn", "KnnPath", "Metric",
     "SmoothKnn", "autotune_path", "exact_knn", "fuzzy_simplicial_set", "knn_smooth", "lib",
-    "smooth_knn", "workspace_bytes",
+    "smallest_eigenpairs", "smooth_knn", "workspace_bytes",
 ]

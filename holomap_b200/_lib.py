@@ -192,6 +192,11 @@ SIGNATURES = {
     "hm_fuzzy_graph_device": (_i32, [_vp, _vp, _vp, _vp, _u64, _u32, _vp, _vp, _vp, _vp, _vp, _sz,
                                      _vp]),
     "hm_fuzzy_graph": (_i32, [_vp, _vp, _vp, _vp, _u64, _u32, _vp, _vp, _vp, _vp]),
+    "hm_laplacian_device": (_i32, [_vp, _vp, _vp, _u64, _u64, _vp, _vp, _vp, _vp]),
+    "hm_laplacian_matvec_device": (_i32, [_vp, _vp, _vp, _u64, _vp, _vp, _vp]),
+    "hm_eigenpairs_workspace_bytes": (_sz, [_u64, _u32]),
+    "hm_eigenpairs_device": (_i32, [_vp, _vp, _vp, _u64, _u32, _vp, _sz, _vp, _vp, _vp, _vp, _vp]),
+    "hm_spectral_eigenpairs": (_i32, [_vp, _vp, _vp, _u64, _u64, _u32, _vp, _vp, _vp, _vp]),
     "hm_last_error": (ctypes.c_char_p, []),
     "hm_abi_version": (_i32, []),
     "hm_autotune_path": (_i32, [_u64, _u32, _u32, _i32]),
@@ -380,6 +385,35 @@ def fuzzy_simplicial_set(knn: Knn, calib: SmoothKnn) -> FuzzyGraph:
                                _ptr(cols), _ptr(vals), ctypes.byref(nnz)))
     m = nnz.value
     return FuzzyGraph(n, rows[:m].copy(), cols[:m].copy(), vals[:m].copy())
+
+
+@dataclass
+class EigenPairs:
+    """k smallest eigenpairs of the normalized Laplacian (src/eigen.rs:20-29):
+    values ascending, vectors as a (k, n) array (row j = eigenvector j)."""
+    values: np.ndarray   # float64, k
+    vectors: np.ndarray  # float64, k x n
+    cycles: int
+
+
+def smallest_eigenpairs(graph: FuzzyGraph, k: int) -> EigenPairs:
+    """Lanczos eigenpairs of the graph's normalized Laplacian on the GPU
+    (src/sparse.rs:56-71 + src/eigen.rs:95-223)."""
+    n = int(graph.n)
+    rows = np.ascontiguousarray(graph.rows, dtype=np.uint32)
+    cols = np.ascontiguousarray(graph.cols, dtype=np.uint32)
+    vals = np.ascontiguousarray(graph.vals, dtype=np.float32)
+    if rows.size != cols.size or rows.size != vals.size:
+        raise HolomapInvalidInput(HM_ERR_INVALID, "rows, cols and vals differ in length")
+    out_v = np.empty(k, dtype=np.float64)
+    out_x = np.empty(max(k, 1) * n, dtype=np.float64)
+    found = ctypes.c_uint32(0)
+    cycles = ctypes.c_uint32(0)
+    check(lib().hm_spectral_eigenpairs(_ptr(rows), _ptr(cols), _ptr(vals), n, rows.size, k,
+                                       _ptr(out_v), _ptr(out_x), ctypes.byref(found),
+                                       ctypes.byref(cycles)))
+    f = found.value
+    return EigenPairs(out_v[:f].copy(), out_x[: f * n].reshape(f, n).copy(), cycles.value)
 
 
 def workspace_bytes(n: int, d: int, k: int, metric="euclidean", path="auto") -> int:

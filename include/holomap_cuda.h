@@ -173,6 +173,46 @@ HM_API int hm_fuzzy_graph(const uint32_t *idx, const float *dist, const float *s
                           uint64_t n, uint32_t k, uint32_t *rows_out, uint32_t *cols_out,
                           float *vals_out, uint64_t *nnz_out);
 
+/* The spectral stage that follows the fuzzy graph (spectral_layout_single,
+ * src/spectral.rs:70-83).
+ *
+ * hm_laplacian_device replaces Laplacian::new (src/sparse.rs:56-71, with
+ * Csr::from_fuzzy :21-35): from the (row, col)-sorted COO of n points
+ * (d_rows / d_cols / d_vals, nnz entries, as hm_fuzzy_graph writes it) it
+ * writes the CSR offsets d_indptr (n + 1), the normalized weights d_svals
+ * (nnz, S = D^-1/2 W D^-1/2) and d_degrees (n), bit for bit as the
+ * reference; the column indices of the CSR are d_cols itself.
+ * hm_laplacian_matvec_device replaces Laplacian::matvec (src/sparse.rs:78-84):
+ * d_y = L d_x = d_x - S d_x, bit for bit.
+ *
+ * hm_eigenpairs_device replaces smallest_eigenpairs (src/eigen.rs:31-37)
+ * with the Lanczos iteration of src/eigen.rs:95-223 at every n: the k
+ * smallest eigenvalues of L (ascending, values_out) and unit eigenvectors
+ * (vectors_out, column-major n x k, canonical sign), both HOST arrays.
+ * *found_out = pairs locked (k unless 200 cycles ran out), *cycles_out (may
+ * be NULL) = restart cycles run.  The eigenpairs agree with the reference to
+ * its tolerances, not bit for bit (the tridiagonal step uses the implicit QL
+ * method; the reference uses nalgebra), and are identical from run to run.
+ * d_workspace: hm_eigenpairs_workspace_bytes(n, k), 256-byte aligned.
+ * Synchronous (the iteration reads a few scalars back every step); 1 <= k <=
+ * min(n, 1024).
+ *
+ * hm_spectral_eigenpairs: host COO in, eigenpairs out (one allocation). */
+HM_API int hm_laplacian_device(const uint32_t *d_rows, const uint32_t *d_cols, const float *d_vals,
+                               uint64_t n, uint64_t nnz, uint64_t *d_indptr, double *d_svals,
+                               double *d_degrees, void *stream);
+HM_API int hm_laplacian_matvec_device(const uint64_t *d_indptr, const uint32_t *d_cols,
+                                      const double *d_svals, uint64_t n, const double *d_x,
+                                      double *d_y, void *stream);
+HM_API size_t hm_eigenpairs_workspace_bytes(uint64_t n, uint32_t k);
+HM_API int hm_eigenpairs_device(const uint64_t *d_indptr, const uint32_t *d_cols,
+                                const double *d_svals, uint64_t n, uint32_t k, void *d_workspace,
+                                size_t workspace_bytes, void *stream, double *values_out,
+                                double *vectors_out, uint32_t *found_out, uint32_t *cycles_out);
+HM_API int hm_spectral_eigenpairs(const uint32_t *rows, const uint32_t *cols, const float *vals,
+                                  uint64_t n, uint64_t nnz, uint32_t k, double *values_out,
+                                  double *vectors_out, uint32_t *found_out, uint32_t *cycles_out);
+
 /* ----------------------------------------------------------------------------
  * Batches: many independent problems of uneven n, d, k and metric in one
  * pass of the device pipeline (every kernel works on the whole batch; the

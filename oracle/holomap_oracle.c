@@ -20,6 +20,10 @@
  *   oracle_expf          libm crate 0.2.16 `expf`, reached from
  *                        src/smooth_knn.rs:46 via src/fmath.rs:119-122
  *   oracle_fuzzy_graph   src/fuzzy.rs:25-91 (t-conorm :67-75)
+ *   oracle_laplacian     src/sparse.rs:21-35, 56-71 (CSR, degrees, S)
+ *   oracle_laplacian_matvec  src/sparse.rs:78-84
+ *   oracle_lanczos       src/eigen.rs:95-238 (tridiagonal by Jacobi rotations:
+ *                        nalgebra's SymmetricEigen is not available here)
  *
  * Parity pins: kNN indices and distances are checked against the reference's
  * own known-answer tests (src/knn.rs:64-105, src/metric.rs:92-102) and the
@@ -27,7 +31,11 @@
  * values 1e-5).  rho/sigma are pinned to 1e-5 by src/smooth_knn.rs:104-124 and
  * the same fixtures.  The fuzzy graph is pinned by src/fuzzy.rs:97-155 and
  * the fixtures' graph_rows / graph_cols (exact) and graph_vals (1e-5,
- * src/fixture_parity.rs:101-117).  The libm crate's source is not available here, so
+ * src/fixture_parity.rs:101-117).  The Laplacian is pinned by
+ * src/sparse.rs:116-160; the eigenpairs to the reference's tolerances by
+ * src/eigen.rs:300-335 and the scipy eigenpairs of
+ * tests/fixtures/spectral_cloud_connected.json (src/fixture_parity.rs:125-185).
+ * The libm crate's source is not available here, so
  * oracle_expf restates its published algorithm (see the comment there); the
  * bit-level identity of sigma with the Rust binary is therefore unpinned
  * beyond those 1e-5 checks.
@@ -527,4 +535,234 @@ long long oracle_fuzzy_graph(const uint32_t *idx, const float *dist, const float
     free(dir);
     free(sup);
     return out;
+}
+
+/* ---------------------------------------------------- spectral stage */
+
+/* Csr::from_fuzzy + Laplacian::new (src/sparse.rs:21-35, 56-71): indptr
+ * (n + 1) by counting rows, degrees as sequential binary64 sums of the
+ * widened weights, s[p] = w[p] * (inv_sqrt[i] * inv_sqrt[j]).  Sums start
+ * from -0.0, the neutral element of the binary64 Sum of Rust >= 1.93. */
+int oracle_laplacian(const uint32_t *rows, const uint32_t *cols, const float *vals, size_t n, size_t nnz,
+                     uint64_t *indptr, double *svals, double *degrees) {
+    double *inv = (double *)malloc((n ? n : 1) * sizeof(double));
+    if (!inv) return -1;
+    memset(indptr, 0, (n + 1) * sizeof(uint64_t));
+    for (size_t p = 0; p < nnz; ++p) indptr[rows[p] + 1] += 1;
+    for (size_t i = 0; i < n; ++i) indptr[i + 1] += indptr[i];
+    for (size_t i = 0; i < n; ++i) {
+        double s = -0.0;
+        for (uint64_t p = indptr[i]; p < indptr[i + 1]; ++p) s += (double)vals[p];
+        degrees[i] = s;
+        inv[i] = 1.0 / sqrt(s);
+    }
+    for (size_t i = 0; i < n; ++i)
+        for (uint64_t p = indptr[i]; p < indptr[i + 1]; ++p)
+            svals[p] = (double)vals[p] * (inv[i] * inv[cols[p]]);
+    free(inv);
+    return 0;
+}
+
+/* Laplacian::matvec (src/sparse.rs:78-84): y = x - S x, row sums in order */
+void oracle_laplacian_matvec(const uint64_t *indptr, const uint32_t *cols, const double *svals, size_t n,
+                             const double *x, double *y) {
+    for (size_t i = 0; i < n; ++i) {
+        double s = -0.0;
+        for (uint64_t p = indptr[i]; p < indptr[i + 1]; ++p) s += svals[p] * x[cols[p]];
+        y[i] = x[i] - s;
+    }
+}
+
+/* src/eigen.rs:225-227 */
+static double sp_dot(const double *a, const double *b, size_t n) {
+    double s = -0.0;
+    for (size_t i = 0; i < n; ++i) s += a[i] * b[i];
+    return s;
+}
+
+/* src/eigen.rs:66-72 */
+static double sp_hash01(size_t i, uint32_t salt) {
+    uint32_t h = ((uint32_t)i + salt) * 2654435761u;
+    return (double)(h >> 8) / (double)(1u << 24);
+}
+
+/* Eigenpairs of a small symmetric matrix a (m x m, row-major, destroyed) by
+ * cyclic Jacobi rotations; vals[m], vecs (m x m, row-major, eigenvectors as
+ * columns).  Stands in for nalgebra's SymmetricEigen, whose source is not
+ * available here: the eigenpairs agree to rounding, not bit for bit. */
+static void sp_jacobi(int m, double *a, double *vals, double *vecs) {
+    for (int i = 0; i < m; ++i)
+        for (int j = 0; j < m; ++j) vecs[i * m + j] = i == j ? 1.0 : 0.0;
+    for (int sweep = 0; sweep < 100; ++sweep) {
+        int rotated = 0;
+        for (int p = 0; p < m; ++p)
+            for (int q = p + 1; q < m; ++q) {
+                double apq = a[p * m + q];
+                if (fabs(apq) <= 1e-300 || fabs(apq) <= 1e-18 * (fabs(a[p * m + p]) + fabs(a[q * m + q]))) {
+                    a[p * m + q] = a[q * m + p] = 0.0;
+                    continue;
+                }
+                rotated = 1;
+                double theta = (a[q * m + q] - a[p * m + p]) / (2.0 * apq);
+                double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(theta * theta + 1.0));
+                double c = 1.0 / sqrt(t * t + 1.0), s = t * c;
+                for (int r = 0; r < m; ++r) {
+                    double arp = a[r * m + p], arq = a[r * m + q];
+                    a[r * m + p] = c * arp - s * arq;
+                    a[r * m + q] = s * arp + c * arq;
+                }
+                for (int r = 0; r < m; ++r) {
+                    double apr = a[p * m + r], aqr = a[q * m + r];
+                    a[p * m + r] = c * apr - s * aqr;
+                    a[q * m + r] = s * apr + c * aqr;
+                }
+                for (int r = 0; r < m; ++r) {
+                    double vrp = vecs[r * m + p], vrq = vecs[r * m + q];
+                    vecs[r * m + p] = c * vrp - s * vrq;
+                    vecs[r * m + q] = s * vrp + c * vrq;
+                }
+            }
+        if (!rotated) break;
+    }
+    for (int i = 0; i < m; ++i) vals[i] = a[i * m + i];
+}
+
+/* lanczos_eigenpairs (src/eigen.rs:95-223) with canonical_sign (:74-90):
+ * modified Gram-Schmidt twice against the basis then the locked vectors,
+ * sequential dot products, the same start vector, restarts, lock test and
+ * cycle bound (max_cycles; the reference's is 200).  values[k] ascending,
+ * vectors column-major n x k.  Returns
+ * the number of pairs found, -1 on allocation failure; *cycles_out gets the
+ * cycle count. */
+long long oracle_lanczos(const uint64_t *indptr, const uint32_t *cols, const double *svals, size_t n, size_t k,
+                         size_t max_cycles, double *values, double *vectors, size_t *cycles_out) {
+    size_t m = 8 * k > 60 ? 8 * k : 60;
+    if (m > n) m = n;
+    const double LOCK_TOL = 1e-10;
+    const size_t MAX_CYCLES = max_cycles; /* 200 in the reference; smaller for timing samples */
+    double *locked = (double *)malloc(k * n * sizeof(double));
+    double *lvals = (double *)malloc(k * sizeof(double));
+    double *basis = (double *)malloc((m + 1) * n * sizeof(double));
+    double *tmp = (double *)malloc(n * sizeof(double));
+    double *w = (double *)malloc(n * sizeof(double));
+    double *r = (double *)malloc(n * sizeof(double));
+    double *x = (double *)malloc(n * sizeof(double));
+    double *alphas = (double *)malloc(m * sizeof(double));
+    double *betas = (double *)malloc(m * sizeof(double));
+    double *T = (double *)malloc(m * m * sizeof(double));
+    double *ev = (double *)malloc(m * sizeof(double));
+    double *Z = (double *)malloc(m * m * sizeof(double));
+    size_t *order = (size_t *)malloc(m * sizeof(size_t));
+    if (!locked || !lvals || !basis || !tmp || !w || !r || !x || !alphas || !betas || !T || !ev || !Z || !order)
+        return -1;
+    size_t nl = 0, cycle = 0;
+    for (size_t i = 0; i < n; ++i) r[i] = 1.0 + 0.01 * (sp_hash01(i, 0) - 0.5);
+    int have_r = 1;
+    while (nl < k && cycle < MAX_CYCLES) {
+        ++cycle;
+        if (!have_r)
+            for (size_t i = 0; i < n; ++i) r[i] = sp_hash01(i, (uint32_t)(cycle - 1)) - 0.5;
+        have_r = 1;
+        for (int pass = 0; pass < 2; ++pass)
+            for (size_t u = 0; u < nl; ++u) {
+                double c = sp_dot(r, locked + u * n, n);
+                for (size_t i = 0; i < n; ++i) r[i] -= c * locked[u * n + i];
+            }
+        double rnorm = sqrt(sp_dot(r, r, n));
+        if (rnorm < 1e-12) {
+            for (size_t i = 0; i < n; ++i) r[i] = sp_hash01(i, (uint32_t)cycle) - 0.5;
+            continue;
+        }
+        for (size_t i = 0; i < n; ++i) basis[i] = r[i] / rnorm;
+        size_t steps = m < n - nl ? m : n - nl;
+        size_t na = 0, nb = 0;
+        for (;;) {
+            size_t j = na;
+            const double *vj = basis + j * n;
+            oracle_laplacian_matvec(indptr, cols, svals, n, vj, tmp);
+            for (size_t i = 0; i < n; ++i) w[i] = 2.0 * vj[i] - tmp[i];
+            alphas[na++] = sp_dot(w, vj, n);
+            for (int pass = 0; pass < 2; ++pass) {
+                for (size_t u = 0; u <= j; ++u) {
+                    double c = sp_dot(w, basis + u * n, n);
+                    for (size_t i = 0; i < n; ++i) w[i] -= c * basis[u * n + i];
+                }
+                for (size_t u = 0; u < nl; ++u) {
+                    double c = sp_dot(w, locked + u * n, n);
+                    for (size_t i = 0; i < n; ++i) w[i] -= c * locked[u * n + i];
+                }
+            }
+            if (na == steps) break;
+            double beta = sqrt(sp_dot(w, w, n));
+            if (beta < 1e-12) break;
+            for (size_t i = 0; i < n; ++i) basis[(j + 1) * n + i] = w[i] / beta;
+            betas[nb++] = beta;
+        }
+        size_t t = na;
+        for (size_t i = 0; i < t * t; ++i) T[i] = 0.0;
+        for (size_t i = 0; i < t; ++i) T[i * t + i] = alphas[i];
+        for (size_t i = 0; i < nb; ++i) T[i * t + i + 1] = T[(i + 1) * t + i] = betas[i];
+        sp_jacobi((int)t, T, ev, Z);
+        for (size_t i = 0; i < t; ++i) order[i] = i;
+        for (size_t i = 1; i < t; ++i) { /* stable insertion sort, descending */
+            size_t v = order[i], j = i;
+            while (j > 0 && ev[order[j - 1]] < ev[v]) { order[j] = order[j - 1]; --j; }
+            order[j] = v;
+        }
+        size_t take = k - nl + 1;
+        if (take > t) take = t;
+        int next = 0;
+        for (size_t c = 0; c < take; ++c) {
+            size_t col = order[c];
+            double theta = ev[col];
+            for (size_t i = 0; i < n; ++i) x[i] = 0.0;
+            for (size_t s = 0; s < t; ++s) {
+                double cf = Z[s * t + col];
+                for (size_t i = 0; i < n; ++i) x[i] += cf * basis[s * n + i];
+            }
+            double nx = sqrt(sp_dot(x, x, n));
+            for (size_t i = 0; i < n; ++i) x[i] /= nx;
+            oracle_laplacian_matvec(indptr, cols, svals, n, x, tmp);
+            double res = -0.0;
+            for (size_t i = 0; i < n; ++i) {
+                double e = 2.0 * x[i] - tmp[i] - theta * x[i];
+                res += e * e;
+            }
+            res = sqrt(res);
+            if (res < LOCK_TOL && nl < k) {
+                memcpy(locked + nl * n, x, n * sizeof(double));
+                lvals[nl++] = 2.0 - theta;
+            } else if (!next) {
+                memcpy(r, x, n * sizeof(double));
+                next = 1;
+            }
+        }
+        if (!next) have_r = 0;
+    }
+    /* ascending lambda (stable), canonical sign */
+    size_t *idx = order; /* m >= k */
+    size_t found = nl < k ? nl : k;
+    size_t *ord2 = (size_t *)malloc((nl ? nl : 1) * sizeof(size_t));
+    for (size_t i = 0; i < nl; ++i) ord2[i] = i;
+    for (size_t i = 1; i < nl; ++i) {
+        size_t v = ord2[i], j = i;
+        while (j > 0 && lvals[ord2[j - 1]] > lvals[v]) { ord2[j] = ord2[j - 1]; --j; }
+        ord2[j] = v;
+    }
+    (void)idx;
+    for (size_t j = 0; j < found; ++j) {
+        values[j] = lvals[ord2[j]];
+        double *out = vectors + j * n;
+        memcpy(out, locked + ord2[j] * n, n * sizeof(double));
+        size_t pivot = 0;
+        for (size_t i = 0; i < n; ++i)
+            if (fabs(out[i]) > fabs(out[pivot]) + 1e-15) pivot = i;
+        if (out[pivot] < 0.0)
+            for (size_t i = 0; i < n; ++i) out[i] = -out[i];
+    }
+    free(ord2);
+    free(locked); free(lvals); free(basis); free(tmp); free(w); free(r); free(x);
+    free(alphas); free(betas); free(T); free(ev); free(Z); free(order);
+    if (cycles_out) *cycles_out = cycle;
+    return (long long)found;
 }

@@ -72,6 +72,13 @@ def lib() -> ctypes.CDLL:
         L.oracle_expf_array.restype = None
         L.oracle_fuzzy_graph.argtypes = [u32p, fp, fp, fp, sz, sz, u32p, u32p, fp]
         L.oracle_fuzzy_graph.restype = ctypes.c_longlong
+        u64p = dp = ctypes.c_void_p
+        L.oracle_laplacian.argtypes = [u32p, u32p, fp, sz, sz, u64p, dp, dp]
+        L.oracle_laplacian.restype = ctypes.c_int
+        L.oracle_laplacian_matvec.argtypes = [u64p, u32p, dp, sz, dp, dp]
+        L.oracle_laplacian_matvec.restype = None
+        L.oracle_lanczos.argtypes = [u64p, u32p, dp, sz, sz, sz, dp, dp, ctypes.c_void_p]
+        L.oracle_lanczos.restype = ctypes.c_longlong
         L.oracle_log2.argtypes = [ctypes.c_double]
         L.oracle_log2.restype = ctypes.c_double
         _lib = L
@@ -166,3 +173,46 @@ def fuzzy_graph(indices: np.ndarray, dists: np.ndarray, sigmas: np.ndarray, rhos
     if m < 0:
         raise MemoryError("oracle_fuzzy_graph")
     return rows[:m].copy(), cols[:m].copy(), vals[:m].copy()
+
+
+def laplacian(rows: np.ndarray, cols: np.ndarray, vals: np.ndarray, n: int):
+    """src/sparse.rs:21-35, 56-71: (indptr uint64 n+1, s float64 nnz,
+    degrees float64 n) of the (row, col)-sorted COO."""
+    r = np.ascontiguousarray(rows, dtype=np.uint32)
+    c = np.ascontiguousarray(cols, dtype=np.uint32)
+    v = np.ascontiguousarray(vals, dtype=np.float32)
+    indptr = np.empty(n + 1, dtype=np.uint64)
+    sv = np.empty(max(r.size, 1), dtype=np.float64)
+    deg = np.empty(n, dtype=np.float64)
+    if lib().oracle_laplacian(_ptr(r), _ptr(c), _ptr(v), n, r.size, _ptr(indptr), _ptr(sv),
+                              _ptr(deg)) != 0:
+        raise MemoryError("oracle_laplacian")
+    return indptr, sv[: r.size], deg
+
+
+def laplacian_matvec(indptr, cols, svals, x):
+    """src/sparse.rs:78-84: y = L x."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.empty_like(x)
+    ip = np.ascontiguousarray(indptr, dtype=np.uint64)
+    c = np.ascontiguousarray(cols, dtype=np.uint32)
+    sv = np.ascontiguousarray(svals, dtype=np.float64)
+    lib().oracle_laplacian_matvec(_ptr(ip), _ptr(c), _ptr(sv), x.size, _ptr(x), _ptr(y))
+    return y
+
+
+def lanczos(indptr, cols, svals, n: int, k: int, max_cycles: int = 200):
+    """src/eigen.rs:95-238: (values ascending, vectors n x found column-major
+    as a (found, n) array, cycles).  max_cycles bounds a timing sample (the
+    reference runs up to 200)."""
+    ip = np.ascontiguousarray(indptr, dtype=np.uint64)
+    c = np.ascontiguousarray(cols, dtype=np.uint32)
+    sv = np.ascontiguousarray(svals, dtype=np.float64)
+    vals = np.empty(k, dtype=np.float64)
+    vecs = np.empty(k * n, dtype=np.float64)
+    cyc = ctypes.c_size_t(0)
+    f = lib().oracle_lanczos(_ptr(ip), _ptr(c), _ptr(sv), n, k, max_cycles, _ptr(vals), _ptr(vecs),
+                             ctypes.byref(cyc))
+    if f < 0:
+        raise MemoryError("oracle_lanczos")
+    return vals[:f], vecs[: f * n].reshape(f, n), cyc.value

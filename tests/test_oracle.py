@@ -204,3 +204,112 @@ def test_expf_subnormal_range_monotone(oracle):
 def test_log2_target_is_platform_log2(oracle):
     for k in (2, 3, 15, 30, 100):
         assert oracle.lib().oracle_log2(float(k)) == math.log2(k)
+
+
+# --- spectral stage: src/sparse.rs and src/eigen.rs tests -------------------
+
+def p3_graph():
+    # src/sparse.rs:105-115: path 0-1-2 with unit weights
+    return (np.array([0, 1, 1, 2], dtype=np.uint32), np.array([1, 0, 2, 1], dtype=np.uint32),
+            np.ones(4, dtype=np.float32), 3)
+
+
+def wiggly_graph(n):
+    """src/eigen.rs:252-273: a path with hashed weights plus two chords, as a
+    (row, col)-sorted COO."""
+    coo = []
+
+    def push(a, b, w):
+        coo.append((a, b, w))
+        coo.append((b, a, w))
+
+    for i in range(n - 1):
+        h = (i * 2654435761) & 0xFFFFFFFF
+        w = np.float32(np.float32(0.5) + np.float32(0.4) * np.float32(np.float32(h >> 16) / np.float32(65536.0)))
+        push(i, i + 1, w)
+    push(0, n // 2, np.float32(0.3))
+    push(n // 4, 3 * n // 4, np.float32(0.2))
+    coo.sort(key=lambda e: (e[0], e[1]))
+    return (np.array([e[0] for e in coo], dtype=np.uint32), np.array([e[1] for e in coo], dtype=np.uint32),
+            np.array([e[2] for e in coo], dtype=np.float32), n)
+
+
+def dense_laplacian(indptr, cols, sv, n):
+    a = np.eye(n)
+    for i in range(n):
+        for p in range(int(indptr[i]), int(indptr[i + 1])):
+            a[i, cols[p]] -= sv[p]
+    return a
+
+
+def test_laplacian_csr_and_degrees(oracle):
+    # src/sparse.rs:117-145
+    r, c, v, n = p3_graph()
+    indptr, sv, deg = oracle.laplacian(r, c, v, n)
+    assert indptr.tolist() == [0, 1, 3, 4]
+    assert deg.tolist() == [1.0, 2.0, 1.0]
+    y = oracle.laplacian_matvec(indptr, c, sv, [1.0, math.sqrt(2.0), 1.0])
+    assert np.abs(y).max() < 1e-12
+    y = oracle.laplacian_matvec(indptr, c, sv, [1.0, 0.0, -1.0])
+    assert np.abs(y - np.array([1.0, 0.0, -1.0])).max() < 1e-12
+
+
+def test_laplacian_dense_matches_matvec(oracle):
+    # src/sparse.rs:147-160
+    r, c, v, n = wiggly_graph(40)
+    indptr, sv, _ = oracle.laplacian(r, c, v, n)
+    a = dense_laplacian(indptr, c, sv, n)
+    for j in range(n):
+        e = np.zeros(n)
+        e[j] = 1.0
+        assert np.abs(a[:, j] - oracle.laplacian_matvec(indptr, c, sv, e)).max() < 1e-15
+
+
+def eigen_close(oracle, indptr, cols, sv, n, vals, vecs, tol):
+    # src/eigen.rs:275-299
+    assert (np.diff(vals) >= -1e-12).all()
+    for j in range(vals.size):
+        v = vecs[j]
+        assert abs(np.sqrt((v * v).sum()) - 1.0) < 1e-8
+        y = oracle.laplacian_matvec(indptr, cols, sv, v)
+        assert np.sqrt(((y - vals[j] * v) ** 2).sum()) < tol
+
+
+def test_lanczos_recovers_p3_spectrum(oracle):
+    # src/eigen.rs:300-316
+    r, c, v, n = p3_graph()
+    indptr, sv, _ = oracle.laplacian(r, c, v, n)
+    vals, vecs, _ = oracle.lanczos(indptr, c, sv, n, 3)
+    assert np.abs(vals - [0.0, 1.0, 2.0]).max() < 1e-12
+    eigen_close(oracle, indptr, c, sv, n, vals, vecs, 1e-10)
+    assert abs(vecs[1][1]) < 1e-10 and abs(abs(vecs[1][0]) - 1 / math.sqrt(2)) < 1e-10
+    assert abs(vecs[1][0] + vecs[1][2]) < 1e-10
+
+
+def test_lanczos_matches_dense_on_wiggly_graph(oracle):
+    # src/eigen.rs:318-336: numpy's dense eigh stands in for nalgebra
+    r, c, v, n = wiggly_graph(120)
+    indptr, sv, _ = oracle.laplacian(r, c, v, n)
+    k = 4
+    vals, vecs, _ = oracle.lanczos(indptr, c, sv, n, k)
+    ev, evec = np.linalg.eigh(dense_laplacian(indptr, c, sv, n))
+    assert np.abs(vals - ev[:k]).max() < 1e-8
+    eigen_close(oracle, indptr, c, sv, n, vals, vecs, 1e-7)
+    for j in range(k):
+        assert abs(vecs[j] @ evec[:, j]) > 1 - 1e-7
+
+
+def test_spectral_golden_fixture(oracle):
+    # src/fixture_parity.rs:125-185: kNN -> smooth-kNN -> fuzzy graph ->
+    # Laplacian -> dim + 1 smallest eigenpairs against scipy's
+    fx = json.loads((GOLDEN / "spectral_cloud_connected.json").read_text())
+    data = f32(fx["data"])
+    k, n, dim = fx["n_neighbors"], fx["n_samples"], fx["dim"]
+    idx, dist = oracle.exact_knn(data, k, "euclidean")
+    sig, rho = oracle.smooth_knn(dist, k)
+    rows, cols, vals = oracle.fuzzy_graph(idx, dist, sig, rho, k)
+    indptr, sv, _ = oracle.laplacian(rows, cols, vals, n)
+    ev, vecs, _ = oracle.lanczos(indptr, cols, sv, n, dim + 1)
+    assert np.abs(ev - np.asarray(fx["eigenvalues"])).max() < 1e-6
+    for j, e in enumerate(fx["eigenvectors"][: dim + 1]):
+        assert abs(vecs[j] @ np.asarray(e)) > 1 - 1e-6
