@@ -70,6 +70,23 @@ def test_laplacian_wiggly(oracle, n):
     check_laplacian(oracle, r, c, v, n, seed=n)
 
 
+@pytest.mark.parametrize("n", [130, 3000])
+def test_laplacian_hub_rows(oracle, n):
+    """Node 0 is joined to every other node (a row of n - 1 entries, summed by
+    the long-row kernel) on top of a path with hashed weights."""
+    edges = {}
+    for j in range(1, n):
+        edges[(0, j)] = edges[(j, 0)] = np.float32(0.25 + (j % 7) / 10)
+    for j in range(1, n - 1):
+        w = np.float32(((j * 2654435761) & 0xFFFF) / 65536.0 + 0.1)
+        edges[(j, j + 1)] = edges[(j + 1, j)] = w
+    keys = sorted(edges)
+    r = np.array([a for a, _ in keys], dtype=np.uint32)
+    c = np.array([b for _, b in keys], dtype=np.uint32)
+    v = np.array([edges[e] for e in keys], dtype=np.float32)
+    check_laplacian(oracle, r, c, v, n, seed=n)
+
+
 @pytest.mark.parametrize("n,k,metric", [(3000, 15, "euclidean"), (20000, 30, "cosine")])
 def test_laplacian_of_fuzzy_graphs(oracle, n, k, metric):
     from parity import edge_case
