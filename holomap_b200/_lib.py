@@ -206,6 +206,7 @@ SIGNATURES = {
     "hm_knn_smooth_noalloc": (_i32, [_vp, _u64, _u32, _u32, _i32, _vp, _vp, _vp, _vp, _vp]),
     "hm_noalloc_scratch_bytes": (_sz, []),
     "hm_debug_set_screen_dump": (_i32, [_vp]),
+    "hm_debug_tridiag_eigen": (_i32, [_vp, _vp, _u32, _vp, _vp]),
     "hm_batch_create": (_i32, [_vp, _u32, _vp]),
     "hm_batch_destroy": (None, [_vp]),
     "hm_batch_workspace_bytes": (_sz, [_vp]),

@@ -583,4 +583,14 @@ int hm_spectral_eigenpairs(const uint32_t *rows, const uint32_t *cols, const flo
     return rc;
 }
 
+int hm_debug_tridiag_eigen(const double *d, const double *e, uint32_t m, double *vals_out, double *vecs_out) {
+    clear_error();
+    if (!d || !vals_out || !vecs_out || (m > 1 && !e) || m == 0) return set_error(HM_ERR_INVALID, "bad arguments");
+    std::vector<double> dd(d, d + m), ee(e ? e : d, e ? e + (m - 1) : d), z;
+    if (!tridiag_eigen(dd, ee, z)) return set_error(HM_ERR_UNSUPPORTED, "tridiagonal eigensolver did not converge");
+    std::memcpy(vals_out, dd.data(), m * sizeof(double));
+    std::memcpy(vecs_out, z.data(), (size_t)m * m * sizeof(double));
+    return HM_OK;
+}
+
 }  // extern "C"

@@ -380,6 +380,12 @@ HM_API uint64_t hm_launch_count(void);
  * every screened value c^_ij into d_out[i * n + j] (n x n floats). */
 HM_API int hm_debug_set_screen_dump(float *d_out);
 
+/* Test hook (host only, no device): the tridiagonal eigensolver of the
+ * Lanczos iteration on diagonal d[m] and off-diagonal e[m - 1]; vals_out[m]
+ * (unordered) and vecs_out (m x m row-major, eigenvectors as columns). */
+HM_API int hm_debug_tridiag_eigen(const double *d, const double *e, uint32_t m, double *vals_out,
+                                  double *vecs_out);
+
 #ifdef __cplusplus
 }
 #endif

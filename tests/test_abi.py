@@ -120,3 +120,74 @@ def test_every_screened_path_plans_for_the_benchmark_shapes():
                             (50000, 384, 30, "cosine")]:
         for path in ("auto", "plain", "screen_bf16", "screen_tf32", "screen_bf16x3"):
             assert hm.workspace_bytes(n, d, k, metric, path) > 0
+
+
+# --- fuzzy graph and spectral stage: host-side checks (no device) ----------
+
+def test_fuzzy_graph_rejects_bad_input_before_the_device():
+    lib = hm.lib()
+    idx = np.array([0, 5, 1, 0], dtype=np.uint32)  # 5 is not below n = 2
+    f = np.zeros(4, np.float32)
+    sig = np.ones(2, np.float32)
+    out_u = np.zeros(8, np.uint32)
+    out_f = np.zeros(8, np.float32)
+    nnz = ctypes.c_uint64(0)
+    rc = lib.hm_fuzzy_graph(idx.ctypes.data, f.ctypes.data, sig.ctypes.data, sig.ctypes.data, 2, 2,
+                            out_u.ctypes.data, out_u.ctypes.data, out_f.ctypes.data, ctypes.byref(nnz))
+    assert rc == hm.HM_ERR_INVALID and b"not below n" in lib.hm_last_error()
+    idx = np.array([0, 1, 1, 0], dtype=np.uint32)
+    neg = np.array([1.0, -0.5], np.float32)
+    rc = lib.hm_fuzzy_graph(idx.ctypes.data, f.ctypes.data, neg.ctypes.data, sig.ctypes.data, 2, 2,
+                            out_u.ctypes.data, out_u.ctypes.data, out_f.ctypes.data, ctypes.byref(nnz))
+    assert rc == hm.HM_ERR_INVALID and b"negative" in lib.hm_last_error()
+    rc = lib.hm_fuzzy_graph(idx.ctypes.data, f.ctypes.data, sig.ctypes.data, sig.ctypes.data, 0, 2,
+                            out_u.ctypes.data, out_u.ctypes.data, out_f.ctypes.data, ctypes.byref(nnz))
+    assert rc == hm.HM_ERR_INVALID
+    with pytest.raises(hm.HolomapInvalidInput, match="not below n"):
+        hm.fuzzy_simplicial_set(hm.Knn(2, idx * 3, f), hm.SmoothKnn(sig, sig))
+
+
+def test_spectral_rejects_bad_input_before_the_device():
+    lib = hm.lib()
+    rows = np.array([1, 0, 1, 2], dtype=np.uint32)  # not sorted
+    cols = np.array([0, 1, 2, 1], dtype=np.uint32)
+    vals = np.ones(4, np.float32)
+    out = np.zeros(16)
+    found, cycles = ctypes.c_uint32(0), ctypes.c_uint32(0)
+
+    def call(r, c, n, k):
+        return lib.hm_spectral_eigenpairs(r.ctypes.data, c.ctypes.data, vals.ctypes.data, n, r.size, k,
+                                          out.ctypes.data, out.ctypes.data, ctypes.byref(found),
+                                          ctypes.byref(cycles))
+
+    assert call(rows, cols, 3, 2) == hm.HM_ERR_INVALID and b"not sorted" in lib.hm_last_error()
+    rows = np.array([0, 1, 1, 2], dtype=np.uint32)
+    assert call(rows, np.array([1, 0, 7, 1], np.uint32), 3, 2) == hm.HM_ERR_INVALID
+    assert b"outside" in lib.hm_last_error()
+    assert call(rows, cols, 3, 4) == hm.HM_ERR_INVALID  # k above n
+    assert call(rows, cols, 3, 0) == hm.HM_ERR_INVALID
+    assert lib.hm_eigenpairs_workspace_bytes(5000, 1025) == 0  # k above 1024
+    assert lib.hm_eigenpairs_workspace_bytes(50000, 3) > 60 * 50000 * 8
+    assert lib.hm_laplacian_device(None, None, None, 3, 4, None, None, None, None) == hm.HM_ERR_INVALID
+
+
+@pytest.mark.parametrize("m,seed", [(1, 0), (2, 1), (7, 2), (60, 3), (61, 4)])
+def test_tridiagonal_eigensolver(m, seed):
+    """The implicit QL solver the Lanczos iteration uses for its tridiagonal,
+    against numpy's dense eigh (residuals and orthonormality), including a
+    matrix with nearly decoupled blocks."""
+    g = np.random.default_rng(seed)
+    d = g.uniform(0.0, 2.0, m)
+    e = g.uniform(0.0, 0.5, max(m - 1, 0))
+    if m > 3:
+        e[m // 2] = 1e-15
+    vals = np.empty(m)
+    vecs = np.empty(m * m)
+    rc = hm.lib().hm_debug_tridiag_eigen(d.ctypes.data, e.ctypes.data if m > 1 else None, m,
+                                         vals.ctypes.data, vecs.ctypes.data)
+    assert rc == hm.HM_OK
+    z = vecs.reshape(m, m)
+    t = np.diag(d) + np.diag(e, 1) + np.diag(e, -1)
+    assert np.abs(t @ z - z * vals).max() < 1e-13
+    assert np.abs(z.T @ z - np.eye(m)).max() < 1e-13
+    assert np.abs(np.sort(vals) - np.linalg.eigvalsh(t)).max() < 1e-13
