@@ -313,3 +313,94 @@ def test_spectral_golden_fixture(oracle):
     assert np.abs(ev - np.asarray(fx["eigenvalues"])).max() < 1e-6
     for j, e in enumerate(fx["eigenvectors"][: dim + 1]):
         assert abs(vecs[j] @ np.asarray(e)) > 1 - 1e-6
+
+
+def fuzzy_by_dict(idx, dist, sig, rho, k):
+    """src/fuzzy.rs:25-91 restated once more with Python containers and numpy
+    binary32 scalars, to check the C restatement."""
+    n = idx.size // k
+    a = {}
+    for i in range(n):
+        for j in range(k):
+            c = int(idx[i * k + j])
+            if c == i:
+                continue
+            d = np.float32(dist[i * k + j]) - np.float32(rho[i])
+            if d <= 0 or sig[i] == 0:
+                w = np.float32(1.0)
+            else:
+                w = np.float32(oracle_expf_scalar(-(d / np.float32(sig[i]))))
+            if w != 0:
+                a[(i, c)] = w
+    coords = sorted(set(a) | {(c, r) for r, c in a})
+    rows, cols, vals = [], [], []
+    zero = np.float32(0.0)
+    for r, c in coords:
+        v, vt = a.get((r, c), zero), a.get((c, r), zero)
+        w = np.float32(np.float32(v + vt) - np.float32(v * vt))
+        if w != 0:
+            rows.append(r)
+            cols.append(c)
+            vals.append(w)
+    return np.array(rows, np.uint32), np.array(cols, np.uint32), np.array(vals, np.float32)
+
+
+def oracle_expf_scalar(x):
+    import holomap_oracle
+    return holomap_oracle.expf(np.array([x], np.float32))[0]
+
+
+@pytest.mark.parametrize("n,k,seed", [(30, 4, 1), (200, 8, 2), (400, 15, 3)])
+def test_fuzzy_oracle_against_a_second_restatement(oracle, n, k, seed):
+    g = np.random.default_rng(seed)
+    idx = np.empty((n, k), np.uint32)
+    for i in range(n):
+        idx[i, 0] = i
+        idx[i, 1:] = g.choice(np.delete(np.arange(n), i), size=k - 1, replace=False)
+    dist = np.zeros((n, k), np.float32)
+    dist[:, 1:] = np.sort(g.gamma(2.0, 1.0, size=(n, k - 1)).astype(np.float32), axis=1)
+    dist, idx = dist.reshape(-1), idx.reshape(-1)
+    sig, rho = oracle.smooth_knn(dist, k)
+    sig = sig.copy()
+    sig[::9] = 0.0
+    a = oracle.fuzzy_graph(idx, dist, sig, rho, k)
+    b = fuzzy_by_dict(idx, dist, sig, rho, k)
+    for x, y, what in zip(a, b, ("rows", "cols", "vals")):
+        assert x.shape == y.shape, what
+        assert (x.view(np.uint32) == y.view(np.uint32)).all(), what
+
+
+@pytest.mark.parametrize("n,seed", [(50, 4), (300, 5)])
+def test_laplacian_oracle_against_a_second_restatement(oracle, n, seed):
+    """src/sparse.rs:21-84 once more in Python floats (binary64, the same
+    order; sums start from -0.0), against the C restatement bit for bit."""
+    g = np.random.default_rng(seed)
+    r, c, v, _ = wiggly_graph(n)
+    v = (v * g.uniform(0.5, 1.5, v.size)).astype(np.float32)
+    # symmetric weights again (the fuzzy graph is symmetric)
+    w = {(int(a), int(b)): v[p] for p, (a, b) in enumerate(zip(r, c))}
+    v = np.array([w[(int(min(a, b)), int(max(a, b)))] for a, b in zip(r, c)], np.float32)
+    indptr, sv, deg = oracle.laplacian(r, c, v, n)
+    ip = [0] * (n + 1)
+    for a in r:
+        ip[int(a) + 1] += 1
+    for i in range(n):
+        ip[i + 1] += ip[i]
+    d = []
+    for i in range(n):
+        s = -0.0
+        for p in range(ip[i], ip[i + 1]):
+            s += float(v[p])
+        d.append(s)
+    inv = [1.0 / math.sqrt(x) for x in d]
+    s2 = [float(v[p]) * (inv[int(r[p])] * inv[int(c[p])]) for p in range(r.size)]
+    assert indptr.tolist() == ip
+    assert np.array(d).view(np.uint64).tolist() == deg.view(np.uint64).tolist()
+    assert np.array(s2).view(np.uint64).tolist() == sv.view(np.uint64).tolist()
+    x = g.normal(size=n)
+    y = oracle.laplacian_matvec(indptr, c, sv, x)
+    for i in range(n):
+        acc = -0.0
+        for p in range(ip[i], ip[i + 1]):
+            acc += s2[p] * x[int(c[p])]
+        assert np.float64(x[i] - acc).view(np.uint64) == y[i].view(np.uint64)
