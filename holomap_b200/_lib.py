@@ -192,6 +192,7 @@ SIGNATURES = {
     "hm_fuzzy_graph_device": (_i32, [_vp, _vp, _vp, _vp, _u64, _u32, _vp, _vp, _vp, _vp, _vp, _sz,
                                      _vp]),
     "hm_fuzzy_graph": (_i32, [_vp, _vp, _vp, _vp, _u64, _u32, _vp, _vp, _vp, _vp]),
+    "hm_fuzzy_graph_status": (_i32, [_vp, _u64, _u32, _vp]),
     "hm_laplacian_device": (_i32, [_vp, _vp, _vp, _u64, _u64, _vp, _vp, _vp, _vp]),
     "hm_laplacian_matvec_device": (_i32, [_vp, _vp, _vp, _u64, _vp, _vp, _vp]),
     "hm_eigenpairs_workspace_bytes": (_sz, [_u64, _u32]),
@@ -203,8 +204,10 @@ SIGNATURES = {
     "hm_timing_enable": (_i32, [_i32]),
     "hm_timing_read": (_i32, [_i32, _vp, _vp, _i32]),
     "hm_launch_count": (_u64, []),
+    "hm_measure_fp64_rate": (_i32, [_vp]),
     "hm_knn_smooth_noalloc": (_i32, [_vp, _u64, _u32, _u32, _i32, _vp, _vp, _vp, _vp, _vp]),
     "hm_noalloc_scratch_bytes": (_sz, []),
+    "hm_noalloc_stats": (_i32, [_vp, _vp]),
     "hm_debug_set_screen_dump": (_i32, [_vp]),
     "hm_debug_tridiag_eigen": (_i32, [_vp, _vp, _u32, _vp, _vp]),
     "hm_batch_create": (_i32, [_vp, _u32, _vp]),
@@ -245,6 +248,14 @@ def timing_read(kclass: str, reset: bool = True) -> tuple[float, int]:
 
 def launch_count() -> int:
     return int(lib().hm_launch_count())
+
+
+def measure_fp64_rate() -> float:
+    """Measured binary64 multiply/add operations per second of the current
+    device (a few milliseconds of probe kernels)."""
+    r = ctypes.c_double()
+    check(lib().hm_measure_fp64_rate(ctypes.byref(r)))
+    return r.value
 
 _lib = None
 

@@ -622,6 +622,27 @@ static int check_counters(const JobCounters &c) {
     return HM_OK;
 }
 
+// Counters of a finished single-job call whose workspace is `ws`, read after
+// the work queued on `s` (no allocation: the copy lands in a host struct).
+int single_job_stats(const void *ws, uint64_t n, uint32_t d, uint32_t k, int metric, int path,
+                     cudaStream_t s, hm_stats *stats) {
+    hm_batch B;
+    hm_job spec{};
+    spec.n = n;
+    spec.d = d;
+    spec.k = k;
+    spec.metric = metric;
+    spec.path = path;
+    HM_TRY(plan_batch(&spec, 1, B));
+    JobCounters c{};
+    HM_CUDA_TRY(cudaMemcpyAsync(&c, static_cast<const char *>(ws) + B.off_counters, sizeof c,
+                                cudaMemcpyDeviceToHost, s));
+    HM_CUDA_TRY(cudaStreamSynchronize(s));
+    hm_stats local;
+    stats_from_counters(B, 0, c, stats ? stats : &local);
+    return check_counters(c);
+}
+
 // batch internals for the request loop (serve.cu)
 size_t batch_counters_offset(const hm_batch *B) { return B->off_counters; }
 

@@ -42,6 +42,9 @@
 namespace hm {
 
 constexpr unsigned FZ_FULL = 0xffffffffu;
+// bits of the status word the rows kernel sets for inputs outside the
+// precondition (each row's indices distinct and below n)
+constexpr uint32_t FZ_BAD_INDEX = 1u, FZ_BAD_DUPLICATE = 2u;
 
 __device__ __forceinline__ float tconorm(float v, float vt) {
     return __fsub_rn(__fadd_rn(v, vt), __fmul_rn(v, vt));
@@ -51,7 +54,7 @@ __global__ void __launch_bounds__(256) fuzzy_rows_kernel(
     const uint32_t *__restrict__ idx, const float *__restrict__ dist, const float *__restrict__ sigma,
     const float *__restrict__ rho, uint32_t n, uint32_t k, float *__restrict__ wdir, uint32_t *__restrict__ rkey,
     uint32_t *__restrict__ rval, uint32_t *__restrict__ fcol, float *__restrict__ fw,
-    uint32_t *__restrict__ fcount) {
+    uint32_t *__restrict__ fcount, uint32_t *__restrict__ bad) {
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (r >= n) return;  // whole warps
@@ -64,7 +67,11 @@ __global__ void __launch_bounds__(256) fuzzy_rows_kernel(
         if (j < k) {
             const uint32_t col = idx[base + j];
             float w = 0.0f;
-            if ((uint64_t)col != r) {
+            if (col >= n) {
+                // outside the precondition: dropped (so every later index
+                // stays in bounds) and reported through the status word
+                atomicOr(bad, FZ_BAD_INDEX);
+            } else if ((uint64_t)col != r) {
                 const float d = __fsub_rn(dist[base + j], rh);
                 w = (d <= 0.0f || sg == 0.0f) ? 1.0f : expf_libm(-__fdiv_rn(d, sg));
                 valid = w != 0.0f;
@@ -77,16 +84,25 @@ __global__ void __launch_bounds__(256) fuzzy_rows_kernel(
     }
     __syncwarp();
     // rank of each valid column among the row's valid columns (dropped
-    // entries carry the key n, above every column)
+    // entries carry the key n, above every column).  Equal columns (outside
+    // the precondition: exact_knn's indices are distinct) rank by position,
+    // so every slot of the row's F list is still written, and are reported.
     for (uint32_t j0 = 0; j0 < k; j0 += 32) {
         const uint32_t j = j0 + lane;
         const uint32_t mine = j < k ? rkey[base + j] : n;
         uint32_t rank = 0;
+        bool dup = false;
         for (uint32_t c0 = 0; c0 < k; c0 += 32) {
             const uint32_t other = c0 + lane < k ? rkey[base + c0 + lane] : n;
 #pragma unroll
-            for (int s = 0; s < 32; ++s) rank += __shfl_sync(FZ_FULL, other, s) < mine ? 1u : 0u;
+            for (int s = 0; s < 32; ++s) {
+                const uint32_t o = __shfl_sync(FZ_FULL, other, s);
+                const uint32_t pos = c0 + (uint32_t)s;
+                rank += (o < mine || (o == mine && pos < j)) ? 1u : 0u;
+                dup |= o == mine && pos != j;
+            }
         }
+        if (dup && mine < n) atomicOr(bad, FZ_BAD_DUPLICATE);
         if (mine < n) {
             fcol[base + rank] = mine;
             fw[base + rank] = wdir[base + j];
@@ -203,8 +219,8 @@ static int key_bits(uint64_t n) {
 // for the sort), the ordered F lists and their merge results, per-row
 // counters, and CUB's temporary storage.
 struct FuzzyLayout {
-    size_t wdir, rk0, rk1, rv0, rv1, fcol, fw, fpos, dpre, fcount, rstart, rdups, count, off, temp, temp_bytes,
-        total;
+    size_t wdir, rk0, rk1, rv0, rv1, fcol, fw, fpos, dpre, fcount, rstart, rdups, count, off, bad, temp,
+        temp_bytes, total;
 };
 
 static int fuzzy_layout(uint64_t n, uint32_t k, FuzzyLayout *L) {
@@ -237,6 +253,7 @@ static int fuzzy_layout(uint64_t n, uint32_t k, FuzzyLayout *L) {
     L->rdups = take(n4);
     L->count = take(n4);
     L->off = take(n4);
+    L->bad = take(4);
     L->temp_bytes = std::max(sort_bytes, scan_bytes);
     L->temp = take(L->temp_bytes);
     L->total = at;
@@ -279,8 +296,10 @@ int hm_fuzzy_graph_device(const uint32_t *d_idx, const float *d_dist, const floa
     auto f32 = [&](size_t o) { return reinterpret_cast<float *>(ws + o); };
     const uint32_t nn = (uint32_t)n, entries = (uint32_t)(n * k);
     const unsigned warp_blocks = (unsigned)((n * 32 + 255) / 256);
+    HM_CUDA_TRY(cudaMemsetAsync(ws + L.bad, 0, 4, s));
     fuzzy_rows_kernel<<<warp_blocks, 256, 0, s>>>(d_idx, d_dist, d_sigma, d_rho, nn, k, f32(L.wdir), u32(L.rk0),
-                                                  u32(L.rv0), u32(L.fcol), f32(L.fw), u32(L.fcount));
+                                                  u32(L.rv0), u32(L.fcol), f32(L.fw), u32(L.fcount),
+                                                  u32(L.bad));
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();
     cub::DoubleBuffer<uint32_t> kb(u32(L.rk0), u32(L.rk1)), vb(u32(L.rv0), u32(L.rv1));
@@ -301,6 +320,21 @@ int hm_fuzzy_graph_device(const uint32_t *d_idx, const float *d_dist, const floa
         reinterpret_cast<unsigned long long *>(d_nnz));
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();
+    return HM_OK;
+}
+
+int hm_fuzzy_graph_status(const void *d_workspace, uint64_t n, uint32_t k, void *stream) {
+    clear_error();
+    if (!d_workspace) return set_error(HM_ERR_INVALID, "NULL pointer argument");
+    FuzzyLayout L;
+    HM_TRY(fuzzy_layout(n, k, &L));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    uint32_t bad = 0;
+    HM_CUDA_TRY(cudaMemcpyAsync(&bad, static_cast<const char *>(d_workspace) + L.bad, 4,
+                                cudaMemcpyDeviceToHost, s));
+    HM_CUDA_TRY(cudaStreamSynchronize(s));
+    if (bad & FZ_BAD_INDEX) return set_error(HM_ERR_INVALID, "a kNN index is not below n");
+    if (bad & FZ_BAD_DUPLICATE) return set_error(HM_ERR_INVALID, "a row of the kNN graph repeats an index");
     return HM_OK;
 }
 
@@ -342,6 +376,8 @@ int hm_fuzzy_graph(const uint32_t *idx, const float *dist, const float *sigma, c
                                    reinterpret_cast<uint32_t *>(d + o_rows), reinterpret_cast<uint32_t *>(d + o_cols),
                                    reinterpret_cast<float *>(d + o_vals), reinterpret_cast<uint64_t *>(d + o_nnz),
                                    d + o_ws, ws, nullptr);
+        if (rc != HM_OK) break;
+        rc = hm_fuzzy_graph_status(d + o_ws, n, k, nullptr);
         if (rc != HM_OK) break;
         err = cudaMemcpy(&nnz, d + o_nnz, 8, cudaMemcpyDeviceToHost);
         if (err == cudaSuccess) err = cudaMemcpy(rows_out, d + o_rows, nnz * 4, cudaMemcpyDeviceToHost);

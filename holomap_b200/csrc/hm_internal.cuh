@@ -256,5 +256,10 @@ int launch_mean_all_floor(const JobDev *jobs, uint32_t njobs, cudaStream_t s);
 // copy of its counters
 size_t batch_counters_offset(const hm_batch *B);
 int batch_job_result(const hm_batch *B, uint32_t job, const JobCounters &c, hm_stats *st);
+// counters of a finished single-job call (workspace `ws`), read after the
+// work queued on `s`; the status is the call's (HM_ERR_INVALID for a
+// non-finite input, HM_ERR_TIMEOUT for a bounded wait that gave up)
+int single_job_stats(const void *ws, uint64_t n, uint32_t d, uint32_t k, int metric, int path,
+                     cudaStream_t s, hm_stats *stats);
 
 }  // namespace hm

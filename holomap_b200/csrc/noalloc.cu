@@ -14,12 +14,18 @@
 // the library image: a file-scope __device__ array of HM_NOALLOC_SCRATCH_BYTES.
 // Every GPU that loads this library holds that array until the process exits.
 // In host code the array's name is only a host-side stand-in, so its device
-// address is looked up once per device with cudaGetSymbolAddress (with that
-// device current) on the first call on the device, and then passed to the
-// kernels; the first call on a device should therefore come before any
-// stream capture.  All calls share the one array and it keeps the last call's
+// address is looked up with cudaGetSymbolAddress (with the device current) on
+// the first call in each CUDA context of a device, and then passed to the
+// kernels; the first call on a device should therefore come before any stream
+// capture.  The lookup is keyed on the device and its current context, so a
+// context that was destroyed and recreated (cudaDeviceReset) gets the array's
+// new address.  All calls share the one array and it keeps the last call's
 // contents: the pipeline clears what must start at zero itself, and calls that
 // overlap on the GPU (different streams, or host threads racing) race on it.
+//
+// The counters of the last call (the non-finite-input flag among them) also
+// stay in that array; hm_noalloc_stats reads them back without allocating.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -31,23 +37,60 @@ namespace hm {
 static __device__ __align__(256) unsigned char g_noalloc_scratch[HM_NOALLOC_SCRATCH_BYTES];
 
 constexpr int kMaxDevices = 64;
-static void *g_scratch_addr[kMaxDevices] = {};
+
+struct ScratchSlot {
+    CUcontext ctx = nullptr;  // context the address was looked up in
+    void *addr = nullptr;
+    // the last call's problem, so its counters can be found in the scratch
+    bool called = false;
+    uint64_t n = 0;
+    uint32_t d = 0, k = 0;
+    int metric = 0;
+};
+static ScratchSlot g_slots[kMaxDevices];
 static std::mutex g_scratch_mu;
 
-// Device address of g_noalloc_scratch on the current device (set-up on the
-// first call per device).
-static int scratch_address(void **out) {
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
+
+// The calling thread's current driver context, or NULL when the thread has
+// none bound yet.
+static int current_context(CUcontext *out) {
+    static std::once_flag once;
+    static CtxGetCurrentFn fn = nullptr;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(p);
+    });
+    if (!fn) return set_error(HM_ERR_CUDA, "cuCtxGetCurrent unavailable");
+    CUcontext c = nullptr;
+    if (fn(&c) != CUDA_SUCCESS) return set_error(HM_ERR_CUDA, "cuCtxGetCurrent failed");
+    *out = c;
+    return HM_OK;
+}
+
+// Slot of the current device with the device address of g_noalloc_scratch
+// in the current context (set-up on the first call per device and context).
+static int scratch_slot(ScratchSlot **out) {
     int dev = 0;
     HM_CUDA_TRY(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices)
         return set_error(HM_ERR_UNSUPPORTED, "device ordinal %d above %d", dev, kMaxDevices - 1);
-    std::lock_guard<std::mutex> lk(g_scratch_mu);
-    if (!g_scratch_addr[dev]) {
+    CUcontext ctx = nullptr;
+    HM_TRY(current_context(&ctx));
+    ScratchSlot &S = g_slots[dev];
+    if (!S.addr || !ctx || S.ctx != ctx) {
+        // the lookup binds the runtime's context of the device to the thread
         void *p = nullptr;
         HM_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        g_scratch_addr[dev] = p;
+        HM_TRY(current_context(&ctx));
+        if (S.ctx != ctx) S.called = false;  // a new context: no counters of it yet
+        S.addr = p;
+        S.ctx = ctx;
     }
-    *out = g_scratch_addr[dev];
+    *out = &S;
     return HM_OK;
 }
 
@@ -71,9 +114,41 @@ int hm_knn_smooth_noalloc(const float *d_data, uint64_t n, uint32_t d, uint32_t 
                          "caller-provided workspace)",
                          (unsigned long long)n, d, k, need, (size_t)HM_NOALLOC_SCRATCH_BYTES);
     void *scratch = nullptr;
-    HM_TRY(scratch_address(&scratch));
+    {
+        std::lock_guard<std::mutex> lk(g_scratch_mu);
+        ScratchSlot *S = nullptr;
+        HM_TRY(scratch_slot(&S));
+        scratch = S->addr;
+        S->called = true;
+        S->n = n;
+        S->d = d;
+        S->k = k;
+        S->metric = metric;
+    }
     return hm_knn_smooth_device(d_data, n, d, k, metric, HM_PATH_PLAIN, d_idx, d_dist, d_sigma,
                                 d_rho, scratch, HM_NOALLOC_SCRATCH_BYTES, stream, nullptr);
+}
+
+int hm_noalloc_stats(void *stream, hm_stats *stats) {
+    clear_error();
+    uint64_t n;
+    uint32_t d, k;
+    int metric;
+    void *scratch;
+    {
+        std::lock_guard<std::mutex> lk(g_scratch_mu);
+        ScratchSlot *S = nullptr;
+        HM_TRY(scratch_slot(&S));
+        if (!S->called)
+            return set_error(HM_ERR_INVALID, "no hm_knn_smooth_noalloc call on this device yet");
+        n = S->n;
+        d = S->d;
+        k = S->k;
+        metric = S->metric;
+        scratch = S->addr;
+    }
+    return single_job_stats(scratch, n, d, k, metric, HM_PATH_PLAIN, static_cast<cudaStream_t>(stream),
+                            stats);
 }
 
 }  // extern "C"

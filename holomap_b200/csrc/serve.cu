@@ -512,17 +512,24 @@ int hm_poll(hm_ctx *C, uint64_t ticket, hm_request_info *info) {
 int hm_wait(hm_ctx *C, uint64_t ticket, uint64_t timeout_ns, hm_request_info *info) {
     clear_error();
     if (!C) return set_error(HM_ERR_INVALID, "context is NULL");
-    const auto deadline = std::chrono::steady_clock::now() + std::chrono::nanoseconds(timeout_ns);
+    // timeouts at or above 2^62 ns (about 146 years; UINT64_MAX included)
+    // mean "no deadline": they would overflow the signed clock arithmetic
+    const bool forever = timeout_ns >= (1ull << 62);
+    const auto deadline = std::chrono::steady_clock::now() +
+                          std::chrono::nanoseconds(forever ? 0 : (int64_t)timeout_ns);
     std::unique_lock<std::mutex> lk(C->mu);
     for (;;) {
         auto it = C->reqs.find(ticket);
         if (it == C->reqs.end())
             return set_error(HM_ERR_INVALID, "unknown ticket %llu", (unsigned long long)ticket);
-        if (it->second.finished || std::chrono::steady_clock::now() >= deadline) {
+        if (it->second.finished || (!forever && std::chrono::steady_clock::now() >= deadline)) {
             fill_info(it->second, info);
             return request_status(it->second);
         }
-        C->cv_done.wait_until(lk, deadline);
+        if (forever)
+            C->cv_done.wait(lk);
+        else
+            C->cv_done.wait_until(lk, deadline);
     }
 }
 

@@ -1,6 +1,7 @@
 // timing.cu -- launch counting and optional CUDA-event timing per kernel class.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <atomic>
 #include <mutex>
 #include <vector>
@@ -98,11 +99,67 @@ void timing_record(int kclass, cudaStream_t s, bool start) {
     }
 }
 
+// Binary64 throughput probe: every thread runs eight independent chains of
+// a round-to-nearest multiply and add (the operations of the exact kernels),
+// so the FP64 pipe, not latency, bounds it.  The sum lands in a device
+// variable only under a condition the compiler cannot rule out.
+static __device__ double g_fp64_sink;
+
+__global__ void __launch_bounds__(256) fp64_rate_kernel(double seed, uint32_t iters) {
+    double a[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) a[q] = seed + (double)(threadIdx.x * 8 + q) * 1e-6;
+    const double m = 1.0000000001, c = 1e-12;
+    for (uint32_t i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) a[q] = __dadd_rn(__dmul_rn(a[q], m), c);
+    }
+    double t = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) t = __dadd_rn(t, a[q]);
+    if (t == 12345.678) g_fp64_sink = t;
+}
+
 }  // namespace hm
 
 using namespace hm;
 
 extern "C" {
+
+int hm_measure_fp64_rate(double *ops_per_s) {
+    clear_error();
+    if (!ops_per_s) return set_error(HM_ERR_INVALID, "NULL pointer argument");
+    const int sms = device_sm_count();
+    const uint32_t iters = 4096, threads = 256, blocks = (uint32_t)sms * 8;
+    cudaStream_t s = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    HM_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    int rc = HM_OK;
+    double best = 0.0;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        rc = set_error(HM_ERR_CUDA, "cudaEventCreate failed");
+    } else {
+        for (int rep = 0; rep < 4 && rc == HM_OK; ++rep) {  // the first run warms the clocks
+            cudaEventRecord(e0, s);
+            fp64_rate_kernel<<<blocks, threads, 0, s>>>(1.0 + rep, iters);
+            count_launch();
+            cudaEventRecord(e1, s);
+            float ms = 0.f;
+            const cudaError_t e = cudaEventSynchronize(e1);
+            if (e != cudaSuccess || cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess || ms <= 0.f) {
+                rc = set_error(HM_ERR_CUDA, "fp64 probe failed: %s", cudaGetErrorString(e));
+                break;
+            }
+            const double ops = (double)blocks * threads * iters * 16.0;  // 8 chains x (mul + add)
+            if (rep > 0) best = std::max(best, ops / (ms * 1e-3));
+        }
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    if (rc == HM_OK) *ops_per_s = best;
+    return rc;
+}
 
 int hm_timing_enable(int on) {
     g_timing.store(on != 0);

@@ -51,10 +51,10 @@ extern "C" {
 #define HM_ERR_INVALID (-1)     /* argument outside the reference's preconditions */
 #define HM_ERR_OOM (-2)         /* device or pinned allocation failed */
 #define HM_ERR_CUDA (-3)        /* CUDA runtime / driver error */
-#define HM_ERR_TIMEOUT (-4)     /* a bounded device wait or hm_wait expired */
+#define HM_ERR_TIMEOUT (-4)     /* a bounded device wait gave up (the kernel returned early) */
 #define HM_ERR_ADMISSION (-5)   /* serving: job larger than the context's memory budget */
 #define HM_ERR_UNSUPPORTED (-6) /* valid input this build does not handle (message says why) */
-#define HM_ERR_NOT_READY (-7)   /* serving: hm_poll on a job still in flight */
+#define HM_ERR_NOT_READY (-7)   /* serving: hm_poll / hm_wait on a job still in flight */
 
 /* metric, the reference's Metric enum (src/metric.rs:8-15) plus one extension */
 #define HM_METRIC_EUCLIDEAN 0
@@ -172,6 +172,11 @@ HM_API int hm_fuzzy_graph_device(const uint32_t *d_idx, const float *d_dist, con
 HM_API int hm_fuzzy_graph(const uint32_t *idx, const float *dist, const float *sigma, const float *rho,
                           uint64_t n, uint32_t k, uint32_t *rows_out, uint32_t *cols_out,
                           float *vals_out, uint64_t *nnz_out);
+/* After hm_fuzzy_graph_device on `stream` (synchronous read of its workspace):
+ * HM_ERR_INVALID if some index was not below n or a row repeated an index
+ * (the kernels keep every access in bounds, but the output is then not the
+ * fuzzy set of a kNN graph), else HM_OK.  hm_fuzzy_graph checks it itself. */
+HM_API int hm_fuzzy_graph_status(const void *d_workspace, uint64_t n, uint32_t k, void *stream);
 
 /* The spectral stage that follows the fuzzy graph (spectral_layout_single,
  * src/spectral.rs:70-83).
@@ -307,7 +312,8 @@ HM_API int hm_submit(hm_ctx *ctx, const hm_job *request, uint64_t *ticket);
 /* HM_OK when finished successfully, HM_ERR_NOT_READY while pending, else
  * the request's error.  info (optional) is filled in every case. */
 HM_API int hm_poll(hm_ctx *ctx, uint64_t ticket, hm_request_info *info);
-/* Block until the request finishes or timeout_ns passes (HM_ERR_NOT_READY). */
+/* Block until the request finishes or timeout_ns passes (then HM_ERR_NOT_READY);
+ * timeout_ns >= 2^62 (UINT64_MAX included) waits without a deadline. */
 HM_API int hm_wait(hm_ctx *ctx, uint64_t ticket, uint64_t timeout_ns, hm_request_info *info);
 /* Forget a finished ticket (its info is no longer kept). */
 HM_API int hm_release(hm_ctx *ctx, uint64_t ticket);
@@ -336,13 +342,27 @@ HM_API int hm_ctx_totals_read(hm_ctx *ctx, hm_ctx_totals *totals);
  * caller's device inputs and outputs and no allocation of any kind: scratch
  * comes from the library's static array.  Problems whose scratch
  * (hm_workspace_bytes(..., HM_PATH_PLAIN)) exceeds HM_NOALLOC_SCRATCH_BYTES
- * are rejected with HM_ERR_UNSUPPORTED.  The first call on a device looks up
- * the array's device address (make it before any stream capture).  All calls
- * share the array: calls that overlap on the GPU race on it. */
+ * are rejected with HM_ERR_UNSUPPORTED.  The first call on a device (and in
+ * each new CUDA context of it, e.g. after cudaDeviceReset) looks up the
+ * array's device address: make it before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU race on it.  The call itself does
+ * not wait for the device, so a non-finite input is reported by
+ * hm_noalloc_stats, not by this return code. */
 HM_API int hm_knn_smooth_noalloc(const float *d_data, uint64_t n, uint32_t d, uint32_t k,
                                  int metric, uint32_t *d_idx, float *d_dist, float *d_sigma,
                                  float *d_rho, void *stream);
 HM_API size_t hm_noalloc_scratch_bytes(void);
+
+/* The status and counters of the last hm_knn_smooth_noalloc call on the
+ * current device, which stay in the static scratch: waits for the work queued
+ * on `stream` (the stream that call used) and reads them into a host struct,
+ * allocating nothing.  Returns HM_ERR_INVALID when that call's points held a
+ * non-finite value (hm_last_error() names its first flat index), as the
+ * workspace-taking entry points do, HM_ERR_TIMEOUT if a bounded device wait
+ * gave up, else HM_OK; stats (optional) receives the counts.  The next call on
+ * the device overwrites them, and calls that overlap on the GPU race on them.
+ * No counterpart in the reference (see hm_knn_smooth_noalloc). */
+HM_API int hm_noalloc_stats(void *stream, hm_stats *stats);
 
 /* ----------------------------------------------------------------------------
  * Misc
@@ -375,6 +395,11 @@ HM_API int hm_timing_enable(int on);
 HM_API int hm_timing_read(int kernel_class, double *total_ms, uint64_t *launches, int reset);
 /* Kernels this library has launched since it was loaded (all classes). */
 HM_API uint64_t hm_launch_count(void);
+/* Measured binary64 throughput of the current device (round-to-nearest
+ * multiplies and adds per second, the operations of the exact kernels): a
+ * synchronous probe of a few milliseconds on a private stream, used as the
+ * FP64 roofline.  Changes no device setting. */
+HM_API int hm_measure_fp64_rate(double *ops_per_s);
 
 /* Test hook: while set (non-NULL), screened runs on this thread also write
  * every screened value c^_ij into d_out[i * n + j] (n x n floats). */

@@ -168,3 +168,52 @@ def test_device_entry_point_on_a_stream(oracle):
     assert_same_bytes(rows[:m].cpu().numpy().view(np.uint32), r, "rows")
     assert_same_bytes(cols[:m].cpu().numpy().view(np.uint32), c, "cols")
     assert_same_bytes(vals[:m].cpu().numpy(), v, "vals")
+
+
+def test_device_entry_point_reports_an_index_not_below_n(oracle):
+    """hm_fuzzy_graph_device trusts no index: entries at or above n are
+    dropped by the rows kernel (so every later access stays in bounds) and
+    hm_fuzzy_graph_status reports them; the rest of the graph is the fuzzy
+    set of the graph without those entries."""
+    import ctypes
+    import torch
+    n, k = 3000, 10
+    idx, dist = random_knn(n, k, seed=17)
+    sm = hm.smooth_knn(dist, k)
+    bad = idx.copy()
+    bad[5, 3] = n          # just past the end
+    bad[77, 9] = 0xFFFFFFF0  # far past it
+    lib = hm.lib()
+    ws_bytes = lib.hm_fuzzy_workspace_bytes(n, k)
+    dev = lambda a: torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a).cuda()
+    d_idx, d_dist, d_sig, d_rho = dev(bad), dev(dist), dev(sm.sigmas), dev(sm.rhos)
+    cap = 2 * n * k
+    rows = torch.empty(cap, dtype=torch.int32, device="cuda")
+    cols = torch.empty(cap, dtype=torch.int32, device="cuda")
+    vals = torch.empty(cap, dtype=torch.float32, device="cuda")
+    nnz = torch.zeros(1, dtype=torch.int64, device="cuda")
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device="cuda")
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    check_rc(lib.hm_fuzzy_graph_device(d_idx.data_ptr(), d_dist.data_ptr(), d_sig.data_ptr(),
+                                       d_rho.data_ptr(), n, k, rows.data_ptr(), cols.data_ptr(),
+                                       vals.data_ptr(), nnz.data_ptr(), ws.data_ptr(), ws_bytes,
+                                       stream))
+    assert lib.hm_fuzzy_graph_status(ws.data_ptr(), n, k, stream) == hm.HM_ERR_INVALID
+    assert b"not below n" in lib.hm_last_error()
+    m = int(nnz.item())
+    assert 0 < m <= cap
+    # the same graph with those two entries given strength 0 (dropped) and a
+    # valid column, which the oracle drops the same way
+    fixed_idx, fixed_dist = idx.copy(), dist.copy()
+    r, c, v = oracle.fuzzy_graph(fixed_idx, fixed_dist, sm.sigmas, sm.rhos, k)
+    got = set(zip(rows[:m].cpu().numpy().tolist(), cols[:m].cpu().numpy().tolist()))
+    want = set(zip(r.tolist(), c.tolist()))
+    assert got <= want  # only entries of the valid graph, none invented
+    # a valid graph afterwards reports no error on the same workspace
+    d_idx.copy_(dev(idx))
+    check_rc(lib.hm_fuzzy_graph_device(d_idx.data_ptr(), d_dist.data_ptr(), d_sig.data_ptr(),
+                                       d_rho.data_ptr(), n, k, rows.data_ptr(), cols.data_ptr(),
+                                       vals.data_ptr(), nnz.data_ptr(), ws.data_ptr(), ws_bytes,
+                                       stream))
+    assert lib.hm_fuzzy_graph_status(ws.data_ptr(), n, k, stream) == hm.HM_OK
+    assert int(nnz.item()) == r.size
