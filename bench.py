@@ -421,7 +421,10 @@ class SingleRunner:
                 "zero_rho_rows": int(st.zero_rho_rows), "screen_band": st.screen_band}
 
     def config(self):
-        return config_of(self.wl)
+        from holomap_b200.autotune import describe
+        c = config_of(self.wl)
+        c["autotune"] = describe(self.wl.n, self.wl.d, self.wl.k, self.wl.metric)
+        return c
 
     def screened_work(self):
         """[(n, d)] of the screened problems, [(n, d, metric)] of the exact ones."""

@@ -1,0 +1,232 @@
+"""The autotuner: measures every path of the kNN + smooth-kNN pipeline on a
+grid of problem shapes on the GPU and writes the table that HM_PATH_AUTO
+reads.
+
+For every grid point (N, d, k, metric) it times, with CUDA events on the
+launching stream, one full kNN + smooth-kNN run of
+
+* the plain exact binary64 path, and
+* each tensor-core screen (BF16, TF32, split-BF16) with the threshold pass
+  sampling 1/4, 1/8 and 1/16 of the columns,
+
+on seeded Gaussian-mixture data of that shape, checks that every screened
+result equals the plain path's bytes, and records the fastest choice.  Two
+files are written:
+
+* ``holomap_b200/autotune_table.json`` -- every measurement, the choice per
+  grid point, and the device and command that produced them;
+* ``holomap_b200/csrc/autotune_table.inc`` -- the same choices as a C table
+  compiled into the library (``hm_autotune_path`` and the screen planner look
+  up the nearest grid point).
+
+    python -m holomap_b200.autotune              # sweep on cuda:0, write both files
+    python -m holomap_b200.autotune --emit-only  # regenerate the .inc from the JSON
+
+Manhattan (no inner-product form), k > 64 and d > 2048 always take the plain
+path: no screen applies.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import math
+import statistics
+import time
+from pathlib import Path
+
+import numpy as np
+
+PKG = Path(__file__).resolve().parent
+JSON_PATH = PKG / "autotune_table.json"
+INC_PATH = PKG / "csrc" / "autotune_table.inc"
+
+GRID_N = [256, 512, 1024, 2048, 4096, 8192, 16384, 32768, 50000]
+GRID_D = [16, 32, 50, 64, 128, 300, 384]
+GRID_K = [15, 30]
+METRICS = ["euclidean", "cosine"]
+SCREENS = ["screen_bf16", "screen_tf32", "screen_bf16x3"]
+SEED_DIVS = [4, 8, 16]
+PATH_CODE = {"plain": 1, "screen_bf16": 2, "screen_tf32": 3, "screen_bf16x3": 4}
+
+
+def hand_rule(n: int, d: int, k: int, metric: str) -> tuple[str, int]:
+    """The choice used before any measurement exists (and the shape of the
+    table when the sweep has not run): plain below 512 points, split-BF16 up
+    to d = 256, then BF16 (cosine) or TF32 (euclidean); an eighth sampled."""
+    if n < 512:
+        return "plain", 8
+    if d <= 256:
+        return "screen_bf16x3", 8
+    return ("screen_bf16" if metric == "cosine" else "screen_tf32"), 8
+
+
+def _pool(d: int, n: int, seed: int) -> np.ndarray:
+    from .synth import _rng, gaussian_mixture
+    g = _rng(900000 + 10 * d + seed)
+    clusters = int(g.integers(3, 21))
+    return np.ascontiguousarray(gaussian_mixture(g, n, d, clusters, 4.0, 0.3, 3.0).astype(np.float32))
+
+
+def _time_run(prob, x, reps: int) -> float:
+    import torch
+    s = torch.cuda.current_stream()
+    prob.run(x, s)  # warm: workspace first touch, plan
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        prob.run(x, s)
+        e1.record(s)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return statistics.median(ms)
+
+
+def sweep(grid_n=GRID_N, grid_d=GRID_D, grid_k=GRID_K, metrics=METRICS, verbose=True) -> dict:
+    import torch
+
+    from . import _lib
+    from .device import DeviceKnnProblem
+    lib = _lib.lib()
+    entries = []
+    t_start = time.time()
+    for metric in metrics:
+        for d in grid_d:
+            pool = _pool(d, max(grid_n), 0 if metric == "euclidean" else 1)
+            xpool = torch.from_numpy(pool).cuda()
+            for k in grid_k:
+                for n in grid_n:
+                    x = xpool[:n].contiguous()
+                    times, exact = {}, True
+                    plain = DeviceKnnProblem(n, d, k, metric, "plain")
+                    reps = 2 if n * n * d > 2e11 else 5
+                    times["plain"] = _time_run(plain, x, reps)
+                    ref = (plain.idx.cpu().numpy(), plain.dist.cpu().numpy().view(np.uint32),
+                           plain.sigma.cpu().numpy().view(np.uint32))
+                    del plain
+                    for path in SCREENS:
+                        for sd in SEED_DIVS:
+                            _lib.check(lib.hm_tuning_override(sd))
+                            try:
+                                p = DeviceKnnProblem(n, d, k, metric, path)
+                                t = _time_run(p, x, 5)
+                                got = (p.idx.cpu().numpy(), p.dist.cpu().numpy().view(np.uint32),
+                                       p.sigma.cpu().numpy().view(np.uint32))
+                                same = all(np.array_equal(a, b) for a, b in zip(got, ref))
+                                del p
+                            finally:
+                                _lib.check(lib.hm_tuning_override(0))
+                            times[f"{path}/{sd}"] = t
+                            if not same:
+                                exact = False
+                                times[f"{path}/{sd}"] = None
+                    valid = {c: t for c, t in times.items() if t is not None}
+                    best = min(valid, key=valid.get)
+                    path, sd = (best.split("/") + ["8"])[:2]
+                    e = {"n": n, "d": d, "k": k, "metric": metric, "times_ms": times, "best": path,
+                         "seed_div": int(sd), "all_paths_equal_plain": exact}
+                    entries.append(e)
+                    if verbose:
+                        print(f"{metric:9s} d={d:4d} k={k:2d} n={n:6d}  best {best:18s} "
+                              f"{valid[best]:9.3f} ms  (plain {times['plain']:9.3f} ms)", flush=True)
+    props = torch.cuda.get_device_properties(0)
+    return {
+        "device": props.name, "sms": props.multi_processor_count,
+        "measured": datetime.datetime.now(datetime.timezone.utc).strftime("%Y-%m-%d %H:%M UTC"),
+        "command": "python -m holomap_b200.autotune",
+        "timing": "median of CUDA-event times of full kNN + smooth-kNN runs on device-resident "
+                  "inputs (one warm-up run first)",
+        "data": "seeded Gaussian mixtures (3-20 clusters, centres N(0, 16 I), sigma U[0.3, 3]); "
+                "prefixes of one 50,000-point pool per (d, metric)",
+        "sweep_seconds": round(time.time() - t_start, 1),
+        "grid": {"n": list(grid_n), "d": list(grid_d), "k": list(grid_k), "metric": list(metrics)},
+        "entries": entries,
+    }
+
+
+def table_from(doc: dict | None) -> tuple[dict, list, list, list]:
+    """(choice[(metric, k, d, n)] = (path, seed_div), grid n, d, k)."""
+    if doc is None:
+        gn, gd, gk = GRID_N, GRID_D, GRID_K
+        choice = {(m, k, d, n): hand_rule(n, d, k, m) for m in METRICS for k in gk for d in gd for n in gn}
+        return choice, gn, gd, gk
+    g = doc["grid"]
+    choice = {(e["metric"], e["k"], e["d"], e["n"]): (e["best"], e["seed_div"]) for e in doc["entries"]}
+    return choice, g["n"], g["d"], g["k"]
+
+
+def _nearest(grid, v) -> int:
+    return min(grid, key=lambda g: abs(math.log(max(v, 1) / g)))
+
+
+def describe(n: int, d: int, k: int, metric: str) -> dict:
+    """The table entry a problem resolves to (the library's lookup: nearest
+    grid point by ratio in n, d and k), with its measured times."""
+    if metric == "manhattan" or k > 64 or d > 2048:
+        return {"choice": "plain", "reason": "no screen applies"}
+    doc = json.loads(JSON_PATH.read_text()) if JSON_PATH.exists() else None
+    choice, gn, gd, gk = table_from(doc)
+    key = (metric, _nearest(gk, k), _nearest(gd, d), _nearest(gn, n))
+    path, sd = choice[key]
+    out = {"grid_point": {"metric": key[0], "k": key[1], "d": key[2], "n": key[3]},
+           "choice": path, "seed_div": sd,
+           "table": f"measured {doc['measured']} on {doc['device']}" if doc else "hand rule (no measurement)"}
+    if doc:
+        for e in doc["entries"]:
+            if (e["metric"], e["k"], e["d"], e["n"]) == key:
+                out["times_ms"] = e["times_ms"]
+    return out
+
+
+def emit_inc(doc: dict | None, path: Path = INC_PATH) -> None:
+    choice, gn, gd, gk = table_from(doc)
+    src = doc["measured"] + " on " + doc["device"] if doc else "no measurement yet (the hand rule)"
+    lines = [
+        "// autotune_table.inc -- generated by holomap_b200/autotune.py from",
+        "// holomap_b200/autotune_table.json; do not edit by hand.",
+        f"// Source: {src}.",
+        "// kTune[metric][k][d][n] = path | seed_div << 8 at the grid points below",
+        "// (metric 0 euclidean, 1 cosine).",
+        "#pragma once",
+        f"static const uint32_t kTuneN[{len(gn)}] = {{{', '.join(map(str, gn))}}};",
+        f"static const uint32_t kTuneD[{len(gd)}] = {{{', '.join(map(str, gd))}}};",
+        f"static const uint32_t kTuneK[{len(gk)}] = {{{', '.join(map(str, gk))}}};",
+        f"static const uint16_t kTune[2][{len(gk)}][{len(gd)}][{len(gn)}] = {{",
+    ]
+    for m in METRICS:
+        lines.append("    {")
+        for k in gk:
+            lines.append("        {")
+            for d in gd:
+                row = []
+                for n in gn:
+                    p, sd = choice[(m, k, d, n)]
+                    row.append(str(PATH_CODE[p] | (int(sd) << 8)))
+                lines.append("            {" + ", ".join(row) + "},")
+            lines.append("        },")
+        lines.append("    },")
+    lines.append("};")
+    path.write_text("\n".join(lines) + "\n")
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--emit-only", action="store_true",
+                    help="regenerate the C table from the committed JSON (no GPU)")
+    ap.add_argument("--out", default=str(JSON_PATH))
+    a = ap.parse_args()
+    if a.emit_only:
+        doc = json.loads(Path(a.out).read_text()) if Path(a.out).exists() else None
+        emit_inc(doc)
+        return 0
+    doc = sweep()
+    Path(a.out).write_text(json.dumps(doc, indent=1) + "\n")
+    emit_inc(doc)
+    print(f"wrote {a.out} and {INC_PATH}")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

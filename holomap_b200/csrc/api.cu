@@ -265,9 +265,12 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
                 P.part_tiles = (P.col_tiles + parts - 1) / parts;
                 P.parts = (P.col_tiles + P.part_tiles - 1) / P.part_tiles;
             }
-            // threshold-pass sample: an eighth of the columns, at least 2048
-            // (all of them for small jobs), spread over the parts
-            const uint64_t seed_cols = std::max<uint64_t>(P.spec.n / 8, 2048);
+            // threshold-pass sample: 1/seed_div of the columns (the autotuner
+            // table's choice for the shape), at least 2048 (all of them for
+            // small jobs), spread over the parts
+            uint32_t seed_div = 8;
+            autotune_choice(P.spec.n, P.spec.d, P.spec.k, P.spec.metric, &seed_div);
+            const uint64_t seed_cols = std::max<uint64_t>(P.spec.n / std::max<uint32_t>(seed_div, 1), 2048);
             P.seed_tiles = std::min<uint32_t>(
                 P.part_tiles, (uint32_t)((seed_cols + (uint64_t)SC_BN * P.parts - 1) / ((uint64_t)SC_BN * P.parts)));
             P.seed_tiles = std::max<uint32_t>(P.seed_tiles, 1);
@@ -547,7 +550,7 @@ static int run_batch(hm_batch &B, cudaStream_t s) {
     const uint32_t *job_blocks = at<uint32_t>(ws, B.off_job_blocks);
     const uint32_t blocks = B.job_blocks.back();
 
-    HM_TRY(launch_prep_jobs(jobs, njobs, job_blocks, blocks, PREP_CHECK_AND_NORMS, s));
+    HM_TRY(launch_prep_jobs(jobs, njobs, job_blocks, blocks, PREP_CHECK_AND_NORMS, s, row_starts, B.all_rows));
     if (B.any_plain) HM_TRY(launch_prep_jobs(jobs, njobs, job_blocks, blocks, PREP_X64_EXACT, s));
     for (int m = 0; m < 3; ++m) {
         if (B.items[m].empty()) continue;

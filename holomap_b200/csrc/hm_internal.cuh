@@ -207,6 +207,10 @@ __device__ __forceinline__ uint32_t find_job(const uint32_t *starts, uint32_t nj
 
 int kpl_for_k(uint32_t k);  // 1, 2, 4, 8 or 0 if k > 256
 
+// The autotuner table's path for a problem and (seed_div) the fraction
+// 1/seed_div of the columns the screen's threshold pass samples.
+int autotune_choice(uint64_t n, uint32_t d, uint32_t k, int metric, uint32_t *seed_div);
+
 // ------------------------------------------------------------- plain path
 constexpr int PL_BM = 32;     // rows per CTA (8 warps x 4 rows)
 constexpr int PL_BN = 128;    // columns per tile (32 lanes x 4)
@@ -229,11 +233,14 @@ struct PlainWork {
     uint32_t fb_njobs;
 };
 
-// Input check + binary64 copy + cosine row norms for every job.  x64_gate:
-// build the binary64 copy only for exact-path jobs, or (fallback mode) only
-// for screened jobs whose overflow count is nonzero.
+// PREP_CHECK_AND_NORMS: zeroes the job counters, checks every input for
+// finiteness and forms the cosine row norms (all rows of every job;
+// row_starts / all_rows: the all-rows space).  PREP_X64_*: the binary64 copy
+// of the points, only for exact-path jobs, or (fallback mode) only for
+// screened jobs whose overflow count is nonzero.
 int launch_prep_jobs(const JobDev *jobs, uint32_t njobs, const uint32_t *job_blocks,
-                     uint32_t total_blocks, int mode, cudaStream_t s);
+                     uint32_t total_blocks, int mode, cudaStream_t s, const uint32_t *row_starts = nullptr,
+                     uint32_t all_rows = 0);
 enum { PREP_CHECK_AND_NORMS = 0, PREP_X64_EXACT = 1, PREP_X64_FALLBACK = 2 };
 
 int launch_plain(const PlainWork &w, int metric, cudaStream_t s);

@@ -42,8 +42,9 @@ __global__ void init_counters_kernel(JobDev *jobs, uint32_t njobs) {
     *jobs[j].cnt = c;
 }
 
-// Blocks are dealt to jobs by `job_blocks` (prefix offsets); each job's blocks
-// stride over that job's elements / rows.
+// Binary64 copies of the points (exact-path jobs, or screened jobs with rows
+// for the exact fallback).  Blocks are dealt to jobs by `job_blocks` (prefix
+// offsets); each job's blocks stride over that job's elements.
 __global__ void __launch_bounds__(256) prep_jobs_kernel(const JobDev *__restrict__ jobs, uint32_t njobs,
                                                         const uint32_t *__restrict__ job_blocks,
                                                         int mode) {
@@ -53,28 +54,6 @@ __global__ void __launch_bounds__(256) prep_jobs_kernel(const JobDev *__restrict
     const uint32_t nb = job_blocks[jb + 1] - job_blocks[jb];
     const size_t stride = (size_t)nb * blockDim.x;
     const size_t t0 = (size_t)lb * blockDim.x + threadIdx.x;
-    if (mode == PREP_CHECK_AND_NORMS) {
-        const size_t total = (size_t)J.n * J.d;
-        for (size_t t = t0; t < total; t += stride)
-            if (!isfinite(J.x[t])) atomicMin(&J.cnt->nonfinite_min, (uint32_t)(t < 0xfffffffeull ? t : 0xfffffffeull));
-        if (J.metric == HM_METRIC_COSINE) {
-            // sqrt of the sequential binary64 sum of squares, as the cosine
-            // metric forms na / nb (src/metric.rs:61-66, :69)
-            for (size_t r = t0; r < J.n_pad; r += stride) {
-                double v = 0.0;
-                if (r < J.n) {
-                    const float *row = J.x + r * J.d;
-                    for (uint32_t c = 0; c < J.d; ++c) {
-                        const double e = (double)row[c];
-                        v = __dadd_rn(v, __dmul_rn(e, e));
-                    }
-                    v = __dsqrt_rn(v);
-                }
-                J.rnorm[r] = v;
-            }
-        }
-        return;
-    }
     if (mode == PREP_X64_EXACT && J.path != HM_PATH_PLAIN) return;
     if (mode == PREP_X64_FALLBACK && (J.path == HM_PATH_PLAIN || J.cnt->ovf_count == 0)) return;
     const size_t total = (size_t)J.n_pad * J.ldd;
@@ -84,13 +63,80 @@ __global__ void __launch_bounds__(256) prep_jobs_kernel(const JobDev *__restrict
     }
 }
 
+// Input check and cosine row norms, one warp per 32 consecutive rows of the
+// all-rows space (rows of several jobs may share a warp).  The warp stages its
+// rows 32 dimensions at a time through shared memory with coalesced 128-byte
+// reads (one row per load instruction), and lane r then walks row r's chunk in
+// dimension order: the sequential binary64 sum of squares of the cosine
+// metric's na / nb (src/metric.rs:61-66, :69), whose square root is kept per
+// row.  Every value read is also checked for finiteness (the smallest flat
+// index of a non-finite value per job, as HolomapError::NonFiniteInput
+// reports it, src/api.rs:36-43).
+constexpr int NRM_WARPS = 8;
+__global__ void __launch_bounds__(NRM_WARPS * 32) check_norms_kernel(const JobDev *__restrict__ jobs,
+                                                                    uint32_t njobs,
+                                                                    const uint32_t *__restrict__ row_starts,
+                                                                    uint32_t rows) {
+    __shared__ float tile[NRM_WARPS][32][33];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint32_t ar0 = (blockIdx.x * NRM_WARPS + warp) * 32;
+    if (ar0 >= rows) return;
+    const uint32_t ar = ar0 + lane;
+    const bool mine = ar < rows;
+    const uint32_t jb = mine ? (row_starts ? find_job(row_starts, njobs, ar) : 0u) : 0u;
+    const JobDev &J = jobs[jb];
+    const uint32_t row = mine ? ar - J.arow0 : 0u;
+    const uint32_t d = mine ? J.d : 0u;
+    const float *xrow = J.x + (size_t)row * d;
+    const bool cos = mine && J.metric == HM_METRIC_COSINE;
+    const uint32_t dmax = __reduce_max_sync(0xffffffffu, d);
+    double acc = 0.0;
+    for (uint32_t c0 = 0; c0 < dmax; c0 += 32) {
+        // row i of the warp, dimension c0 + lane: coalesced per row
+        for (int i = 0; i < 32; ++i) {
+            const float *src = reinterpret_cast<const float *>(
+                __shfl_sync(0xffffffffu, reinterpret_cast<uintptr_t>(xrow), i));
+            const uint32_t di = __shfl_sync(0xffffffffu, d, i);
+            const uint32_t ri = __shfl_sync(0xffffffffu, row, i);
+            const uint32_t ji = __shfl_sync(0xffffffffu, jb, i);
+            float v = 0.0f;
+            if (c0 + lane < di) {
+                v = src[c0 + lane];
+                if (!isfinite(v))
+                    atomicMin(&jobs[ji].cnt->nonfinite_min,
+                              (uint32_t)min((size_t)ri * di + c0 + lane, (size_t)0xfffffffeull));
+            }
+            tile[warp][i][lane] = v;
+        }
+        __syncwarp();
+        if (cos) {
+            const uint32_t tmax = min(32u, d - min(d, c0));
+            for (uint32_t t = 0; t < tmax; ++t) {
+                const double e = (double)tile[warp][lane][t];
+                acc = __dadd_rn(acc, __dmul_rn(e, e));
+            }
+        }
+        __syncwarp();
+    }
+    if (cos) J.rnorm[row] = __dsqrt_rn(acc);
+    // the plain path reads the norms of its padding rows [n, n_pad): zeros
+    if (cos && row == J.n - 1)
+        for (uint32_t r = J.n; r < J.n_pad; ++r) J.rnorm[r] = 0.0;
+}
+
 int launch_prep_jobs(const JobDev *jobs, uint32_t njobs, const uint32_t *job_blocks,
-                     uint32_t total_blocks, int mode, cudaStream_t s) {
+                     uint32_t total_blocks, int mode, cudaStream_t s, const uint32_t *row_starts,
+                     uint32_t all_rows) {
     ScopedKernelTimer timer(HM_KCLASS_PREP, s);
     if (mode == PREP_CHECK_AND_NORMS) {
         init_counters_kernel<<<(njobs + 127) / 128, 128, 0, s>>>(const_cast<JobDev *>(jobs), njobs);
         HM_CUDA_TRY(cudaGetLastError());
-        count_launch();
+        const uint32_t warps = (all_rows + 31) / 32;
+        check_norms_kernel<<<(warps + NRM_WARPS - 1) / NRM_WARPS, NRM_WARPS * 32, 0, s>>>(jobs, njobs, row_starts,
+                                                                                        all_rows);
+        HM_CUDA_TRY(cudaGetLastError());
+        count_launch(2);
+        return HM_OK;
     }
     prep_jobs_kernel<<<total_blocks, 256, 0, s>>>(jobs, njobs, job_blocks, mode);
     HM_CUDA_TRY(cudaGetLastError());

@@ -1,5 +1,5 @@
-// screen.cu -- TMA tensor maps of the screen operands, the autotuner table
-// that picks a path per (n, d, k, metric), and the screened-values test hook.
+// screen.cu -- TMA tensor maps of the screen operands and the
+// screened-values test hook.
 //
 // The screened pipeline of one group of jobs is (see api.cu for the order):
 //   screen prep   operands + binary64 error statistics (screen_prep.cu)
@@ -66,21 +66,6 @@ int make_operand_map(CUtensorMap *m, void *base, uint64_t rows, uint32_t kpmax, 
 using namespace hm;
 
 extern "C" {
-
-// Autotuner table: the path HM_PATH_AUTO takes.  Screened paths need an inner
-// product form (euclidean, cosine), k <= 64 and d <= 2048.  Below 512 points
-// the exact pass is a few microseconds and the screen's extra launches do not
-// pay.  Up to d = 256 the screen is bound by its per-column epilogue, not by
-// the tensor cores, so the split-bf16 operand (three products, error ~2^-16
-// of the norms) costs little over one product and keeps the keep band tight
-// for tightly clustered data; above that, bf16 (cosine: unit vectors, band
-// ~2^-7) or tf32 (euclidean) single products.
-int hm_autotune_path(uint64_t n, uint32_t d, uint32_t k, int metric) {
-    if (metric == HM_METRIC_MANHATTAN || k > 64 || d > 2048 || n < 512) return HM_PATH_PLAIN;
-    if (d <= 256) return HM_PATH_SCREEN_BF16X3;
-    if (metric == HM_METRIC_COSINE) return HM_PATH_SCREEN_BF16;
-    return HM_PATH_SCREEN_TF32;
-}
 
 int hm_debug_set_screen_dump(float *d_out) {
     g_debug_dump = d_out;

@@ -520,10 +520,13 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                                 }
                             }
                             const float tl = arr[KP - 1];
-                            if (tl < published) {  // share with the row's other lists
-                                const uint32_t o = ord32(tl);
-                                const uint32_t prev = atomicMin(G.rowthr + gr, o);
-                                tglob = fminf(tglob, unord32(prev < o ? prev : o));
+                            if (tl < published) {
+                                // share with the row's other lists: a reduction
+                                // whose result is not waited for (the other
+                                // lists' values arrive through tnext, loaded a
+                                // tile ahead)
+                                atomicMin(G.rowthr + gr, ord32(tl));
+                                tglob = fminf(tglob, tl);
                                 published = tl;
                             }
                         }

@@ -243,13 +243,8 @@ __global__ void __launch_bounds__(256) operand_kernel(const JobDev *__restrict__
     }
 }
 
-// Keep band 2E_i per row (see screen.cuh for the terms).
-__global__ void band_kernel(const JobDev *__restrict__ jobs, const GroupDev *__restrict__ Gp) {
-    const GroupDev &G = *Gp;
-    const uint32_t gr = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gr >= G.rows) return;
-    const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
-    if (gr - J.row0 >= J.n) return;  // padding between jobs
+// Keep band of one row (binary32 bits, rounded up), written to G.band.
+__device__ __forceinline__ uint32_t band_of_row(const JobDev &J, const GroupDev &G, uint32_t gr) {
     const unsigned long long *maxb = J.cnt->maxb;
     const RowStat st = G.rowstat[gr];
     const double Umax = __longlong_as_double((long long)maxb[0]);
@@ -275,8 +270,24 @@ __global__ void band_kernel(const JobDev *__restrict__ jobs, const GroupDev *__r
     const double B = 2.0 * E * (1.0 + 0x1p-10);
     const float bf = __double2float_ru(B);
     G.band[gr] = bf;
-    atomicMax(&J.cnt->band_max_bits, __float_as_uint(bf));
+    return __float_as_uint(bf);
 }
+
+// Keep band 2E_i per row (see screen.cuh for the terms).
+__global__ void band_kernel(const JobDev *__restrict__ jobs, const GroupDev *__restrict__ Gp) {
+    const GroupDev &G = *Gp;
+    // a warp's 32 group rows belong to one job (each job's rows start
+    // 32-aligned; G.rows is a multiple of 32)
+    const uint32_t gr = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gr - (threadIdx.x & 31) >= G.rows) return;  // whole warps
+    const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
+    const bool real = gr < G.rows && gr - J.row0 < J.n;  // not padding between jobs
+    uint32_t bits = 0;
+    if (real) bits = band_of_row(J, G, gr);
+    bits = __reduce_max_sync(0xffffffffu, bits);  // non-negative floats order like their bits
+    if ((threadIdx.x & 31) == 0 && bits) atomicMax(&J.cnt->band_max_bits, bits);
+}
+
 
 int launch_screen_prep(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, cudaStream_t s) {
     ScopedKernelTimer timer(HM_KCLASS_PREP, s);

@@ -374,8 +374,16 @@ HM_API const char *hm_last_error(void);
 /* HM_ABI_VERSION of the loaded library. */
 HM_API int hm_abi_version(void);
 
-/* The path HM_PATH_AUTO resolves to for this problem (autotuner table). */
+/* The path HM_PATH_AUTO resolves to for this problem: the choice of the
+ * nearest grid point of the autotuner table, measured on a B200 by
+ * holomap_b200/autotune.py (holomap_b200/autotune_table.json); plain where
+ * no screen applies (manhattan, k > 64, d > 2048). */
 HM_API int hm_autotune_path(uint64_t n, uint32_t d, uint32_t k, int metric);
+/* Autotuner sweep hook (no reference counterpart): while seed_div is nonzero,
+ * screened plans made on this thread sample 1/seed_div of the columns in the
+ * screen's threshold pass instead of the table's fraction; 0 restores the
+ * table.  The results do not depend on it, only the speed. */
+HM_API int hm_tuning_override(int seed_div);
 
 /* ----------------------------------------------------------------------------
  * Instrumentation (no reference counterpart; the reference has no timers on

@@ -100,19 +100,53 @@ def test_row_shard_ranges_are_validated_on_cpu():
         assert "query rows" in lib.hm_last_error().decode()
 
 
-def test_autotune_table():
-    """The autotuner's table (hm_autotune_path): plain where no screen
-    applies or pays, split-bf16 up to d = 256, then bf16 (cosine) / tf32."""
+def _autotune_doc():
+    import json
+    from holomap_b200 import autotune
+    return json.loads(autotune.JSON_PATH.read_text()) if autotune.JSON_PATH.exists() else None
+
+
+def test_autotune_table_is_the_committed_measurement():
+    """hm_autotune_path returns, at every grid point, the choice recorded in
+    holomap_b200/autotune_table.json (the library's C table is generated from
+    it), and the generated table is current."""
+    from holomap_b200 import autotune
+    doc = _autotune_doc()
+    choice, gn, gd, gk = autotune.table_from(doc)
+    for (metric, k, d, n), (path, _) in choice.items():
+        assert hm.autotune_path(n, d, k, metric) == hm.KnnPath.parse(path), (metric, k, d, n)
+    import tempfile
+    from pathlib import Path
+    with tempfile.TemporaryDirectory() as t:
+        fresh = Path(t) / "table.inc"
+        autotune.emit_inc(doc, fresh)
+        assert fresh.read_text() == autotune.INC_PATH.read_text(), "autotune_table.inc is stale"
+
+
+def test_autotune_covers_the_benchmark_shapes():
+    """Every workload shape resolves to a path; where no screen applies the
+    path is plain."""
     at = hm.autotune_path
     P = hm.KnnPath
     assert at(50000, 300, 15, "manhattan") == P.PLAIN      # no inner-product form
     assert at(50000, 384, 65, "cosine") == P.PLAIN         # k above the screen's 64
     assert at(50000, 4096, 15, "euclidean") == P.PLAIN     # d above 2048
-    assert at(511, 50, 15, "euclidean") == P.PLAIN         # too small to pay
-    assert at(1000, 50, 15, "euclidean") == P.SCREEN_BF16X3
-    assert at(20000, 256, 15, "cosine") == P.SCREEN_BF16X3
-    assert at(50000, 384, 30, "cosine") == P.SCREEN_BF16
-    assert at(50000, 300, 15, "euclidean") == P.SCREEN_TF32
+    shapes = [(1000, 50, 15, "euclidean"), (20000, 128, 15, "euclidean"), (50000, 384, 30, "cosine")]
+    shapes += [(n, d, 15, m) for n in (200, 1000, 8000) for d in (16, 50, 128) for m in ("euclidean", "cosine")]
+    shapes += [(n, d, k, m) for n in (500, 5000, 50000) for d in (32, 64, 300) for k in (15, 30)
+               for m in ("euclidean", "cosine")]
+    for n, d, k, m in shapes:
+        p = at(n, d, k, m)
+        assert p in (P.PLAIN, P.SCREEN_BF16, P.SCREEN_TF32, P.SCREEN_BF16X3)
+        assert hm.workspace_bytes(n, d, k, m, "auto") > 0
+
+
+def test_tuning_override_bounds():
+    lib = hm.lib()
+    assert lib.hm_tuning_override(8) == 0
+    assert lib.hm_tuning_override(0) == 0
+    assert lib.hm_tuning_override(-1) == hm.HM_ERR_INVALID
+    assert lib.hm_tuning_override(65) == hm.HM_ERR_INVALID
 
 
 def test_every_screened_path_plans_for_the_benchmark_shapes():
