@@ -441,6 +441,158 @@ class SingleRunner:
         return single_parity(self.wl, out, threads)
 
 
+class ShardedRunner:
+    """One dataset split by query rows over the ranks (N > 1): rank r builds
+    the kNN rows of its contiguous shard against all n points
+    (hm_knn_rows_device), the shards' indices and distances are all-gathered
+    over NCCL (the one exchange of the path), every rank calibrates its own
+    rows against the gathered distance matrix (hm_smooth_knn_rows_device: a
+    rho == 0 row's floor needs the mean of all n * k distances) and the
+    shards' sigmas and rhos are all-gathered.  Every rank ends the step with
+    the whole graph and calibration; the total work is one graph per step
+    (strong scaling)."""
+
+    def __init__(self, wl, path, dev, world, rank):
+        import ctypes
+
+        import torch
+
+        import holomap_b200 as hm
+        from holomap_b200 import _lib
+        from holomap_b200.shard import row_bounds
+        self.wl, self.dev, self.world, self.rank = wl, dev, world, rank
+        p = hm.KnnPath.parse(path)
+        self.path = hm.autotune_path(wl.n, wl.d, wl.k, wl.metric) if p == hm.KnnPath.AUTO else p
+        self.plain = self.path == hm.KnnPath.PLAIN
+        self.m = int(_lib.Metric.parse(wl.metric))
+        self.bounds = row_bounds(wl.n, world)
+        self.b0, self.b1 = self.bounds[rank]
+        self.most = max(e - b for b, e in self.bounds)
+        n, d, k = wl.n, wl.d, wl.k
+        L = _lib.lib()
+        self.L = L
+        self.ws_bytes = L.hm_knn_rows_workspace_bytes(n, d, k, self.m, int(self.path), self.b0, self.b1)
+        if self.ws_bytes == 0:
+            _lib.check(-1)
+        self.ws = torch.empty(self.ws_bytes + 256, dtype=torch.uint8, device=dev)
+        self.ws_ptr = (self.ws.data_ptr() + 255) // 256 * 256
+        self.sm_ws = torch.empty(L.hm_smooth_workspace_bytes(n) + 256, dtype=torch.uint8, device=dev)
+        self.sm_ptr = (self.sm_ws.data_ptr() + 255) // 256 * 256
+        self.x_dev = torch.from_numpy(wl.data).to(dev)
+        f32, i32 = torch.float32, torch.int32
+        self.idx_sh = torch.zeros((self.most, k), dtype=i32, device=dev)
+        self.dist_sh = torch.zeros((self.most, k), dtype=f32, device=dev)
+        self.sig_sh = torch.zeros(self.most, dtype=f32, device=dev)
+        self.rho_sh = torch.zeros(self.most, dtype=f32, device=dev)
+        self.idx_pad = torch.empty((world * self.most, k), dtype=i32, device=dev)
+        self.dist_pad = torch.empty((world * self.most, k), dtype=f32, device=dev)
+        self.sig_pad = torch.empty(world * self.most, dtype=f32, device=dev)
+        self.rho_pad = torch.empty(world * self.most, dtype=f32, device=dev)
+        self.dist_all = torch.empty((n, k), dtype=f32, device=dev)
+        self.graphs_per_step = 1.0 / world  # main() multiplies by the world size
+        self.ctypes = ctypes
+
+    def step(self, stream, graph=False):
+        import torch
+        import torch.distributed as dist
+
+        from holomap_b200 import _lib
+        wl = self.wl
+        with torch.cuda.stream(stream):
+            if self.b1 > self.b0:
+                _lib.check(self.L.hm_knn_rows_device(
+                    self.x_dev.data_ptr(), wl.n, wl.d, wl.k, self.m, int(self.path), self.b0, self.b1,
+                    self.idx_sh.data_ptr(), self.dist_sh.data_ptr(), self.ws_ptr, self.ws_bytes,
+                    stream.cuda_stream, None))
+            dist.all_gather_into_tensor(self.idx_pad, self.idx_sh)
+            dist.all_gather_into_tensor(self.dist_pad, self.dist_sh)
+            for r, (b, e) in enumerate(self.bounds):
+                if e > b:
+                    self.dist_all[b:e].copy_(self.dist_pad[r * self.most: r * self.most + e - b])
+            if self.b1 > self.b0:
+                _lib.check(self.L.hm_smooth_knn_rows_device(
+                    self.dist_all.data_ptr(), wl.n, wl.k, self.b0, self.b1, self.sig_sh.data_ptr(),
+                    self.rho_sh.data_ptr(), self.sm_ptr, stream.cuda_stream))
+            dist.all_gather_into_tensor(self.sig_pad, self.sig_sh)
+            dist.all_gather_into_tensor(self.rho_pad, self.rho_sh)
+
+    def assembled(self):
+        """(indices, dists, sigmas, rhos) of all n rows as numpy arrays."""
+        def cat(t):
+            return np.concatenate([t[r * self.most: r * self.most + e - b].cpu().numpy()
+                                   for r, (b, e) in enumerate(self.bounds) if e > b])
+        return (cat(self.idx_pad).view(np.uint32), cat(self.dist_pad), cat(self.sig_pad),
+                cat(self.rho_pad))
+
+    def single_gpu_matches(self) -> bool:
+        """Rank 0: the assembled bytes equal a single-GPU run of the whole
+        dataset (hm_knn_smooth_device on this device)."""
+        import torch
+
+        from holomap_b200.device import DeviceKnnProblem
+        wl = self.wl
+        p = DeviceKnnProblem(wl.n, wl.d, wl.k, wl.metric, self.path, device=self.dev)
+        p.run(self.x_dev)
+        torch.cuda.synchronize(self.dev)
+        one = (p.idx.cpu().numpy().view(np.uint32), p.dist.cpu().numpy(), p.sigma.cpu().numpy(),
+               p.rho.cpu().numpy())
+        got = self.assembled()
+        return all(np.array_equal(a.reshape(-1).view(np.uint32), b.reshape(-1).view(np.uint32))
+                   for a, b in zip(got, one))
+
+    def e2e_prepare(self):
+        import torch
+        self.pin_x = torch.from_numpy(self.wl.data).pin_memory()
+        self.pin_out = [torch.empty_like(t, device="cpu").pin_memory()
+                        for t in (self.idx_pad, self.dist_pad, self.sig_pad, self.rho_pad)]
+
+    def e2e_step(self):
+        """Host points in on every rank, the sharded step, the whole result
+        back to the host on every rank."""
+        import torch
+        s = torch.cuda.current_stream(self.dev)
+        self.x_dev.copy_(self.pin_x, non_blocking=True)
+        self.step(s)
+        for h, t in zip(self.pin_out, (self.idx_pad, self.dist_pad, self.sig_pad, self.rho_pad)):
+            h.copy_(t, non_blocking=True)
+        s.synchronize()
+
+    def e2e_matches(self) -> bool:
+        return bool(torch_equal(self.pin_out[0], self.idx_pad) and torch_equal(self.pin_out[2], self.sig_pad))
+
+    def io_bytes(self):
+        wl = self.wl
+        # per rank: the points in, the whole (padded) result out
+        return (int(wl.n * wl.d * 4 * self.world),
+                int(self.world * self.world * self.most * (wl.k * 8 + 8)))
+
+    def stats(self) -> dict:
+        from holomap_b200 import _lib
+        st = _lib.HmStats()
+        wl = self.wl
+        rc = self.L.hm_knn_rows_stats(self.ws_ptr, wl.n, wl.d, wl.k, self.m, int(self.path), self.b0, self.b1,
+                                      self.ctypes.byref(st))
+        _lib.check(rc)
+        rows = max(self.b1 - self.b0, 1)
+        return {"rank_rows": [self.b0, self.b1], "path_used": int(st.path_used),
+                "candidates_per_row": st.candidates_total / rows,
+                "emitted_per_row": st.candidates_emitted / rows, "overflow_rows": int(st.overflow_rows)}
+
+    def config(self):
+        c = config_of(self.wl)
+        c["parallelism"] = f"rows{self.world}"
+        c["shards"] = [list(b) for b in self.bounds]
+        return c
+
+    def screened_work(self):
+        wl = self.wl
+        # the screen of this rank's shard: 2 x rows x n x d flops, written as
+        # the (n, d) of a square problem of the same flops for roofline()
+        rows = self.b1 - self.b0
+        eq = (rows * wl.n) ** 0.5
+        return (([] if self.plain else [(eq, wl.d)]), ([(eq, wl.d, wl.metric)] if self.plain else []))
+
+
 class BatchRunner:
     """All datasets of a batch in one pass of the pipeline, replayed as one
     captured CUDA graph per step (hm_batch_graph_launch)."""
@@ -734,6 +886,8 @@ def main():
     if args.workload == "batch_256":
         from holomap_b200.synth import batch_256
         runner = BatchRunner(batch_256(), dev)
+    elif world > 1:
+        runner = ShardedRunner(workload(args.workload, args.rows), args.path, dev, world, rank)
     else:
         runner = SingleRunner(workload(args.workload, args.rows), args.path, dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
@@ -806,7 +960,7 @@ def main():
     same = runner.e2e_matches()
     e2e_sync = e2e_value
     pipelined, p_value = False, None
-    if hasattr(runner, "e2e_pipelined"):
+    if hasattr(runner, "e2e_pipelined") and world == 1:
         # the public asynchronous API with two requests in flight
         barrier()
         p_s, p_same = (runner.e2e_pipelined(e2e_steps, args.e2e_window) if hasattr(runner, "wl")
@@ -820,12 +974,14 @@ def main():
         pipelined = p_value >= e2e_sync  # report the faster public-API method
         e2e_value = max(p_value, e2e_sync)
 
+    sharded_same = runner.single_gpu_matches() if (rank == 0 and isinstance(runner, ShardedRunner)) else None
     if rank == 0:
         h2d, d2h = runner.io_bytes()
         line = {
             "metric": METRIC_NAME, "value": value, "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "higher_is_better": True,
+            "scaling": "strong" if isinstance(runner, ShardedRunner) else "weak", "vs_baseline": None,
             "dtype": "f64" if runner.plain else "bf16+f64",
             "data": "synthetic", "config": runner.config(),
             "path": str(getattr(runner, "path", "auto")).split(".")[-1].lower(),
@@ -845,7 +1001,9 @@ def main():
                         "max": max(step_ms)},
             "stats": stats,
         }
-        if hasattr(runner, "wl") and not runner.plain:
+        if sharded_same is not None:
+            line["shards_equal_single_gpu"] = sharded_same
+        if isinstance(runner, SingleRunner) and not runner.plain:
             line["screen_error"] = screen_error(runner.wl, runner.path)
             p = plain_arm(runner.wl, dev, flush, max(2, min(args.steps, 3)), fp64_rate)
             p["screened_over_plain"] = value / p["value"]

@@ -188,6 +188,7 @@ SIGNATURES = {
     "hm_stats_from_workspace": (_i32, [_vp, _u64, _u32, _u32, _i32, _i32, _vp]),
     "hm_smooth_workspace_bytes": (_sz, [_u64]),
     "hm_smooth_knn_device": (_i32, [_vp, _u64, _u32, _vp, _vp, _vp, _vp]),
+    "hm_smooth_knn_rows_device": (_i32, [_vp, _u64, _u32, _u64, _u64, _vp, _vp, _vp, _vp]),
     "hm_fuzzy_workspace_bytes": (_sz, [_u64, _u32]),
     "hm_fuzzy_graph_device": (_i32, [_vp, _vp, _vp, _vp, _u64, _u32, _vp, _vp, _vp, _vp, _vp, _sz,
                                      _vp]),

@@ -927,6 +927,42 @@ int hm_smooth_knn_device(const float *d_dists, uint64_t n, uint32_t k, float *d_
     return HM_OK;
 }
 
+// smooth-kNN of rows [row_begin, row_end) of an n x k distance matrix: the
+// job's rows are addressed from row_begin (arow0 = -row_begin in the kernels'
+// unsigned arithmetic) and its outputs through pointers shifted by the same
+// amount, while the global-mean floor still averages all n * k distances.
+int hm_smooth_knn_rows_device(const float *d_dists, uint64_t n, uint32_t k, uint64_t row_begin,
+                              uint64_t row_end, float *d_sigma, float *d_rho, void *d_workspace,
+                              void *stream) {
+    clear_error();
+    if (!d_dists || !d_sigma || !d_rho || !d_workspace)
+        return set_error(HM_ERR_INVALID, "NULL pointer argument");
+    if (n == 0 || k == 0) return set_error(HM_ERR_INVALID, "empty distance matrix");
+    if (n > 0x7fffffffull) return set_error(HM_ERR_UNSUPPORTED, "n exceeds the supported range");
+    if (row_begin >= row_end || row_end > n)
+        return set_error(HM_ERR_INVALID, "rows [%llu, %llu) outside [0, %llu)", (unsigned long long)row_begin,
+                         (unsigned long long)row_end, (unsigned long long)n);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    char *w = static_cast<char *>(d_workspace);
+    JobDev J{};
+    J.n = (uint32_t)n;
+    J.k = k;
+    J.arow0 = (uint32_t)(0u - (uint32_t)row_begin);
+    J.dist = const_cast<float *>(d_dists);
+    J.sigma = d_sigma - row_begin;
+    J.rho = d_rho - row_begin;
+    J.target = std::log2((double)k);  // src/smooth_knn.rs:25 (platform log2)
+    J.cnt = reinterpret_cast<JobCounters *>(w + align256(sizeof(JobDev)));
+    J.zero_rows = reinterpret_cast<uint32_t *>(w + align256(sizeof(JobDev)) + align256(sizeof(JobCounters)));
+    JobDev *jd = reinterpret_cast<JobDev *>(w);
+    write_smooth_job_kernel<<<1, 32, 0, s>>>(jd, J);
+    HM_CUDA_TRY(cudaGetLastError());
+    count_launch();
+    HM_TRY(launch_smooth(jd, 1, nullptr, (uint32_t)(row_end - row_begin), k, s));
+    HM_TRY(launch_mean_all_floor(jd, 1, s));
+    return HM_OK;
+}
+
 int hm_smooth_knn(const float *dists, uint64_t n, uint32_t k, float *sigma_out, float *rho_out) {
     clear_error();
     if (!dists || !sigma_out || !rho_out) return set_error(HM_ERR_INVALID, "NULL pointer argument");

@@ -149,6 +149,14 @@ HM_API int hm_knn_rows_stats(const void *d_workspace, uint64_t n, uint32_t d, ui
 HM_API size_t hm_smooth_workspace_bytes(uint64_t n);
 HM_API int hm_smooth_knn_device(const float *d_dists, uint64_t n, uint32_t k, float *d_sigma,
                          float *d_rho, void *d_workspace, void *stream);
+/* smooth-kNN of the rows [row_begin, row_end) of an n x k distance matrix,
+ * for a row shard: d_sigma / d_rho receive (row_end - row_begin) values, the
+ * same bits as rows [row_begin, row_end) of hm_smooth_knn_device over all n
+ * rows (a rho == 0 row's floor is the mean of all n * k distances,
+ * src/smooth_knn.rs:26, :70-74).  d_workspace: hm_smooth_workspace_bytes(n). */
+HM_API int hm_smooth_knn_rows_device(const float *d_dists, uint64_t n, uint32_t k, uint64_t row_begin,
+                                     uint64_t row_end, float *d_sigma, float *d_rho, void *d_workspace,
+                                     void *stream);
 
 /* The fuzzy simplicial set (replaces fuzzy_simplicial_set, src/fuzzy.rs:25-91):
  * the kNN graph (n x k indices and distances, each row's indices distinct, as

@@ -46,3 +46,34 @@ def test_local_shards_reassemble_the_single_call(world, path):
     assert_same_bytes(dist.cpu().numpy().reshape(-1), whole.dists, "dists")
     assert_same_bytes(sig.cpu().numpy(), sm.sigmas, "sigma")
     assert_same_bytes(rho.cpu().numpy(), sm.rhos, "rho")
+
+
+@pytest.mark.parametrize("k", [15, 40])
+def test_smooth_rows_equal_rows_of_the_whole_calibration(oracle, k):
+    """hm_smooth_knn_rows_device on a row range of the whole distance matrix
+    returns those rows of the whole calibration, including rows whose rho is 0
+    (their floor is the mean of all n * k distances, src/smooth_knn.rs:26)."""
+    import ctypes
+    import torch
+    g = np.random.default_rng(k)
+    n = 3000
+    d = np.sort(g.exponential(size=(n, k)).astype(np.float32), axis=1)
+    d[:, 0] = 0.0
+    d[::13] = 0.0  # rows with no positive distance: the global-mean floor
+    osig, orho = oracle.smooth_knn(d, k)
+    lib = hm.lib()
+    dt = torch.from_numpy(d).cuda()
+    ws = torch.empty(lib.hm_smooth_workspace_bytes(n) + 256, dtype=torch.uint8, device="cuda")
+    wp = (ws.data_ptr() + 255) // 256 * 256
+    stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for b, e in [(0, n), (0, 1), (1, 14), (1024, 2048), (2999, 3000), (13, 2987)]:
+        sig = torch.empty(e - b, dtype=torch.float32, device="cuda")
+        rho = torch.empty(e - b, dtype=torch.float32, device="cuda")
+        assert lib.hm_smooth_knn_rows_device(dt.data_ptr(), n, k, b, e, sig.data_ptr(), rho.data_ptr(),
+                                             wp, stream) == hm.HM_OK, lib.hm_last_error()
+        torch.cuda.synchronize()
+        assert_same_bytes(sig.cpu().numpy(), osig[b:e], f"rows [{b},{e}) sigma")
+        assert_same_bytes(rho.cpu().numpy(), orho[b:e], f"rows [{b},{e}) rho")
+    for b, e in [(5, 5), (10, 3), (0, n + 1)]:
+        assert lib.hm_smooth_knn_rows_device(dt.data_ptr(), n, k, b, e, sig.data_ptr(), rho.data_ptr(),
+                                             wp, stream) == hm.HM_ERR_INVALID
