@@ -97,6 +97,11 @@ struct JobPlan {
     uint32_t row0 = 0, unit0 = 0, kp1 = 0, k_stages = 0, row_blocks = 0, col_tiles = 0;
     uint32_t parts = 1, part_tiles = 0, cap = 0, seed_tiles = 0;
     uint64_t slot0 = 0, cand0 = 0, topk0 = 0;
+    // emission pass: symmetric (tiles on and above the diagonal), its column
+    // parts per row block of ept tiles, candidate lists per row
+    bool sym = false;
+    uint32_t ept = 0, elists = 0;
+    uint64_t eslot0 = 0;
 };
 
 struct GroupPlan {
@@ -106,11 +111,15 @@ struct GroupPlan {
     uint32_t kp = 32, kpl = 1, dmax = 0;
     int metric_mask = 0;
     std::vector<uint32_t> jobs;
-    uint64_t lists = 0, cand = 0, topk = 0;
+    uint64_t lists = 0, cand = 0, topk = 0, elists = 0;
+    std::vector<uint4> eunits;  // emission units, largest first
+    bool any_sym = false;
+    uint32_t egrid = 0, stage_cap = 0;
     size_t off_opa = 0, off_opb = 0, off_rowstat = 0, off_rowterm = 0, off_colterm = 0;
     size_t off_band = 0, off_force = 0, off_rowthr = 0, off_cand = 0, off_cnt = 0, off_topk = 0;
+    size_t off_ethr = 0, off_evstar = 0, off_stage_row = 0, off_stage_key = 0, off_stage_cnt = 0;
     // tables
-    size_t off_gdev = 0, off_job_ids = 0, off_row_starts = 0, off_unit_starts = 0;
+    size_t off_gdev = 0, off_job_ids = 0, off_row_starts = 0, off_unit_starts = 0, off_eunits = 0;
     GroupDev host{};
     CUtensorMap ta{}, tb{};
 };
@@ -126,6 +135,7 @@ struct hm_batch {
     uint32_t fb_per_job[3] = {1, 1, 1};
     std::vector<uint32_t> job_blocks;  // prep block offsets
     bool any_plain = false, any_screen = false, any_smooth = false, any_split = false;
+    bool sym_enabled = true;  // symmetric emission for whole datasets
     size_t off_tables = 0, off_jobs = 0, off_counters = 0, off_row_starts = 0, off_job_blocks = 0;
     size_t off_items[3] = {}, off_fb[3] = {};
     size_t tables_bytes = 0, tables_used = 0, total = 0;
@@ -158,6 +168,7 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
     if (njobs > (1u << 16)) return set_error(HM_ERR_UNSUPPORTED, "more than 65536 jobs");
     const uint32_t G = (uint32_t)sm_count();
     B.jobs.assign(njobs, JobPlan{});
+    B.sym_enabled = tuning_symmetric();
     for (int g = 0; g < 3; ++g) B.groups[g] = GroupPlan{};
     B.groups[0].kind = SCREEN_KIND_BF16;
     B.groups[1].kind = SCREEN_KIND_TF32;
@@ -284,10 +295,58 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
             P.slot0 = Gp.lists;
             const uint64_t lists = P.spec.n * 2ull * P.parts;
             Gp.lists += lists;
-            P.cand0 = Gp.cand;
-            Gp.cand += lists * P.cap;
             P.topk0 = Gp.topk;
             Gp.topk += lists * P.spec.k;
+            // Emission pass.  A whole dataset (not a row shard) with at least
+            // two column tiles takes the symmetric form: row block rb walks
+            // the column tiles from the one holding its own diagonal block
+            // (rb / 2) to the end, in parts of ept tiles; the rows of the
+            // blocks above the diagonal get their candidates as columns.  Its
+            // candidate lists per row: two per part, then the column list,
+            // which takes two lists' room.
+            P.sym = B.sym_enabled && P.q0 == 0 && P.q1 == P.spec.n && P.col_tiles >= 2;
+            if (P.sym) {
+                uint64_t tiles = 0;
+                for (uint32_t rb = 0; rb < P.row_blocks; ++rb) tiles += P.col_tiles - rb / 2;
+                P.ept = (uint32_t)std::max<uint64_t>(4, (tiles + 4ull * G - 1) / (4ull * G));
+                const uint32_t eparts = (P.col_tiles + P.ept - 1) / P.ept;
+                P.elists = 2 * eparts + 2;
+                Gp.any_sym = true;
+            } else {
+                P.ept = P.part_tiles;
+                P.elists = 2 * P.parts;
+            }
+            P.eslot0 = Gp.elists;
+            Gp.elists += P.spec.n * (uint64_t)P.elists;
+            P.cand0 = Gp.cand;
+            Gp.cand += P.spec.n * (uint64_t)P.elists * P.cap;
+        }
+        // emission units of the group: (job slot | sym, row block, first tile,
+        // end tile | part), the largest first so the persistent CTAs' static
+        // round-robin finishes together
+        for (uint32_t gj = 0; gj < Gp.jobs.size(); ++gj) {
+            const JobPlan &P = B.jobs[Gp.jobs[gj]];
+            for (uint32_t r = 0; r < P.row_blocks; ++r) {
+                const uint32_t rb = P.rb0 + r;
+                const uint32_t first = P.sym ? rb / 2 : 0u;
+                for (uint32_t part = 0, t0 = first; t0 < P.col_tiles; ++part, t0 += P.ept) {
+                    const uint32_t t1 = std::min<uint32_t>(P.col_tiles, t0 + P.ept);
+                    Gp.eunits.push_back(make_uint4(gj | (P.sym ? 0x80000000u : 0u), rb, t0, t1 | (part << 24)));
+                }
+            }
+        }
+        std::stable_sort(Gp.eunits.begin(), Gp.eunits.end(), [](const uint4 &a, const uint4 &b) {
+            return (a.w & 0xffffffu) - a.z > (b.w & 0xffffffu) - b.z;
+        });
+        Gp.egrid = std::min<uint32_t>((uint32_t)Gp.eunits.size(), G);
+        if (Gp.any_sym) {
+            // column-side candidates staged per CTA: room for half of every
+            // sym row's expected list share (a full stage sends the affected
+            // rows to the exact path, it never loses a candidate silently)
+            uint64_t want = 0;
+            for (uint32_t j : Gp.jobs)
+                if (B.jobs[j].sym) want += B.jobs[j].spec.n * (uint64_t)B.jobs[j].cap / 2;
+            Gp.stage_cap = (uint32_t)std::min<uint64_t>(0x7fffffffull, (want + Gp.egrid - 1) / Gp.egrid + 4096);
         }
     }
 
@@ -347,6 +406,7 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
         Gp.off_job_ids = pack(sizeof(uint32_t) * Gp.jobs.size());
         Gp.off_row_starts = pack(sizeof(uint32_t) * (Gp.jobs.size() + 1));
         Gp.off_unit_starts = pack(sizeof(uint32_t) * (Gp.jobs.size() + 1));
+        Gp.off_eunits = pack(sizeof(uint4) * Gp.eunits.size());
     }
     B.tables_used = off - B.off_tables;
     off = align256(off);
@@ -379,8 +439,16 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
         Gp.off_force = take(rows);
         Gp.off_rowthr = take(rows * sizeof(uint32_t));
         Gp.off_cand = take(Gp.cand * sizeof(unsigned long long));
-        Gp.off_cnt = take(Gp.lists * sizeof(uint32_t));
+        Gp.off_cnt = take(Gp.elists * sizeof(uint32_t));
         Gp.off_topk = take(Gp.topk * sizeof(float));
+        if (Gp.any_sym) {
+            const size_t padded = round_up(rows, SC_BN) + SC_BN;
+            Gp.off_ethr = take(padded * sizeof(float));
+            Gp.off_evstar = take(padded * sizeof(float));
+            Gp.off_stage_row = take((size_t)Gp.egrid * Gp.stage_cap * sizeof(uint32_t));
+            Gp.off_stage_key = take((size_t)Gp.egrid * Gp.stage_cap * sizeof(unsigned long long));
+            Gp.off_stage_cnt = take((size_t)Gp.egrid * sizeof(uint32_t));
+        }
     }
     B.total = off;
     return HM_OK;
@@ -465,6 +533,9 @@ static int bind_batch(hm_batch &B, void *d_ws, size_t bytes, cudaStream_t s) {
         J.slot0 = P.slot0;
         J.cand0 = P.cand0;
         J.topk0 = P.topk0;
+        J.elists = P.elists;
+        J.sym = P.sym ? 1u : 0u;
+        J.eslot0 = P.eslot0;
         J.scale = s.metric == HM_METRIC_EUCLIDEAN ? 2.0f : 1.0f;
         J.mu = P.group >= 0 ? at<double>(ws, P.off_mu) : nullptr;
         J.csum = P.group >= 0 ? at<double>(ws, P.off_csum) : nullptr;
@@ -496,6 +567,8 @@ static int bind_batch(hm_batch &B, void *d_ws, size_t bytes, cudaStream_t s) {
         memcpy(host + Gp.off_job_ids, Gp.jobs.data(), sizeof(uint32_t) * gj);
         memcpy(host + Gp.off_row_starts, rs.data(), sizeof(uint32_t) * (gj + 1));
         memcpy(host + Gp.off_unit_starts, us.data(), sizeof(uint32_t) * (gj + 1));
+        if (!Gp.eunits.empty())
+            memcpy(host + Gp.off_eunits, Gp.eunits.data(), sizeof(uint4) * Gp.eunits.size());
         GroupDev D{};
         D.rows = Gp.rows;
         D.njobs = gj;
@@ -519,6 +592,16 @@ static int bind_batch(hm_batch &B, void *d_ws, size_t bytes, cudaStream_t s) {
         D.cand = at<unsigned long long>(ws, Gp.off_cand);
         D.cand_cnt = at<uint32_t>(ws, Gp.off_cnt);
         D.topk = at<float>(ws, Gp.off_topk);
+        D.eunits = at<uint4>(ws, Gp.off_eunits);
+        D.neunits = (uint32_t)Gp.eunits.size();
+        if (Gp.any_sym) {
+            D.ethr = at<float>(ws, Gp.off_ethr);
+            D.evstar = at<float>(ws, Gp.off_evstar);
+            D.stage_row = at<uint32_t>(ws, Gp.off_stage_row);
+            D.stage_key = at<unsigned long long>(ws, Gp.off_stage_key);
+            D.stage_cnt = at<uint32_t>(ws, Gp.off_stage_cnt);
+            D.stage_cap = Gp.stage_cap;
+        }
         Gp.host = D;
         memcpy(host + Gp.off_gdev, &D, sizeof D);
         HM_TRY(make_operand_map(&Gp.ta, D.opa, Gp.rows, Gp.kpmax, Gp.elem_bytes, Gp.kslice, SC_BM));
@@ -570,7 +653,12 @@ static int run_batch(hm_batch &B, cudaStream_t s) {
         HM_TRY(launch_screen_band(jobs, Gp.host, Gd, s));
         HM_TRY(launch_screen_gemm(jobs, Gp.host, Gd, Gp.kp, Gp.ta, Gp.tb, debug_dump_pointer(), 0, s));
         HM_TRY(launch_screen_threshold(jobs, Gp.host, Gd, Gp.kpl, s));
+        // lists no unit writes (parts a row block does not have) and the
+        // column lists the scatter fills start empty
+        HM_CUDA_TRY(cudaMemsetAsync(Gp.host.cand_cnt, 0, Gp.elists * sizeof(uint32_t), s));
+        if (Gp.any_sym) HM_TRY(launch_emit_limits(jobs, Gp.host, Gd, s));
         HM_TRY(launch_screen_gemm(jobs, Gp.host, Gd, Gp.kp, Gp.ta, Gp.tb, nullptr, 1, s));
+        if (Gp.any_sym) HM_TRY(launch_column_scatter(jobs, Gp.host, Gd, Gp.egrid, s));
         HM_TRY(launch_rerank(jobs, Gp.host, Gd, Gp.kpl, Gp.dmax, Gp.metric_mask, s));
     }
     if (B.any_screen) {

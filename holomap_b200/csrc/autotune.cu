@@ -19,6 +19,9 @@
 namespace hm {
 
 static thread_local uint32_t g_seed_override = 0;
+static thread_local bool g_symmetric = true;
+
+bool tuning_symmetric() { return g_symmetric; }
 
 template <size_t N>
 static size_t nearest_ratio(const uint32_t (&grid)[N], double v) {
@@ -64,6 +67,11 @@ int hm_autotune_path(uint64_t n, uint32_t d, uint32_t k, int metric) {
 int hm_tuning_override(int seed_div) {
     if (seed_div < 0 || seed_div > 64) return set_error(HM_ERR_INVALID, "seed_div %d outside [0, 64]", seed_div);
     g_seed_override = (uint32_t)seed_div;
+    return HM_OK;
+}
+
+int hm_tuning_symmetric(int on) {
+    g_symmetric = on != 0;
     return HM_OK;
 }
 

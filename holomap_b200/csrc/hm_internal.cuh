@@ -184,9 +184,13 @@ struct JobDev {
     // screened path
     uint32_t group, row0, unit0, kp1, k_stages, row_blocks, col_tiles, parts, part_tiles, cap;
     uint32_t seed_tiles;         // leading column tiles of each part in the threshold pass
-    unsigned long long slot0;    // first candidate list (2 * parts lists per row)
-    unsigned long long cand0;    // first candidate slot: list l holds [cand0 + (l - slot0) * cap, +cap)
+    unsigned long long slot0;    // first threshold-pass list (2 * parts lists per row)
     unsigned long long topk0;    // first k-array entry: list l's is [topk0 + (l - slot0) * k, +k)
+    // candidate lists of the emission pass: elists per row (two per column
+    // part; with the symmetric emission one more, the row's column list, last)
+    uint32_t elists, sym;        // sym: the emission pass covers the tiles on and above the diagonal
+    unsigned long long eslot0;   // first candidate list of the job
+    unsigned long long cand0;    // first candidate slot: list l holds [cand0 + (l - eslot0) * cap, +cap)
     float scale;                 // 1 (cosine) or 2 (euclidean)
     double *mu, *csum;           // euclidean column mean and its partial sums
     uint32_t csum_blocks, csum_rows;
@@ -210,6 +214,9 @@ int kpl_for_k(uint32_t k);  // 1, 2, 4, 8 or 0 if k > 256
 // The autotuner table's path for a problem and (seed_div) the fraction
 // 1/seed_div of the columns the screen's threshold pass samples.
 int autotune_choice(uint64_t n, uint32_t d, uint32_t k, int metric, uint32_t *seed_div);
+// whether screened plans made on this thread may use the symmetric emission
+// pass (hm_tuning_symmetric; on by default)
+bool tuning_symmetric();
 
 // ------------------------------------------------------------- plain path
 constexpr int PL_BM = 32;     // rows per CTA (8 warps x 4 rows)

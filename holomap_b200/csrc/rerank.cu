@@ -138,9 +138,15 @@ __device__ __forceinline__ void cp_async_wait() {
 }
 
 // The survivors of one row live at the front of its list region (the row's
-// 2 * parts lists are contiguous).
+// elists candidate lists are contiguous).
 __device__ __forceinline__ unsigned long long *row_region(const JobDev &J, const GroupDev &G, uint32_t row) {
-    return G.cand + J.cand0 + (list_index(J, row, 0) - J.slot0) * J.cap;
+    return cand_slots(J, G, cand_list(J, row, 0));
+}
+
+// Capacity of a row's candidate list s: the symmetric emission's column list
+// (s = elists - 2) takes the room of two lists.
+__device__ __forceinline__ uint32_t list_cap(const JobDev &J, uint32_t s) {
+    return (J.sym && s == J.elists - 2) ? 2 * J.cap : J.cap;
 }
 
 // Phase 1 for one row: returns the survivor count (0 for rows sent to the
@@ -148,14 +154,14 @@ __device__ __forceinline__ unsigned long long *row_region(const JobDev &J, const
 template <int KPL>
 __device__ __forceinline__ uint32_t select_row(const JobDev &J, const GroupDev &G, uint32_t gr, uint32_t row,
                                                RrWarpSmem &sm, int lane) {
-    const uint32_t k = J.k, lists = 2 * J.parts;
-    const size_t l0 = list_index(J, row, 0);
+    const uint32_t k = J.k, lists = J.elists;
+    const size_t l0 = cand_list(J, row, 0);
     // overflow / unbounded rows go to the exact plain path
     bool ovf = G.force[gr] != 0;
     uint32_t total = 0;
     for (uint32_t p = lane; p < lists; p += 32) {
         const uint32_t c = G.cand_cnt[l0 + p];
-        ovf |= c > J.cap;
+        ovf |= c > list_cap(J, p);
         total += c;
     }
     ovf = __any_sync(0xffffffffu, ovf);
@@ -408,6 +414,75 @@ __global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const JobDev *__r
         atomicAdd(&J.cnt->candidates, (unsigned long long)kept);
         atomicMax(&J.cnt->max_row, kept_max);
     }
+}
+
+// Symmetric emission: each row's emission limit tau1 + 2 band (rounded up)
+// and its raw-product form v* for cosine rows, for the column-side tests of
+// the tiles above the diagonal; rows that take no column-side candidates
+// (padding, zero vectors under cosine, jobs without the symmetric form) get
+// limits nothing passes.
+__global__ void __launch_bounds__(256) emit_limits_kernel(const JobDev *__restrict__ jobs,
+                                                         const GroupDev *__restrict__ Gp, uint32_t padded) {
+    const GroupDev &G = *Gp;
+    const uint32_t gr = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gr >= padded) return;
+    const float INF = __int_as_float(0x7f800000);
+    float lim = -INF, vs = INF;
+    if (gr < G.rows) {
+        const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
+        const uint32_t row = gr - J.row0;
+        if (J.sym && row < J.n && !G.force[gr]) {
+            const float b = G.band[gr];
+            lim = __fadd_ru(__fadd_ru(unord32(G.rowthr[gr]), b), b);
+            vs = !(lim < INF) ? -INF : __fsub_rd(__fsub_rd(1.0f, lim), fmaxf(fabsf(lim), 1.0f) * 0x1p-20f);
+        }
+    }
+    G.ethr[gr] = lim;
+    G.evstar[gr] = vs;
+}
+
+int launch_emit_limits(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, cudaStream_t s) {
+    ScopedKernelTimer timer(HM_KCLASS_SELECT, s);
+    const uint32_t padded = (uint32_t)(round_up(G.rows, SC_BN) + SC_BN);
+    emit_limits_kernel<<<(padded + 255) / 256, 256, 0, s>>>(jobs, Gd, padded);
+    HM_CUDA_TRY(cudaGetLastError());
+    count_launch();
+    return HM_OK;
+}
+
+// Symmetric emission: the column-side candidates the emission pass staged
+// (per CTA: the column's group row, the raw product and the candidate row)
+// move into the rows' column lists with their exact screened values
+// c^_ji = rowterm_j + colterm_i - scale v, the arithmetic row j's own tiles
+// use.  blockIdx.y is the staging CTA.
+__global__ void __launch_bounds__(256) column_scatter_kernel(const JobDev *__restrict__ jobs,
+                                                            const GroupDev *__restrict__ Gp) {
+    const GroupDev &G = *Gp;
+    const uint32_t c = blockIdx.y;
+    const uint32_t cnt = min(G.stage_cnt[c], G.stage_cap);
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < cnt; e += gridDim.x * blockDim.x) {
+        const size_t at = (size_t)c * G.stage_cap + e;
+        const uint32_t gr = G.stage_row[at];
+        const unsigned long long key = G.stage_key[at];
+        const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
+        const uint32_t j = gr - J.row0, i = (uint32_t)key;
+        const float v = __uint_as_float((uint32_t)(key >> 32));
+        const float rt = J.metric == HM_METRIC_EUCLIDEAN ? G.colterm[gr] : 0.0f;
+        const float c2 = __fsub_rn(__fadd_rn(rt, G.colterm[J.row0 + i]), __fmul_rn(J.scale, v));
+        const size_t l = cand_list(J, j, J.elists - 2);
+        const uint32_t slot = atomicAdd(&G.cand_cnt[l], 1u);
+        if (slot < 2 * J.cap) cand_slots(J, G, l)[slot] = ((unsigned long long)__float_as_uint(c2) << 32) | i;
+    }
+}
+
+int launch_column_scatter(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t ctas,
+                          cudaStream_t s) {
+    if (ctas == 0) return HM_OK;
+    ScopedKernelTimer timer(HM_KCLASS_SELECT, s);
+    column_scatter_kernel<<<dim3(8, ctas), 256, 0, s>>>(jobs, Gd);
+    HM_CUDA_TRY(cudaGetLastError());
+    count_launch();
+    return HM_OK;
 }
 
 // tau1 of every row: the k-th smallest of the union of its lists' k smallest

@@ -72,6 +72,19 @@ struct GroupDev {
     unsigned long long *cand;     // candidate lists, (c^ bits << 32) | job-local column
     uint32_t *cand_cnt;
     float *topk;                  // each list's k smallest mini-chunk minima, ascending
+    // emission pass: its work units (x = group job slot | sym << 31, y = row
+    // block, z = first column tile, w = end column tile | column part << 24),
+    // largest first
+    const uint4 *eunits;
+    uint32_t neunits;
+    // symmetric emission: per group row (padded like colterm) the emission
+    // limit tau1 + 2 band and its cosine raw-product form; the column-side
+    // candidates each CTA staged (group row of the column, raw product bits
+    // << 32 | job-local row) and their counts
+    float *ethr, *evstar;
+    uint32_t *stage_row, *stage_cnt;
+    unsigned long long *stage_key;
+    uint32_t stage_cap;
 };
 
 // binary32 <-> unsigned key with the same order (for atomicMin)
@@ -83,9 +96,18 @@ __device__ __forceinline__ float unord32(uint32_t o) {
     return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
 }
 
-// Locations of row i's list s (s < 2 * parts) of job J.
+// Row i's threshold-pass list s (s < 2 * parts) of job J (its k-array).
 __device__ __forceinline__ size_t list_index(const JobDev &J, uint32_t i, uint32_t s) {
     return (size_t)J.slot0 + (size_t)i * 2 * J.parts + s;
+}
+
+// Row i's candidate list s (s < elists) of job J: its count is
+// G.cand_cnt[cand_list(J, i, s)], its slots follow cand_slots.
+__device__ __forceinline__ size_t cand_list(const JobDev &J, uint32_t i, uint32_t s) {
+    return (size_t)J.eslot0 + (size_t)i * J.elists + s;
+}
+__device__ __forceinline__ unsigned long long *cand_slots(const JobDev &J, const GroupDev &G, size_t list) {
+    return G.cand + J.cand0 + (list - J.eslot0) * J.cap;
 }
 
 int launch_screen_prep(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, cudaStream_t s);
@@ -97,5 +119,13 @@ int launch_screen_threshold(const JobDev *jobs, const GroupDev &G, const GroupDe
                             cudaStream_t s);
 int launch_rerank(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t kpl,
                   uint32_t dmax, int metric_mask, cudaStream_t s);
+// symmetric emission: the per-row limits before the emission pass, and the
+// column-side candidates moved from the CTAs' staging into the rows' column
+// lists after it (grid: the emission pass's CTAs)
+int launch_emit_limits(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, cudaStream_t s);
+int launch_column_scatter(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t ctas,
+                          cudaStream_t s);
+// the emission pass's grid (one CTA per SM, at most one per unit)
+uint32_t emission_grid(const GroupDev &G);
 
 }  // namespace hm

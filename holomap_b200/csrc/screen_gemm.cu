@@ -194,15 +194,27 @@ __device__ __forceinline__ void raise_error(volatile uint32_t *abort_flag, uint3
 }
 
 struct UnitTiles {
-    uint32_t job, rb, part, ct_begin, ct_end;
+    uint32_t job, rb, part, ct_begin, ct_end, sym;
 };
 
 // Pass 0 (the threshold pass) walks only the first seed_tiles tiles of each
 // part: a sample of the row's columns whose k-th smallest screened value
-// already bounds the row's k-th from above.
+// already bounds the row's k-th from above.  Pass 1 (the emission pass) takes
+// its units from the group's table.
 __device__ __forceinline__ UnitTiles unit_tiles(const JobDev *jobs, const GroupDev &G, uint32_t u, int pass) {
-    const uint32_t g = find_job(G.unit_starts, G.njobs, u);
     UnitTiles t;
+    if (pass == 1) {
+        const uint4 e = G.eunits[u];
+        t.job = G.job_ids[e.x & 0x7fffffffu];
+        t.sym = e.x >> 31;
+        t.rb = e.y;
+        t.ct_begin = e.z;
+        t.ct_end = e.w & 0xffffffu;
+        t.part = e.w >> 24;
+        return t;
+    }
+    const uint32_t g = find_job(G.unit_starts, G.njobs, u);
+    t.sym = 0;
     t.job = G.job_ids[g];
     const JobDev &J = jobs[t.job];
     const uint32_t lu = u - G.unit_starts[g];
@@ -234,8 +246,10 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
     uint64_t *aempty = afull + 1;           // resident A consumed by the unit's MMAs
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(aempty + 1);
     volatile uint32_t *abort_flag = tmem_slot + 1;
+    uint32_t *s_colcnt = tmem_slot + 2;  // column-side candidates this CTA staged
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t nunits = PASS == 1 ? G.neunits : G.units;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < SC_STAGES; ++s) {
@@ -249,6 +263,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         mbar_init(smem_u32(afull), 1);
         mbar_init(smem_u32(aempty), 1);
         *abort_flag = 0;
+        *s_colcnt = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
@@ -268,7 +283,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
             uint32_t it = 0, un = 0;
             bool ok = true;
             constexpr uint32_t kelems = SC_SLICE_BYTES / (KIND == SCREEN_KIND_BF16 ? 2 : 4);
-            for (uint32_t u = blockIdx.x; ok && u < G.units; u += gridDim.x) {
+            for (uint32_t u = blockIdx.x; ok && u < nunits; u += gridDim.x) {
                 const UnitTiles ut = unit_tiles(jobs, G, u, PASS);
                 const JobDev &J = jobs[ut.job];
                 if (a_res) {
@@ -324,7 +339,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         if (lane == 0) {
             uint32_t it = 0, tile = 0, un = 0;
             bool ok = true;
-            for (uint32_t u = blockIdx.x; ok && u < G.units; u += gridDim.x) {
+            for (uint32_t u = blockIdx.x; ok && u < nunits; u += gridDim.x) {
                 const UnitTiles ut = unit_tiles(jobs, G, u, PASS);
                 const JobDev &J = jobs[ut.job];
                 if (a_res) {
@@ -388,7 +403,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         const float INF = __int_as_float(0x7f800000);
         uint32_t tile = 0;
         bool ok = true;
-        for (uint32_t u = blockIdx.x; ok && u < G.units; u += gridDim.x) {
+        for (uint32_t u = blockIdx.x; ok && u < nunits; u += gridDim.x) {
             const UnitTiles ut = unit_tiles(jobs, G, u, PASS);
             const JobDev &J = jobs[ut.job];
             const uint32_t n = J.n;
@@ -401,7 +416,10 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
             const float band = valid ? G.band[gr] : 0.0f;
             const float rowterm = valid ? G.rowterm[gr] : 0.0f;
             const float scale = J.scale;
-            const size_t list = list_index(J, valid ? row : 0, ut.part * 2 + half);
+            // pass 0: the row's threshold-pass list (its k-array); pass 1: its
+            // candidate list for this column part and half
+            const size_t list = PASS == 0 ? list_index(J, valid ? row : 0, ut.part * 2 + half)
+                                          : cand_list(J, valid ? row : 0, ut.part * 2 + half);
             const float *colterm = G.colterm + J.row0;
             // pass 0: the k smallest mini-chunk minima seen (ascending;
             // arr[KP-1] is the list's k-th) and the row's shared k-th
@@ -411,30 +429,63 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
             float tglob = INF, published = INF;
             uint32_t tnext = 0xff800000u;  // ordered key of +inf
             const bool chunk_min = J.seed_tiles < J.part_tiles;
-            // pass 1: the row's fixed threshold tau1 + band
-            const float thr = (PASS == 1 && valid) ? __fadd_ru(unord32(G.rowthr[gr]), band) : -INF;
+            // pass 1: the row's fixed limit, tau1 + band (symmetric: tau1 +
+            // 2 band, precomputed; a pair's value may come from the tile of the
+            // other orientation, within 2E of the threshold pass's value)
+            float thr = -INF;
+            if (PASS == 1 && valid) thr = ut.sym ? G.ethr[gr] : __fadd_ru(unord32(G.rowthr[gr]), band);
             // cosine fast path of pass 1: every v with fl(1 - v) <= thr has
             // v >= 1 - thr - ulp(thr)/2 >= vstar (2^-20 relative margin)
             const float vstar = !(thr < INF) ? -INF
                                              : __fsub_rd(__fsub_rd(1.0f, thr), fmaxf(fabsf(thr), 1.0f) * 0x1p-20f);
             uint32_t cnt = 0;
-            unsigned long long *cand = G.cand + J.cand0 + (list - J.slot0) * J.cap;
+            unsigned long long *cand = PASS == 1 ? cand_slots(J, G, list) : nullptr;
+            // symmetric: this row's own term in its pairs' column-side values
+            // (c^_ji = rowterm_j + colterm_i - scale v) and the column-side
+            // candidates this thread staged in the unit
+            const float own_ct = (PASS == 1 && ut.sym && valid) ? G.colterm[gr] : 0.0f;
+            uint32_t colsum = 0;
 
             for (uint32_t ct = ut.ct_begin; ct < ut.ct_end; ++ct, ++tile) {
                 const uint32_t buf = tile & 1, use = tile >> 1;
-                if (!mbar_wait(smem_u32(&accf[buf]), use & 1, abort_flag)) {
+                // symmetric emission: this warp's 128 columns form block jb of
+                // the job; below the row block's diagonal its pairs belong to
+                // another unit's column side, above it they also serve the
+                // columns' rows
+                const uint32_t jb = 2 * ct + half;
+                const bool skip = PASS == 1 && ut.sym && jb < ut.rb;
+                const bool colside = PASS == 1 && ut.sym && jb > ut.rb && jb * (uint32_t)(SC_BN / 2) < n;
+                const uint32_t c_base = ct * SC_BN + half * (SC_BN / 2);
+                // the columns' limits (lane t holds column c_base + 32 q + t),
+                // loaded while the accumulator is still being filled
+                float cthr[4] = {-INF, -INF, -INF, -INF}, cvs[4] = {INF, INF, INF, INF}, cterm[4] = {0, 0, 0, 0};
+                if (colside) {
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        const size_t gc = (size_t)J.row0 + c_base + 32 * q + lane;
+                        cthr[q] = G.ethr[gc];
+                        cvs[q] = G.evstar[gc];
+                        cterm[q] = G.colterm[gc];
+                    }
+                }
+                const bool got = mbar_wait(smem_u32(&accf[buf]), use & 1, abort_flag);
+                if (!__all_sync(0xffffffffu, got)) {
                     raise_error(abort_flag, &J.cnt->error_code, SC_ERR_EPILOGUE);
                     ok = false;
                     break;
                 }
                 fence_after_sync();
+                if (skip) {
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(smem_u32(&acce[buf]));
+                    continue;
+                }
                 if (PASS == 0 && valid) {
                     // the row's other lists may have tightened its k-th: use the
                     // value loaded during the previous tile, load the next one
                     tglob = fminf(tglob, unord32(tnext));
                     tnext = *(volatile const uint32_t *)(G.rowthr + gr);
                 }
-                const uint32_t c_base = ct * SC_BN + half * (SC_BN / 2);
                 const bool diag = (ct * SC_BN < ut.rb * SC_BM + SC_BM) && (ut.rb * SC_BM < ct * SC_BN + SC_BN);
                 const uint32_t t_base = tmem_base + ((quad * 32) << 16) + buf * SC_BN + half * (SC_BN / 2);
                 // one chunk = 32 columns; the accumulator registers are
@@ -473,6 +524,77 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                                 if (j0 + t == row) c[t] = 0.0f;
                         }
                     };
+                    // symmetric emission, column side, on the raw products:
+                    // column j of the chunk takes this row as a candidate when
+                    // c^_ji <= its limit (cosine without zero rows: the raw
+                    // product against the column's v* form, a superset)
+                    if (PASS == 1 && colside) {
+                        const float cl_thr = ch == 0 ? cthr[0] : ch == 1 ? cthr[1] : ch == 2 ? cthr[2] : cthr[3];
+                        const float cl_vs = ch == 0 ? cvs[0] : ch == 1 ? cvs[1] : ch == 2 ? cvs[2] : cvs[3];
+                        const float cl_term = ch == 0 ? cterm[0] : ch == 1 ? cterm[1] : ch == 2 ? cterm[2] : cterm[3];
+                        uint32_t colmask = 0;
+                        if (fast_cos) {
+                            float m = cl_vs;  // smallest v* of each 8-column group
+                            m = fminf(m, __shfl_xor_sync(0xffffffffu, m, 1));
+                            m = fminf(m, __shfl_xor_sync(0xffffffffu, m, 2));
+                            m = fminf(m, __shfl_xor_sync(0xffffffffu, m, 4));
+#pragma unroll
+                            for (int g = 0; g < 4; ++g) {
+                                const float cm = __shfl_sync(0xffffffffu, m, 8 * g);
+                                float x = c[8 * g];
+#pragma unroll
+                                for (int e = 1; e < 8; ++e) x = fmaxf(x, c[8 * g + e]);
+                                if (__any_sync(0xffffffffu, valid && x >= cm)) {
+#pragma unroll
+                                    for (int e = 0; e < 8; ++e) {
+                                        const float vs = __shfl_sync(0xffffffffu, cl_vs, 8 * g + e);
+                                        if (valid && c[8 * g + e] >= vs && j0 + 8 * g + e < n)
+                                            colmask |= 1u << (8 * g + e);
+                                    }
+                                }
+                            }
+                        } else {
+                            const bool euc = J.metric == HM_METRIC_EUCLIDEAN;
+#pragma unroll
+                            for (int t = 0; t < 32; ++t) {
+                                const float lim = __shfl_sync(0xffffffffu, cl_thr, t);
+                                const float rt = __shfl_sync(0xffffffffu, cl_term, t);
+                                const float c2 = __fsub_rn(__fadd_rn(euc ? rt : 0.0f, own_ct), __fmul_rn(scale, c[t]));
+                                if (valid && j0 + t < n && !(c2 > lim)) colmask |= 1u << t;
+                            }
+                        }
+                        // stage them: one shared-memory atomic per warp and chunk
+                        const uint32_t mine = __popc(colmask);
+                        uint32_t inc = mine;
+#pragma unroll
+                        for (int o = 1; o < 32; o <<= 1) {
+                            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+                            if (lane >= o) inc += y;
+                        }
+                        const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+                        if (total) {
+                            uint32_t base = 0;
+                            if (lane == 0) base = atomicAdd(s_colcnt, total);
+                            uint32_t pos = __shfl_sync(0xffffffffu, base, 0) + inc - mine;
+                            colsum += mine;
+                            while (colmask) {
+                                const int t = __ffs(colmask) - 1;
+                                colmask &= colmask - 1;
+                                float x = c[0];
+#pragma unroll
+                                for (int q = 1; q < 32; ++q) x = (t == q) ? c[q] : x;
+                                if (pos < G.stage_cap) {
+                                    const size_t at = (size_t)blockIdx.x * G.stage_cap + pos;
+                                    G.stage_row[at] = J.row0 + j0 + t;
+                                    G.stage_key[at] = ((unsigned long long)__float_as_uint(x) << 32) | row;
+                                } else {
+                                    // a full stage: the column's row goes to the exact path
+                                    atomicMax(&G.cand_cnt[cand_list(J, j0 + t, J.elists - 2)], 2 * J.cap + 1);
+                                }
+                                ++pos;
+                            }
+                        }
+                    }
                     // cosine fast path: c = 1 - v is monotone in v, so a
                     // minimum of c is 1 - (the maximum of v), bit for bit
                     const bool quick = fast_cos && full && !self_here && (PASS == 1 || !dump);
@@ -612,17 +734,19 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                 __syncwarp();
                 if (lane == 0) mbar_arrive(smem_u32(&acce[buf]));
             }
-            if (valid) {
-                if (PASS == 0) {
+            if (!ok) break;
+            if (PASS == 0) {
+                if (valid) {
                     // the list's k smallest mini-chunk minima (ascending)
                     float *kk = G.topk + J.topk0 + (list - J.slot0) * J.k;
 #pragma unroll
                     for (int q = 0; q < KP; ++q)
                         if (q >= KP - (int)J.k) kk[q - (KP - (int)J.k)] = arr[q];
-                } else {
-                    G.cand_cnt[list] = cnt;
-                    atomicAdd(&J.cnt->emitted, (unsigned long long)cnt);
                 }
+            } else {
+                if (valid) G.cand_cnt[list] = cnt;
+                const uint32_t e = __reduce_add_sync(0xffffffffu, (valid ? cnt : 0u) + colsum);
+                if (lane == 0 && e) atomicAdd(&J.cnt->emitted, (unsigned long long)e);
             }
         }
     }
@@ -634,6 +758,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
                      "r"(SC_TMEM_COLS));
     }
+    if (PASS == 1 && threadIdx.x == 0 && G.stage_cnt) G.stage_cnt[blockIdx.x] = *s_colcnt;
 }
 
 template <int KIND, int KP, int PASS>
@@ -641,7 +766,8 @@ static int launch_kind(const JobDev *jobs, const GroupDev &G, const CUtensorMap 
                        const CUtensorMap &tb, float *dump, uint32_t idesc, cudaStream_t s) {
     HM_TRY(ensure_dynamic_smem((const void *)screen_gemm_kernel<KIND, KP, PASS>, (int)SC_SMEM_BYTES));
     const uint32_t sms = (uint32_t)device_sm_count();
-    const uint32_t grid = G.units < sms ? G.units : sms;
+    const uint32_t grid = PASS == 1 ? emission_grid(G) : (G.units < sms ? G.units : sms);
+    if (grid == 0) return HM_OK;
     // every job's K slices fit the resident A block
     const uint32_t a_res = (G.kpmax / G.kslice) <= SC_ARES_STAGES ? 1u : 0u;
     screen_gemm_kernel<KIND, KP, PASS><<<grid, SC_THREADS, SC_SMEM_BYTES, s>>>(ta, tb, jobs, G, dump, idesc,
@@ -649,6 +775,11 @@ static int launch_kind(const JobDev *jobs, const GroupDev &G, const CUtensorMap 
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();
     return HM_OK;
+}
+
+uint32_t emission_grid(const GroupDev &G) {
+    const uint32_t sms = (uint32_t)device_sm_count();
+    return G.neunits < sms ? G.neunits : sms;
 }
 
 static uint32_t make_idesc(int kind) {

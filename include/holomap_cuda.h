@@ -392,6 +392,12 @@ HM_API int hm_autotune_path(uint64_t n, uint32_t d, uint32_t k, int metric);
  * screen's threshold pass instead of the table's fraction; 0 restores the
  * table.  The results do not depend on it, only the speed. */
 HM_API int hm_tuning_override(int seed_div);
+/* Sweep and test hook (no reference counterpart): with on = 0, screened plans
+ * made on this thread run the emission pass over every column tile instead of
+ * only the tiles on and above the diagonal (each tile's values then serve its
+ * rows only).  Same results; on = 1 (the default) restores the symmetric
+ * form. */
+HM_API int hm_tuning_symmetric(int on);
 
 /* ----------------------------------------------------------------------------
  * Instrumentation (no reference counterpart; the reference has no timers on

@@ -127,3 +127,28 @@ def test_device_data_at_a_4_byte_offset(oracle, path):
     assert_same_bytes(p.idx.cpu().numpy().view(np.uint32), oi, "indices")
     assert_same_bytes(p.dist.cpu().numpy(), od, "dists")
     assert p.stats().path_used == hm.KnnPath.parse(path)
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("metric", ["euclidean", "cosine"])
+def test_full_and_symmetric_emission_agree_with_the_oracle(oracle, path, metric):
+    """The emission pass over every column tile (hm_tuning_symmetric(0)) and
+    over the tiles on and above the diagonal only (the default, whose rows
+    also take candidates as columns) return the oracle's bytes; the zero rows
+    under cosine exercise the column side's general (non raw-product) test."""
+    lib = hm.lib()
+    x = edge_case("zeros" if metric == "cosine" else "duplicates", 2600, 40, seed=5)
+    x[::7] += 0.5  # keep most rows non-zero
+    oi, od = oracle.exact_knn(x, 15, metric)
+    osig, orho = oracle.smooth_knn(od, 15)
+    for sym in (0, 1):
+        assert lib.hm_tuning_symmetric(sym) == 0
+        try:
+            st = hm.HmStats()
+            knn, sm = hm.knn_smooth(x, 40, 15, metric, path, stats=st)
+        finally:
+            lib.hm_tuning_symmetric(1)
+        assert_same_bytes(knn.indices, oi, f"sym={sym} indices")
+        assert_same_bytes(knn.dists, od, f"sym={sym} dists")
+        assert_same_bytes(sm.sigmas, osig, f"sym={sym} sigma")
+        assert_same_bytes(sm.rhos, orho, f"sym={sym} rho")
