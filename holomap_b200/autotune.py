@@ -7,7 +7,9 @@ launching stream, one full kNN + smooth-kNN run of
 
 * the plain exact binary64 path, and
 * each tensor-core screen (BF16, TF32, split-BF16) with the threshold pass
-  sampling 1/4, 1/8 and 1/16 of the columns,
+  sampling 1/4, 1/8 and 1/16 of the columns and the symmetric emission pass
+  (tiles on and above the diagonal), and the fastest of those again with the
+  emission pass over every tile,
 
 on seeded Gaussian-mixture data of that shape, checks that every screened
 result equals the plain path's bytes, and records the fastest choice.  Two
@@ -50,15 +52,16 @@ SEED_DIVS = [4, 8, 16]
 PATH_CODE = {"plain": 1, "screen_bf16": 2, "screen_tf32": 3, "screen_bf16x3": 4}
 
 
-def hand_rule(n: int, d: int, k: int, metric: str) -> tuple[str, int]:
+def hand_rule(n: int, d: int, k: int, metric: str) -> tuple[str, int, int]:
     """The choice used before any measurement exists (and the shape of the
     table when the sweep has not run): plain below 512 points, split-BF16 up
-    to d = 256, then BF16 (cosine) or TF32 (euclidean); an eighth sampled."""
+    to d = 256, then BF16 (cosine) or TF32 (euclidean); an eighth sampled;
+    the symmetric emission pass."""
     if n < 512:
-        return "plain", 8
+        return "plain", 8, 1
     if d <= 256:
-        return "screen_bf16x3", 8
-    return ("screen_bf16" if metric == "cosine" else "screen_tf32"), 8
+        return "screen_bf16x3", 8, 1
+    return ("screen_bf16" if metric == "cosine" else "screen_tf32"), 8, 1
 
 
 def _pool(d: int, n: int, seed: int) -> np.ndarray:
@@ -106,27 +109,35 @@ def sweep(grid_n=GRID_N, grid_d=GRID_D, grid_k=GRID_K, metrics=METRICS, verbose=
                     ref = (plain.idx.cpu().numpy(), plain.dist.cpu().numpy().view(np.uint32),
                            plain.sigma.cpu().numpy().view(np.uint32))
                     del plain
+                    def measure(path, sd, sym):
+                        _lib.check(lib.hm_tuning_override(sd))
+                        _lib.check(lib.hm_tuning_symmetric(sym))
+                        try:
+                            p = DeviceKnnProblem(n, d, k, metric, path)
+                            t = _time_run(p, x, 5)
+                            got = (p.idx.cpu().numpy(), p.dist.cpu().numpy().view(np.uint32),
+                                   p.sigma.cpu().numpy().view(np.uint32))
+                            same = all(np.array_equal(a, b) for a, b in zip(got, ref))
+                            del p
+                        finally:
+                            _lib.check(lib.hm_tuning_override(0))
+                            _lib.check(lib.hm_tuning_symmetric(1))
+                        return t if same else None
+
                     for path in SCREENS:
                         for sd in SEED_DIVS:
-                            _lib.check(lib.hm_tuning_override(sd))
-                            try:
-                                p = DeviceKnnProblem(n, d, k, metric, path)
-                                t = _time_run(p, x, 5)
-                                got = (p.idx.cpu().numpy(), p.dist.cpu().numpy().view(np.uint32),
-                                       p.sigma.cpu().numpy().view(np.uint32))
-                                same = all(np.array_equal(a, b) for a, b in zip(got, ref))
-                                del p
-                            finally:
-                                _lib.check(lib.hm_tuning_override(0))
-                            times[f"{path}/{sd}"] = t
-                            if not same:
-                                exact = False
-                                times[f"{path}/{sd}"] = None
+                            times[f"{path}/{sd}/sym"] = measure(path, sd, 1)
+                    screened = {c: t for c, t in times.items() if t is not None and c != "plain"}
+                    if screened:
+                        c0 = min(screened, key=screened.get)
+                        p0, sd0, _ = c0.split("/")
+                        times[f"{p0}/{sd0}/full"] = measure(p0, int(sd0), 0)
+                    exact = all(t is not None for t in times.values())
                     valid = {c: t for c, t in times.items() if t is not None}
                     best = min(valid, key=valid.get)
-                    path, sd = (best.split("/") + ["8"])[:2]
+                    path, sd, form = (best.split("/") + ["8", "sym"])[:3]
                     e = {"n": n, "d": d, "k": k, "metric": metric, "times_ms": times, "best": path,
-                         "seed_div": int(sd), "all_paths_equal_plain": exact}
+                         "seed_div": int(sd), "symmetric": int(form == "sym"), "all_paths_equal_plain": exact}
                     entries.append(e)
                     if verbose:
                         print(f"{metric:9s} d={d:4d} k={k:2d} n={n:6d}  best {best:18s} "
@@ -147,13 +158,14 @@ def sweep(grid_n=GRID_N, grid_d=GRID_D, grid_k=GRID_K, metrics=METRICS, verbose=
 
 
 def table_from(doc: dict | None) -> tuple[dict, list, list, list]:
-    """(choice[(metric, k, d, n)] = (path, seed_div), grid n, d, k)."""
+    """(choice[(metric, k, d, n)] = (path, seed_div, symmetric), grid n, d, k)."""
     if doc is None:
         gn, gd, gk = GRID_N, GRID_D, GRID_K
         choice = {(m, k, d, n): hand_rule(n, d, k, m) for m in METRICS for k in gk for d in gd for n in gn}
         return choice, gn, gd, gk
     g = doc["grid"]
-    choice = {(e["metric"], e["k"], e["d"], e["n"]): (e["best"], e["seed_div"]) for e in doc["entries"]}
+    choice = {(e["metric"], e["k"], e["d"], e["n"]): (e["best"], e["seed_div"], e.get("symmetric", 1))
+              for e in doc["entries"]}
     return choice, g["n"], g["d"], g["k"]
 
 
@@ -169,9 +181,9 @@ def describe(n: int, d: int, k: int, metric: str) -> dict:
     doc = json.loads(JSON_PATH.read_text()) if JSON_PATH.exists() else None
     choice, gn, gd, gk = table_from(doc)
     key = (metric, _nearest(gk, k), _nearest(gd, d), _nearest(gn, n))
-    path, sd = choice[key]
+    path, sd, sym = choice[key]
     out = {"grid_point": {"metric": key[0], "k": key[1], "d": key[2], "n": key[3]},
-           "choice": path, "seed_div": sd,
+           "choice": path, "seed_div": sd, "symmetric_emission": bool(sym),
            "table": f"measured {doc['measured']} on {doc['device']}" if doc else "hand rule (no measurement)"}
     if doc:
         for e in doc["entries"]:
@@ -187,7 +199,8 @@ def emit_inc(doc: dict | None, path: Path = INC_PATH) -> None:
         "// autotune_table.inc -- generated by holomap_b200/autotune.py from",
         "// holomap_b200/autotune_table.json; do not edit by hand.",
         f"// Source: {src}.",
-        "// kTune[metric][k][d][n] = path | seed_div << 8 at the grid points below",
+        "// kTune[metric][k][d][n] = path | seed_div << 8 | symmetric << 15 at the grid",
+        "// points below",
         "// (metric 0 euclidean, 1 cosine).",
         "#pragma once",
         f"static const uint32_t kTuneN[{len(gn)}] = {{{', '.join(map(str, gn))}}};",
@@ -202,8 +215,8 @@ def emit_inc(doc: dict | None, path: Path = INC_PATH) -> None:
             for d in gd:
                 row = []
                 for n in gn:
-                    p, sd = choice[(m, k, d, n)]
-                    row.append(str(PATH_CODE[p] | (int(sd) << 8)))
+                    p, sd, sym = choice[(m, k, d, n)]
+                    row.append(str(PATH_CODE[p] | (int(sd) << 8) | (int(sym) << 15)))
                 lines.append("            {" + ", ".join(row) + "},")
             lines.append("        },")
         lines.append("    },")

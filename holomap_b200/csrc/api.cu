@@ -135,7 +135,6 @@ struct hm_batch {
     uint32_t fb_per_job[3] = {1, 1, 1};
     std::vector<uint32_t> job_blocks;  // prep block offsets
     bool any_plain = false, any_screen = false, any_smooth = false, any_split = false;
-    bool sym_enabled = true;  // symmetric emission for whole datasets
     size_t off_tables = 0, off_jobs = 0, off_counters = 0, off_row_starts = 0, off_job_blocks = 0;
     size_t off_items[3] = {}, off_fb[3] = {};
     size_t tables_bytes = 0, tables_used = 0, total = 0;
@@ -168,7 +167,6 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
     if (njobs > (1u << 16)) return set_error(HM_ERR_UNSUPPORTED, "more than 65536 jobs");
     const uint32_t G = (uint32_t)sm_count();
     B.jobs.assign(njobs, JobPlan{});
-    B.sym_enabled = tuning_symmetric();
     for (int g = 0; g < 3; ++g) B.groups[g] = GroupPlan{};
     B.groups[0].kind = SCREEN_KIND_BF16;
     B.groups[1].kind = SCREEN_KIND_TF32;
@@ -280,7 +278,8 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
             // table's choice for the shape), at least 2048 (all of them for
             // small jobs), spread over the parts
             uint32_t seed_div = 8;
-            autotune_choice(P.spec.n, P.spec.d, P.spec.k, P.spec.metric, &seed_div);
+            bool sym_ok = true;
+            autotune_choice(P.spec.n, P.spec.d, P.spec.k, P.spec.metric, &seed_div, &sym_ok);
             const uint64_t seed_cols = std::max<uint64_t>(P.spec.n / std::max<uint32_t>(seed_div, 1), 2048);
             P.seed_tiles = std::min<uint32_t>(
                 P.part_tiles, (uint32_t)((seed_cols + (uint64_t)SC_BN * P.parts - 1) / ((uint64_t)SC_BN * P.parts)));
@@ -304,7 +303,7 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
             // blocks above the diagonal get their candidates as columns.  Its
             // candidate lists per row: two per part, then the column list,
             // which takes two lists' room.
-            P.sym = B.sym_enabled && P.q0 == 0 && P.q1 == P.spec.n && P.col_tiles >= 2;
+            P.sym = sym_ok && P.q0 == 0 && P.q1 == P.spec.n && P.col_tiles >= 2;
             if (P.sym) {
                 uint64_t tiles = 0;
                 for (uint32_t rb = 0; rb < P.row_blocks; ++rb) tiles += P.col_tiles - rb / 2;

@@ -7,7 +7,7 @@
 // plain path and the three screens (each with 1/4, 1/8 or 1/16 of the columns
 // sampled), all of which return the same bytes.  A problem takes the choice of
 // the nearest grid point (n by ratio, d by ratio, k by the nearer of the
-// measured k).  Where no screen applies (manhattan, k > 64, d > 2048) the path
+// measured k), including whether the emission pass takes the symmetric form.  Where no screen applies (manhattan, k > 64, d > 2048) the path
 // is plain.
 #include <cuda_runtime.h>
 
@@ -20,8 +20,6 @@ namespace hm {
 
 static thread_local uint32_t g_seed_override = 0;
 static thread_local bool g_symmetric = true;
-
-bool tuning_symmetric() { return g_symmetric; }
 
 template <size_t N>
 static size_t nearest_ratio(const uint32_t (&grid)[N], double v) {
@@ -44,13 +42,15 @@ static uint16_t table_entry(uint64_t n, uint32_t d, uint32_t k, int metric) {
     return kTune[metric == HM_METRIC_COSINE ? 1 : 0][ik][id][in];
 }
 
-int autotune_choice(uint64_t n, uint32_t d, uint32_t k, int metric, uint32_t *seed_div) {
+int autotune_choice(uint64_t n, uint32_t d, uint32_t k, int metric, uint32_t *seed_div, bool *symmetric) {
     if (metric == HM_METRIC_MANHATTAN || k > 64 || d > 2048) {
         if (seed_div) *seed_div = 8;
+        if (symmetric) *symmetric = true;
         return HM_PATH_PLAIN;
     }
     const uint16_t e = table_entry(n, d, k, metric);
-    if (seed_div) *seed_div = g_seed_override ? g_seed_override : (uint32_t)(e >> 8);
+    if (seed_div) *seed_div = g_seed_override ? g_seed_override : (uint32_t)((e >> 8) & 0x7f);
+    if (symmetric) *symmetric = g_symmetric && (e >> 15) != 0;
     return (int)(e & 0xff);
 }
 
@@ -61,7 +61,7 @@ using namespace hm;
 extern "C" {
 
 int hm_autotune_path(uint64_t n, uint32_t d, uint32_t k, int metric) {
-    return autotune_choice(n, d, k, metric, nullptr);
+    return autotune_choice(n, d, k, metric, nullptr, nullptr);
 }
 
 int hm_tuning_override(int seed_div) {

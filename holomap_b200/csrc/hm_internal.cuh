@@ -211,12 +211,11 @@ __device__ __forceinline__ uint32_t find_job(const uint32_t *starts, uint32_t nj
 
 int kpl_for_k(uint32_t k);  // 1, 2, 4, 8 or 0 if k > 256
 
-// The autotuner table's path for a problem and (seed_div) the fraction
-// 1/seed_div of the columns the screen's threshold pass samples.
-int autotune_choice(uint64_t n, uint32_t d, uint32_t k, int metric, uint32_t *seed_div);
-// whether screened plans made on this thread may use the symmetric emission
-// pass (hm_tuning_symmetric; on by default)
-bool tuning_symmetric();
+// The autotuner table's path for a problem, (seed_div) the fraction
+// 1/seed_div of the columns the screen's threshold pass samples, and
+// (symmetric) whether its emission pass takes the symmetric form (never when
+// hm_tuning_symmetric(0) is in force on this thread).
+int autotune_choice(uint64_t n, uint32_t d, uint32_t k, int metric, uint32_t *seed_div, bool *symmetric);
 
 // ------------------------------------------------------------- plain path
 constexpr int PL_BM = 32;     // rows per CTA (8 warps x 4 rows)
