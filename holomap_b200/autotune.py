@@ -56,12 +56,12 @@ def hand_rule(n: int, d: int, k: int, metric: str) -> tuple[str, int, int]:
     """The choice used before any measurement exists (and the shape of the
     table when the sweep has not run): plain below 512 points, split-BF16 up
     to d = 256, then BF16 (cosine) or TF32 (euclidean); an eighth sampled;
-    the symmetric emission pass."""
+    the emission pass over every column tile."""
     if n < 512:
-        return "plain", 8, 1
+        return "plain", 8, 0
     if d <= 256:
-        return "screen_bf16x3", 8, 1
-    return ("screen_bf16" if metric == "cosine" else "screen_tf32"), 8, 1
+        return "screen_bf16x3", 8, 0
+    return ("screen_bf16" if metric == "cosine" else "screen_tf32"), 8, 0
 
 
 def _pool(d: int, n: int, seed: int) -> np.ndarray:

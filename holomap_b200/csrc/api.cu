@@ -118,6 +118,7 @@ struct GroupPlan {
     size_t off_opa = 0, off_opb = 0, off_rowstat = 0, off_rowterm = 0, off_colterm = 0;
     size_t off_band = 0, off_force = 0, off_rowthr = 0, off_cand = 0, off_cnt = 0, off_topk = 0;
     size_t off_ethr = 0, off_evstar = 0, off_stage_row = 0, off_stage_key = 0, off_stage_cnt = 0;
+    size_t off_rowcnt = 0;
     // tables
     size_t off_gdev = 0, off_job_ids = 0, off_row_starts = 0, off_unit_starts = 0, off_eunits = 0;
     GroupDev host{};
@@ -308,6 +309,7 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
                 uint64_t tiles = 0;
                 for (uint32_t rb = 0; rb < P.row_blocks; ++rb) tiles += P.col_tiles - rb / 2;
                 P.ept = (uint32_t)std::max<uint64_t>(4, (tiles + 4ull * G - 1) / (4ull * G));
+                P.ept = std::max<uint32_t>(P.ept, (P.col_tiles + 7) / 8);  // at most 8 parts: 18 lists
                 const uint32_t eparts = (P.col_tiles + P.ept - 1) / P.ept;
                 P.elists = 2 * eparts + 2;
                 Gp.any_sym = true;
@@ -440,6 +442,7 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
         Gp.off_cand = take(Gp.cand * sizeof(unsigned long long));
         Gp.off_cnt = take(Gp.elists * sizeof(uint32_t));
         Gp.off_topk = take(Gp.topk * sizeof(float));
+        Gp.off_rowcnt = take(rows * sizeof(uint32_t));
         if (Gp.any_sym) {
             const size_t padded = round_up(rows, SC_BN) + SC_BN;
             Gp.off_ethr = take(padded * sizeof(float));
@@ -591,6 +594,7 @@ static int bind_batch(hm_batch &B, void *d_ws, size_t bytes, cudaStream_t s) {
         D.cand = at<unsigned long long>(ws, Gp.off_cand);
         D.cand_cnt = at<uint32_t>(ws, Gp.off_cnt);
         D.topk = at<float>(ws, Gp.off_topk);
+        D.row_cnt = at<uint32_t>(ws, Gp.off_rowcnt);
         D.eunits = at<uint4>(ws, Gp.off_eunits);
         D.neunits = (uint32_t)Gp.eunits.size();
         if (Gp.any_sym) {

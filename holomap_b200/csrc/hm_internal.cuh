@@ -83,6 +83,11 @@ __device__ __forceinline__ uint64_t shfl_u64(uint64_t v, int src) {
     uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(v >> 32), src);
     return ((uint64_t)hi << 32) | lo;
 }
+__device__ __forceinline__ uint64_t shfl_xor_u64(uint64_t v, int mask) {
+    uint32_t lo = __shfl_xor_sync(0xffffffffu, (uint32_t)v, mask);
+    uint32_t hi = __shfl_xor_sync(0xffffffffu, (uint32_t)(v >> 32), mask);
+    return ((uint64_t)hi << 32) | lo;
+}
 __device__ __forceinline__ uint64_t shfl_up_u64(uint64_t v, int delta) {
     uint32_t lo = __shfl_up_sync(0xffffffffu, (uint32_t)v, delta);
     uint32_t hi = __shfl_up_sync(0xffffffffu, (uint32_t)(v >> 32), delta);

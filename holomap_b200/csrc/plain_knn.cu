@@ -92,22 +92,35 @@ __global__ void __launch_bounds__(NRM_WARPS * 32) check_norms_kernel(const JobDe
     const uint32_t dmax = __reduce_max_sync(0xffffffffu, d);
     double acc = 0.0;
     for (uint32_t c0 = 0; c0 < dmax; c0 += 32) {
-        // row i of the warp, dimension c0 + lane: coalesced per row
+        // row i of the warp, dimension c0 + lane: coalesced per row; all 32
+        // rows' loads are issued before any is used
+        float v[32];
+#pragma unroll
         for (int i = 0; i < 32; ++i) {
             const float *src = reinterpret_cast<const float *>(
                 __shfl_sync(0xffffffffu, reinterpret_cast<uintptr_t>(xrow), i));
             const uint32_t di = __shfl_sync(0xffffffffu, d, i);
+            v[i] = (c0 + lane < di) ? src[c0 + lane] : 0.0f;
+        }
+        uint32_t bad = 0;
+#pragma unroll
+        for (int i = 0; i < 32; ++i) bad |= isfinite(v[i]) ? 0u : (1u << i);
+        bad = __reduce_or_sync(0xffffffffu, bad);
+        while (bad) {  // rare: a non-finite value in one of the rows
+            const int i = __ffs(bad) - 1;
+            bad &= bad - 1;
+            const uint32_t di = __shfl_sync(0xffffffffu, d, i);
             const uint32_t ri = __shfl_sync(0xffffffffu, row, i);
             const uint32_t ji = __shfl_sync(0xffffffffu, jb, i);
-            float v = 0.0f;
-            if (c0 + lane < di) {
-                v = src[c0 + lane];
-                if (!isfinite(v))
-                    atomicMin(&jobs[ji].cnt->nonfinite_min,
-                              (uint32_t)min((size_t)ri * di + c0 + lane, (size_t)0xfffffffeull));
-            }
-            tile[warp][i][lane] = v;
+            float vi = 0.0f;
+#pragma unroll
+            for (int q = 0; q < 32; ++q) vi = (q == i) ? v[q] : vi;
+            if (c0 + lane < di && !isfinite(vi))
+                atomicMin(&jobs[ji].cnt->nonfinite_min,
+                          (uint32_t)min((size_t)ri * di + c0 + lane, (size_t)0xfffffffeull));
         }
+#pragma unroll
+        for (int i = 0; i < 32; ++i) tile[warp][i][lane] = v[i];
         __syncwarp();
         if (cos) {
             const uint32_t tmax = min(32u, d - min(d, c0));

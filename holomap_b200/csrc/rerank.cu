@@ -96,9 +96,10 @@ __device__ __forceinline__ uint32_t kth_of(KeyFn key, uint32_t total, uint32_t k
     return kth_load<16>(key, total, k, lane);
 }
 
-constexpr int RR_ROWS = 8;        // group rows per warp
-constexpr int RR_WARPS = 4;       // warps per block
+constexpr int RR_ROWS = 8;        // group rows per warp of the exact phase
+constexpr int RR_WARPS = 4;       // warps per block of the exact phase
 constexpr int RR_CBUF = 512;      // emitted candidates a warp stages in shared memory
+constexpr int RS_WARPS = 8;       // rows (warps) per block of the select and top-k phases
 constexpr int RR_STAGES = 3;      // chunks in flight
 constexpr int RR_CH = 32;         // dimensions per chunk
 constexpr int RR_XJ_STRIDE = 36;  // floats per staged candidate chunk (144 B: 16-byte aligned rows
@@ -106,18 +107,22 @@ constexpr int RR_XJ_STRIDE = 36;  // floats per staged candidate chunk (144 B: 1
 constexpr int RR_QROWS = 4;       // query rows per slice
 constexpr int RR_XI_STRIDE = 36;  // doubles per converted query-row chunk (rows 8 banks apart)
 
-// Shared memory of one warp: the select phase's staging buffer and the exact
-// phase's chunk pipeline are never live together.
+// Shared memory of one warp of the exact phase: the chunk pipeline.
 struct RrWarpSmem {
-    union {
-        unsigned long long cbuf[RR_CBUF];
-        struct {
-            float xj[RR_STAGES][32][RR_XJ_STRIDE];
-            float xi[RR_STAGES][RR_QROWS][32];
-            double xid[RR_QROWS][RR_XI_STRIDE];
-            uint32_t cj[32];
-        } ex;
-    };
+    struct {
+        float xj[RR_STAGES][32][RR_XJ_STRIDE];
+        float xi[RR_STAGES][RR_QROWS][32];
+        double xid[RR_QROWS][RR_XI_STRIDE];
+        uint32_t cj[32];
+    } ex;
+};
+
+// Shared memory of one warp of the select phase: the row's emitted
+// candidates and the radix-select histogram.
+struct RsWarpSmem {
+    unsigned long long cbuf[RR_CBUF];
+    uint32_t hist[256];
+    uint32_t loff[32];  // first staged position of each list
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -149,23 +154,94 @@ __device__ __forceinline__ uint32_t list_cap(const JobDev &J, uint32_t s) {
     return (J.sym && s == J.elists - 2) ? 2 * J.cap : J.cap;
 }
 
-// Phase 1 for one row: returns the survivor count (0 for rows sent to the
-// exact fallback).
+// k-th smallest (1-based k <= total) of the order-preserving keys held in
+// registers (lane l: keys l, l + 32, ...; NQ per lane), by a most-significant-
+// byte-first radix select: each pass counts the keys that share the bytes
+// chosen so far in 256 shared-memory bins, and the bin holding the k-th
+// fixes the next byte.  Bytes the keys all share are skipped.
+template <int NQ>
+__device__ __forceinline__ uint32_t radix_kth(const uint32_t (&key)[NQ], uint32_t total, uint32_t k,
+                                              uint32_t *hist, int lane) {
+    uint32_t mn = 0xffffffffu, mx = 0u;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+        if ((uint32_t)(q * 32 + lane) < total) {
+            mn = min(mn, key[q]);
+            mx = max(mx, key[q]);
+        }
+    }
+    mn = __reduce_min_sync(0xffffffffu, mn);
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if (mn == mx) return mn;
+    const int hb = (31 - __clz(mn ^ mx)) >> 3;  // highest byte where the keys differ
+    uint32_t mask = hb == 3 ? 0u : ~((1u << (8 * hb + 8)) - 1u);
+    uint32_t prefix = mn & mask, kk = k;
+    for (int shift = 8 * hb; shift >= 0; shift -= 8) {
+        for (int b = lane; b < 256; b += 32) hist[b] = 0u;
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < NQ; ++q)
+            if ((uint32_t)(q * 32 + lane) < total && (key[q] & mask) == prefix)
+                atomicAdd(&hist[(key[q] >> shift) & 255u], 1u);
+        __syncwarp();
+        // lane l holds bins [8 l, 8 l + 8): the bin where the count reaches kk
+        uint32_t h[8], sum = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            h[j] = hist[8 * lane + j];
+            sum += h[j];
+        }
+        uint32_t incl = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int owner = __ffs(__ballot_sync(0xffffffffu, incl >= kk)) - 1;
+        uint32_t bin = 0, below = incl - sum;
+        bool found = false;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            if (!found && below + h[j] >= kk) {
+                bin = 8 * lane + j;
+                found = true;
+            } else if (!found) {
+                below += h[j];
+            }
+        }
+        bin = __shfl_sync(0xffffffffu, bin, owner);
+        below = __shfl_sync(0xffffffffu, below, owner);
+        kk -= below;
+        prefix |= bin << shift;
+        mask |= 255u << shift;
+        __syncwarp();
+    }
+    return prefix;
+}
+
+template <int NQ>
+__device__ __forceinline__ uint32_t kth_staged(const unsigned long long *cbuf, uint32_t total, uint32_t k,
+                                               uint32_t *hist, int lane) {
+    uint32_t key[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+        const uint32_t e = q * 32 + lane;
+        key[q] = e < total ? ord32(__uint_as_float((uint32_t)(cbuf[e] >> 32))) : 0xffffffffu;
+    }
+    return radix_kth<NQ>(key, total, k, hist, lane);
+}
+
+// Select phase for one row: returns the survivor count (0 for rows sent to
+// the exact fallback).
 template <int KPL>
 __device__ __forceinline__ uint32_t select_row(const JobDev &J, const GroupDev &G, uint32_t gr, uint32_t row,
-                                               RrWarpSmem &sm, int lane) {
+                                               RsWarpSmem &sm, int lane) {
     const uint32_t k = J.k, lists = J.elists;
     const size_t l0 = cand_list(J, row, 0);
-    // overflow / unbounded rows go to the exact plain path
-    bool ovf = G.force[gr] != 0;
-    uint32_t total = 0;
-    for (uint32_t p = lane; p < lists; p += 32) {
-        const uint32_t c = G.cand_cnt[l0 + p];
-        ovf |= c > list_cap(J, p);
-        total += c;
-    }
-    ovf = __any_sync(0xffffffffu, ovf);
-    total = __reduce_add_sync(0xffffffffu, total);
+    // lane p < lists holds list p's count; overflow / unbounded rows go to
+    // the exact plain path
+    const uint32_t myc = (uint32_t)lane < lists ? G.cand_cnt[l0 + lane] : 0u;
+    const bool ovf = __any_sync(0xffffffffu, G.force[gr] != 0 || ((uint32_t)lane < lists && myc > list_cap(J, lane)));
     if (ovf) {
         if (lane == 0) {
             const uint32_t at = atomicAdd(&J.cnt->ovf_count, 1u);
@@ -173,25 +249,55 @@ __device__ __forceinline__ uint32_t select_row(const JobDev &J, const GroupDev &
         }
         return 0;
     }
+    uint32_t incl = myc;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
     unsigned long long *region = row_region(J, G, row);
     // Threshold: the exact k-th smallest screened value of the row, over the
     // emitted candidates (they include the row's k smallest).  Up to RR_CBUF
-    // candidates are staged in shared memory and the k-th found by a bitwise
-    // search on the order-preserving keys; longer rows use a warp top-k.
+    // candidates are staged in shared memory (every list's chunk c loaded
+    // before any is stored) and the k-th found by a radix select; longer rows
+    // use a warp top-k.
     const bool staged = total <= RR_CBUF;
     float tau = __int_as_float(0x7f800000);
     if (staged) {
-        uint32_t base = 0;
-        for (uint32_t p = 0; p < lists; ++p) {
-            const uint32_t cnt = G.cand_cnt[l0 + p];
-            const unsigned long long *cand = region + (size_t)p * J.cap;
-            for (uint32_t e = lane; e < cnt; e += 32) sm.cbuf[base + e] = cand[e];
-            base += cnt;
+        // flat copy: staged position e lies in the last list whose first
+        // position is <= e (an empty list shares its successor's first
+        // position, so the search lands on the list that holds e)
+        if ((uint32_t)lane < lists) sm.loff[lane] = incl - myc;
+        __syncwarp();
+        for (uint32_t e0 = 0; e0 < total; e0 += 128) {
+            unsigned long long v[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t e = e0 + 32 * u + lane;
+                if (e < total) {
+                    uint32_t lo = 0, hi = lists;
+                    while (hi - lo > 1) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (sm.loff[mid] <= e) lo = mid; else hi = mid;
+                    }
+                    v[u] = region[(size_t)lo * J.cap + (e - sm.loff[lo])];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const uint32_t e = e0 + 32 * u + lane;
+                if (e < total) sm.cbuf[e] = v[u];
+            }
         }
         __syncwarp();
-        if (total >= k)
-            tau = unord32(kth_of([&](uint32_t e) { return ord32(__uint_as_float((uint32_t)(sm.cbuf[e] >> 32))); },
-                                 total, k, lane));
+        if (total >= k) {
+            uint32_t r;
+            if (total <= 128) r = kth_staged<4>(sm.cbuf, total, k, sm.hist, lane);
+            else if (total <= 256) r = kth_staged<8>(sm.cbuf, total, k, sm.hist, lane);
+            else r = kth_staged<16>(sm.cbuf, total, k, sm.hist, lane);
+            tau = unord32(r);
+        }
     } else {
         WarpTopK<KPL> sel;
         sel.reset();
@@ -237,6 +343,40 @@ __device__ __forceinline__ uint32_t select_row(const JobDev &J, const GroupDev &
     }
     __syncwarp();
     return fill;
+}
+
+// Select phase: one warp per group row; the block's rows (8-aligned) belong
+// to one job, whose counters take one update per block.
+template <int KPL>
+__global__ void __launch_bounds__(RS_WARPS * 32, 4) rr_select_kernel(const JobDev *__restrict__ jobs,
+                                                                  const GroupDev *__restrict__ Gp) {
+    extern __shared__ __align__(16) unsigned char rs_smem_raw[];
+    __shared__ uint32_t s_kept[RS_WARPS];
+    const GroupDev &G = *Gp;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    RsWarpSmem &sm = reinterpret_cast<RsWarpSmem *>(rs_smem_raw)[warp];
+    const uint32_t gr = blockIdx.x * RS_WARPS + warp;
+    const uint32_t g0 = blockIdx.x * RS_WARPS;
+    const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, g0 < G.rows ? g0 : 0u)]];
+    uint32_t c = 0;
+    if (gr < G.rows) {
+        const uint32_t row = gr - J.row0;
+        if (row < J.n && row >= J.q0 && row < J.q1) c = select_row<KPL>(J, G, gr, row, sm, lane);
+        if (lane == 0) G.row_cnt[gr] = c;
+    }
+    if (lane == 0) s_kept[warp] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t sum = 0, mx = 0;
+        for (int w = 0; w < RS_WARPS; ++w) {
+            sum += s_kept[w];
+            mx = max(mx, s_kept[w]);
+        }
+        if (sum) {
+            atomicAdd(&J.cnt->candidates, (unsigned long long)sum);
+            atomicMax(&J.cnt->max_row, mx);
+        }
+    }
 }
 
 // Phase 2: exact distances of the flat survivor sequence of the warp's rows
@@ -363,56 +503,87 @@ __device__ __forceinline__ void exact_pairs(const JobDev &J, const GroupDev &G, 
     }
 }
 
-template <int KPL>
-__global__ void __launch_bounds__(RR_WARPS * 32) rerank_kernel(const JobDev *__restrict__ jobs,
-                                                               const GroupDev *__restrict__ Gp) {
+// Exact phase: one warp per 8 consecutive group rows (always of one job:
+// each job's rows start 32-aligned in the group).
+__global__ void __launch_bounds__(RR_WARPS * 32) rr_exact_kernel(const JobDev *__restrict__ jobs,
+                                                                 const GroupDev *__restrict__ Gp) {
     extern __shared__ __align__(16) unsigned char rr_smem_raw[];
     const GroupDev &G = *Gp;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     RrWarpSmem &sm = reinterpret_cast<RrWarpSmem *>(rr_smem_raw)[warp];
     const uint32_t gr0 = (blockIdx.x * RR_WARPS + warp) * RR_ROWS;
     if (gr0 >= G.rows) return;
-    // gr0 is 8-aligned and every job's rows start 32-aligned: the warp's
-    // rows belong to one job (or are padding after it)
     const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr0)]];
-    uint32_t cnt_l = 0, kept = 0, kept_max = 0;
-    for (uint32_t r = 0; r < RR_ROWS; ++r) {
-        const uint32_t row = gr0 + r - J.row0;
-        uint32_t c = 0;
-        if (row < J.n && row >= J.q0 && row < J.q1) c = select_row<KPL>(J, G, gr0 + r, row, sm, lane);
-        if ((uint32_t)lane == r) cnt_l = c;
-        kept += c;
-        kept_max = max(kept_max, c);
-    }
-    if (__any_sync(0xffffffffu, cnt_l != 0)) {
-        if (J.metric == HM_METRIC_EUCLIDEAN)
-            exact_pairs<HM_METRIC_EUCLIDEAN>(J, G, gr0, cnt_l, sm, lane);
-        else
-            exact_pairs<HM_METRIC_COSINE>(J, G, gr0, cnt_l, sm, lane);
-    }
-    // phase 3: each row's k smallest exact keys
-    const uint32_t k = J.k;
-    for (uint32_t r = 0; r < RR_ROWS; ++r) {
-        const uint32_t c = __shfl_sync(0xffffffffu, cnt_l, r);
-        if (c == 0) continue;
-        const uint32_t row = gr0 + r - J.row0;
-        const unsigned long long *keys = row_region(J, G, row);
-        WarpTopK<KPL> top;
-        top.reset();
-        for (uint32_t e0 = 0; e0 < c; e0 += 32)
-            top.offer(e0 + lane < c ? (uint64_t)keys[e0 + lane] : KEY_NONE, k, lane);
+    const uint32_t cnt_l = lane < RR_ROWS ? G.row_cnt[gr0 + lane] : 0u;
+    if (!__any_sync(0xffffffffu, cnt_l != 0)) return;
+    if (J.metric == HM_METRIC_EUCLIDEAN)
+        exact_pairs<HM_METRIC_EUCLIDEAN>(J, G, gr0, cnt_l, sm, lane);
+    else
+        exact_pairs<HM_METRIC_COSINE>(J, G, gr0, cnt_l, sm, lane);
+}
+
+// Bitonic sort of 64 keys held two per lane (element lane and 32 + lane),
+// ascending.
+__device__ __forceinline__ void bitonic64(uint64_t &a, uint64_t &b, int lane) {
 #pragma unroll
-        for (int q = 0; q < KPL; ++q) {
-            const uint32_t e = q * 32 + lane;
-            if (e < k) {
-                J.idx[(size_t)row * k + e] = key_idx(top.v[q]);
-                J.dist[(size_t)row * k + e] = key_dist(top.v[q]);
+    for (int size = 2; size <= 64; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            if (stride == 32) {
+                const uint64_t lo = a < b ? a : b, hi = a < b ? b : a;
+                a = lo;  // size 64: every pair ascending
+                b = hi;
+            } else {
+                const bool lower = (lane & stride) == 0;
+                const uint64_t pa = shfl_xor_u64(a, stride), pb = shfl_xor_u64(b, stride);
+                const bool asc0 = (lane & size) == 0, asc1 = ((32 + lane) & size) == 0;
+                a = (lower == asc0) ? (a < pa ? a : pa) : (a < pa ? pa : a);
+                b = (lower == asc1) ? (b < pb ? b : pb) : (b < pb ? pb : b);
             }
         }
     }
-    if (lane == 0 && kept) {
-        atomicAdd(&J.cnt->candidates, (unsigned long long)kept);
-        atomicMax(&J.cnt->max_row, kept_max);
+}
+
+// Top-k phase: one warp per group row; the k smallest exact keys of the
+// row's survivors are its output.
+template <int KPL>
+__global__ void __launch_bounds__(RS_WARPS * 32) rr_topk_kernel(const JobDev *__restrict__ jobs,
+                                                                const GroupDev *__restrict__ Gp) {
+    const GroupDev &G = *Gp;
+    const int lane = threadIdx.x & 31;
+    const uint32_t gr = blockIdx.x * RS_WARPS + (threadIdx.x >> 5);
+    if (gr >= G.rows) return;
+    const uint32_t c = G.row_cnt[gr];
+    if (c == 0) return;
+    const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
+    const uint32_t row = gr - J.row0, k = J.k;
+    const unsigned long long *keys = row_region(J, G, row);
+    uint32_t *idx = J.idx + (size_t)row * k;
+    float *dist = J.dist + (size_t)row * k;
+    if (c <= 64) {
+        uint64_t a = (uint32_t)lane < c ? (uint64_t)keys[lane] : KEY_NONE;
+        uint64_t b = 32u + lane < c ? (uint64_t)keys[32 + lane] : KEY_NONE;
+        bitonic64(a, b, lane);
+        if ((uint32_t)lane < k) {
+            idx[lane] = key_idx(a);
+            dist[lane] = key_dist(a);
+        }
+        if (32u + lane < k) {
+            idx[32 + lane] = key_idx(b);
+            dist[32 + lane] = key_dist(b);
+        }
+        return;
+    }
+    WarpTopK<KPL> top;
+    top.reset();
+    for (uint32_t e0 = 0; e0 < c; e0 += 32) top.offer(e0 + lane < c ? (uint64_t)keys[e0 + lane] : KEY_NONE, k, lane);
+#pragma unroll
+    for (int q = 0; q < KPL; ++q) {
+        const uint32_t e = q * 32 + lane;
+        if (e < k) {
+            idx[e] = key_idx(top.v[q]);
+            dist[e] = key_dist(top.v[q]);
+        }
     }
 }
 
@@ -536,27 +707,34 @@ int launch_screen_threshold(const JobDev *jobs, const GroupDev &G, const GroupDe
     return HM_OK;
 }
 
-// One launch covers every job of the group, both metrics.
+// Three launches cover every job of the group, both metrics: select (the
+// exact tau^ and the survivors), exact distances, per-row top-k.
 int launch_rerank(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t kpl, uint32_t,
                   int, cudaStream_t s) {
     if (G.rows == 0) return HM_OK;
+    if (kpl != 1 && kpl != 2) return set_error(HM_ERR_UNSUPPORTED, "rerank width %u", kpl);
     ScopedKernelTimer timer(HM_KCLASS_SELECT, s);
-    const size_t smem = (size_t)RR_WARPS * sizeof(RrWarpSmem);
-    const uint32_t warps = (G.rows + RR_ROWS - 1) / RR_ROWS;
-    const int blocks = (int)((warps + RR_WARPS - 1) / RR_WARPS);
-    switch (kpl) {
-    case 1:
-        HM_TRY(ensure_dynamic_smem((const void *)rerank_kernel<1>, (int)smem));
-        rerank_kernel<1><<<blocks, RR_WARPS * 32, smem, s>>>(jobs, Gd);
-        break;
-    case 2:
-        HM_TRY(ensure_dynamic_smem((const void *)rerank_kernel<2>, (int)smem));
-        rerank_kernel<2><<<blocks, RR_WARPS * 32, smem, s>>>(jobs, Gd);
-        break;
-    default: return set_error(HM_ERR_UNSUPPORTED, "rerank width %u", kpl);
+    const int rs_blocks = (int)((G.rows + RS_WARPS - 1) / RS_WARPS);
+    const size_t rs_smem = (size_t)RS_WARPS * sizeof(RsWarpSmem);
+    if (kpl == 1) {
+        HM_TRY(ensure_dynamic_smem((const void *)rr_select_kernel<1>, (int)rs_smem));
+        rr_select_kernel<1><<<rs_blocks, RS_WARPS * 32, rs_smem, s>>>(jobs, Gd);
+    } else {
+        HM_TRY(ensure_dynamic_smem((const void *)rr_select_kernel<2>, (int)rs_smem));
+        rr_select_kernel<2><<<rs_blocks, RS_WARPS * 32, rs_smem, s>>>(jobs, Gd);
     }
     HM_CUDA_TRY(cudaGetLastError());
-    count_launch();
+    const size_t ex_smem = (size_t)RR_WARPS * sizeof(RrWarpSmem);
+    const uint32_t warps = (G.rows + RR_ROWS - 1) / RR_ROWS;
+    HM_TRY(ensure_dynamic_smem((const void *)rr_exact_kernel, (int)ex_smem));
+    rr_exact_kernel<<<(int)((warps + RR_WARPS - 1) / RR_WARPS), RR_WARPS * 32, ex_smem, s>>>(jobs, Gd);
+    HM_CUDA_TRY(cudaGetLastError());
+    if (kpl == 1)
+        rr_topk_kernel<1><<<rs_blocks, RS_WARPS * 32, 0, s>>>(jobs, Gd);
+    else
+        rr_topk_kernel<2><<<rs_blocks, RS_WARPS * 32, 0, s>>>(jobs, Gd);
+    HM_CUDA_TRY(cudaGetLastError());
+    count_launch(3);
     return HM_OK;
 }
 

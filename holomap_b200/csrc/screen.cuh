@@ -72,6 +72,7 @@ struct GroupDev {
     unsigned long long *cand;     // candidate lists, (c^ bits << 32) | job-local column
     uint32_t *cand_cnt;
     float *topk;                  // each list's k smallest mini-chunk minima, ascending
+    uint32_t *row_cnt;            // rerank: survivors per group row (0: none or exact fallback)
     // emission pass: its work units (x = group job slot | sym << 31, y = row
     // block, z = first column tile, w = end column tile | column part << 24),
     // largest first

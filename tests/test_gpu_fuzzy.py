@@ -180,9 +180,10 @@ def test_device_entry_point_reports_an_index_not_below_n(oracle):
     n, k = 3000, 10
     idx, dist = random_knn(n, k, seed=17)
     sm = hm.smooth_knn(dist, k)
-    bad = idx.copy()
+    bad = idx.copy().reshape(n, k)
     bad[5, 3] = n          # just past the end
     bad[77, 9] = 0xFFFFFFF0  # far past it
+    bad = bad.reshape(-1)
     lib = hm.lib()
     ws_bytes = lib.hm_fuzzy_workspace_bytes(n, k)
     dev = lambda a: torch.from_numpy(a.view(np.int32) if a.dtype == np.uint32 else a).cuda()
