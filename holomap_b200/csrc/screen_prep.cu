@@ -158,41 +158,55 @@ __global__ void __launch_bounds__(256) operand_kernel(const JobDev *__restrict__
         const size_t kp = G.kpmax;
         double uu = 0.0, ee = 0.0, rr = 0.0, aa = 0.0;
         const float *xr = J.x + (size_t)row * J.d;
-        for (uint32_t t = lane; t < J.kp1; t += 32) {
-            double u = 0.0;
-            if (t < J.d) {
-                u = (J.metric == HM_METRIC_EUCLIDEAN) ? ((double)xr[t] - J.mu[t]) * scale
-                                                      : (zero_row ? 0.0 : (double)xr[t] / J.rnorm[row]);
+        // cosine rows are scaled by 1 / ||x|| (the operand u is whatever this
+        // arithmetic forms: the band is measured from it)
+        const bool euc = J.metric == HM_METRIC_EUCLIDEAN;
+        const double mul = scale;
+        // the row's elements four at a time, their loads issued together
+        for (uint32_t t0 = 0; t0 < J.kp1; t0 += 128) {
+            float xs[4];
+            double ms[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t t = t0 + 32 * q + lane;
+                xs[q] = t < J.d ? xr[t] : 0.0f;
+                ms[q] = (euc && t < J.d) ? J.mu[t] : 0.0;
             }
-            uu += u * u;
-            if (G.kind == SCREEN_KIND_TF32) {
-                double r;
-                const uint32_t b = to_tf32_bits(u, &r);
-                reinterpret_cast<uint32_t *>(G.opa)[(size_t)gr * kp + t] = b;
-                ee += (r - u) * (r - u);
-                aa += r * r;
-            } else if (!G.split) {
-                double r;
-                const uint16_t b = to_bf16_bits(u, &r);
-                reinterpret_cast<uint16_t *>(G.opa)[(size_t)gr * kp + t] = b;
-                ee += (r - u) * (r - u);
-                aa += r * r;
-            } else {
-                double hi, lo;
-                const uint16_t bh = to_bf16_bits(u, &hi);
-                const uint16_t bl = to_bf16_bits(u - hi, &lo);
-                const double res = (u - hi) - lo;
-                uint16_t *A = reinterpret_cast<uint16_t *>(G.opa) + (size_t)gr * kp;
-                uint16_t *B = reinterpret_cast<uint16_t *>(G.opb) + (size_t)gr * kp;
-                A[t] = bh;
-                A[J.kp1 + t] = bh;
-                A[2 * J.kp1 + t] = bl;
-                B[t] = bh;
-                B[J.kp1 + t] = bl;
-                B[2 * J.kp1 + t] = bh;
-                ee += lo * lo;
-                rr += res * res;
-                aa += 2.0 * hi * hi + lo * lo;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t t = t0 + 32 * q + lane;
+                if (t >= J.kp1) break;
+                const double u = t < J.d ? (euc ? ((double)xs[q] - ms[q]) * mul : (double)xs[q] * mul) : 0.0;
+                uu += u * u;
+                if (G.kind == SCREEN_KIND_TF32) {
+                    double r;
+                    const uint32_t b = to_tf32_bits(u, &r);
+                    reinterpret_cast<uint32_t *>(G.opa)[(size_t)gr * kp + t] = b;
+                    ee += (r - u) * (r - u);
+                    aa += r * r;
+                } else if (!G.split) {
+                    double r;
+                    const uint16_t b = to_bf16_bits(u, &r);
+                    reinterpret_cast<uint16_t *>(G.opa)[(size_t)gr * kp + t] = b;
+                    ee += (r - u) * (r - u);
+                    aa += r * r;
+                } else {
+                    double hi, lo;
+                    const uint16_t bh = to_bf16_bits(u, &hi);
+                    const uint16_t bl = to_bf16_bits(u - hi, &lo);
+                    const double res = (u - hi) - lo;
+                    uint16_t *A = reinterpret_cast<uint16_t *>(G.opa) + (size_t)gr * kp;
+                    uint16_t *B = reinterpret_cast<uint16_t *>(G.opb) + (size_t)gr * kp;
+                    A[t] = bh;
+                    A[J.kp1 + t] = bh;
+                    A[2 * J.kp1 + t] = bl;
+                    B[t] = bh;
+                    B[J.kp1 + t] = bl;
+                    B[2 * J.kp1 + t] = bh;
+                    ee += lo * lo;
+                    rr += res * res;
+                    aa += 2.0 * hi * hi + lo * lo;
+                }
             }
         }
         uu = warp_sum(uu);
