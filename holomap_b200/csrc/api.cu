@@ -323,8 +323,7 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
             Gp.cand += P.spec.n * (uint64_t)P.elists * P.cap;
         }
         // emission units of the group: (job slot | sym, row block, first tile,
-        // end tile | part), the largest first so the persistent CTAs' static
-        // round-robin finishes together
+        // end tile | part)
         for (uint32_t gj = 0; gj < Gp.jobs.size(); ++gj) {
             const JobPlan &P = B.jobs[Gp.jobs[gj]];
             for (uint32_t r = 0; r < P.row_blocks; ++r) {
@@ -336,9 +335,12 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
                 }
             }
         }
-        std::stable_sort(Gp.eunits.begin(), Gp.eunits.end(), [](const uint4 &a, const uint4 &b) {
-            return (a.w & 0xffffffu) - a.z > (b.w & 0xffffffu) - b.z;
-        });
+        // symmetric units differ in size: the largest first, so the
+        // persistent CTAs' static round-robin finishes together
+        if (Gp.any_sym)
+            std::stable_sort(Gp.eunits.begin(), Gp.eunits.end(), [](const uint4 &a, const uint4 &b) {
+                return (a.w & 0xffffffu) - a.z > (b.w & 0xffffffu) - b.z;
+            });
         Gp.egrid = std::min<uint32_t>((uint32_t)Gp.eunits.size(), G);
         if (Gp.any_sym) {
             // column-side candidates staged per CTA: room for half of every
@@ -660,7 +662,7 @@ static int run_batch(hm_batch &B, cudaStream_t s) {
         // column lists the scatter fills start empty
         HM_CUDA_TRY(cudaMemsetAsync(Gp.host.cand_cnt, 0, Gp.elists * sizeof(uint32_t), s));
         if (Gp.any_sym) HM_TRY(launch_emit_limits(jobs, Gp.host, Gd, s));
-        HM_TRY(launch_screen_gemm(jobs, Gp.host, Gd, Gp.kp, Gp.ta, Gp.tb, nullptr, 1, s));
+        HM_TRY(launch_screen_gemm(jobs, Gp.host, Gd, Gp.kp, Gp.ta, Gp.tb, nullptr, Gp.any_sym ? 2 : 1, s));
         if (Gp.any_sym) HM_TRY(launch_column_scatter(jobs, Gp.host, Gd, Gp.egrid, s));
         HM_TRY(launch_rerank(jobs, Gp.host, Gd, Gp.kpl, Gp.dmax, Gp.metric_mask, s));
     }

@@ -100,7 +100,7 @@ constexpr int RR_ROWS = 8;        // group rows per warp of the exact phase
 constexpr int RR_WARPS = 4;       // warps per block of the exact phase
 constexpr int RR_CBUF = 512;      // emitted candidates a warp stages in shared memory
 constexpr int RS_WARPS = 8;       // rows (warps) per block of the select and top-k phases
-constexpr int RR_STAGES = 3;      // chunks in flight
+constexpr int RR_STAGES = 2;      // chunks in flight (11.5 KB of shared memory per warp)
 constexpr int RR_CH = 32;         // dimensions per chunk
 constexpr int RR_XJ_STRIDE = 36;  // floats per staged candidate chunk (144 B: 16-byte aligned rows
                                   // whose 16-byte reads by 32 lanes need the minimum 4 wavefronts)
@@ -426,16 +426,25 @@ __device__ __forceinline__ void exact_pairs(const JobDev &J, const GroupDev &G, 
         sm.ex.cj[lane] = j;
         __syncwarp();
 
+        // the rows this lane copies from, fixed for the slice: candidate
+        // 4 i + lane / 8 (16-byte pieces, vector path) and query row a
+        const uint32_t sub = (uint32_t)lane & 7u;
+        const float *cp[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) cp[i] = x + (size_t)sm.ex.cj[4 * i + ((uint32_t)lane >> 3)] * d + 4 * sub;
+        const float *qp[RR_QROWS];
+#pragma unroll
+        for (int a = 0; a < RR_QROWS; ++a)
+            qp[a] = x + (size_t)(gr0 + r_s + min((uint32_t)a, nr - 1) - J.row0) * d + lane;
+
         auto issue = [&](uint32_t c, uint32_t st) {
             const uint32_t dim0 = c * RR_CH;
             if (vec) {
-                const uint32_t sub = (uint32_t)lane & 7u, dp = dim0 + 4 * sub;
-                const uint32_t bytes = dp < d ? 16u : 0u;  // d % 4 == 0: a piece is all in or all out
+                const bool in = dim0 + 4 * sub < d;  // d % 4 == 0: a piece is all in or all out
 #pragma unroll
-                for (uint32_t i = 0; i < 8; ++i) {
+                for (int i = 0; i < 8; ++i) {
                     const uint32_t cand = 4 * i + ((uint32_t)lane >> 3);
-                    const float *src = x + (size_t)sm.ex.cj[cand] * d + (bytes ? dp : 0u);
-                    cp_async16(&sm.ex.xj[st][cand][4 * sub], src, bytes);
+                    cp_async16(&sm.ex.xj[st][cand][4 * sub], in ? cp[i] + dim0 : cp[i], in ? 16u : 0u);
                 }
             } else {
                 const uint32_t dp = dim0 + (uint32_t)lane;
@@ -445,23 +454,21 @@ __device__ __forceinline__ void exact_pairs(const JobDev &J, const GroupDev &G, 
                     cp_async4(&sm.ex.xj[st][cand][lane], src, bytes);
                 }
             }
-            const uint32_t dp = dim0 + (uint32_t)lane;
-            const uint32_t bytes = dp < d ? 4u : 0u;
-            for (uint32_t a = 0; a < nr; ++a) {
-                const uint32_t qrow = gr0 + r_s + a - J.row0;
-                cp_async4(&sm.ex.xi[st][a][lane], x + (size_t)qrow * d + (bytes ? dp : 0u), bytes);
-            }
+            const bool qin = dim0 + (uint32_t)lane < d;
+#pragma unroll
+            for (int a = 0; a < RR_QROWS; ++a)
+                if ((uint32_t)a < nr) cp_async4(&sm.ex.xi[st][a][lane], qin ? qp[a] + dim0 : qp[a] - lane, qin ? 4u : 0u);
         };
 
-        issue(0, 0);
-        cp_async_commit();
-        if (nch > 1) issue(1, 1);
-        cp_async_commit();
+        for (uint32_t c = 0; c + 1 < RR_STAGES; ++c) {
+            if (c < nch) issue(c, c);
+            cp_async_commit();
+        }
         double acc = 0.0;
         for (uint32_t c = 0; c < nch; ++c) {
-            if (c + 2 < nch) issue(c + 2, (c + 2) % RR_STAGES);
+            if (c + RR_STAGES - 1 < nch) issue(c + RR_STAGES - 1, (c + RR_STAGES - 1) % RR_STAGES);
             cp_async_commit();  // possibly empty: keeps the group count uniform
-            cp_async_wait<2>();
+            cp_async_wait<RR_STAGES - 1>();
             __syncwarp();
             const uint32_t st = c % RR_STAGES;
             for (uint32_t a = 0; a < nr; ++a) sm.ex.xid[a][lane] = (double)sm.ex.xi[st][a][lane];

@@ -18,7 +18,12 @@
 //      k-th of the union, tau1, an upper bound of the row's k-th screened value;
 //   1  emission pass over all columns with the fixed limit tau1 + band: 8-column
 //      group minima gate the per-column test, which writes every column within
-//      the limit into the row's list.
+//      the limit into the row's list;
+//   2  the emission pass of a group whose whole datasets take the symmetric
+//      form: a row block walks only the tiles from its diagonal on, with the
+//      limit tau1 + 2 band, and each value above the diagonal is also tested
+//      for its column's row (staged per CTA, moved to that row's column list
+//      by column_scatter_kernel).
 // Work units are (row block of 128, column part); the columns of a unit are
 // walked in 256-wide tiles with the two accumulators double buffered, so the
 // epilogue of one tile overlaps the MMAs of the next.
@@ -203,7 +208,7 @@ struct UnitTiles {
 // its units from the group's table.
 __device__ __forceinline__ UnitTiles unit_tiles(const JobDev *jobs, const GroupDev &G, uint32_t u, int pass) {
     UnitTiles t;
-    if (pass == 1) {
+    if (pass >= 1) {
         const uint4 e = G.eunits[u];
         t.job = G.job_ids[e.x & 0x7fffffffu];
         t.sym = e.x >> 31;
@@ -249,7 +254,10 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
     uint32_t *s_colcnt = tmem_slot + 2;  // column-side candidates this CTA staged
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t nunits = PASS == 1 ? G.neunits : G.units;
+    const uint32_t nunits = PASS >= 1 ? G.neunits : G.units;
+    // PASS 2 is the emission pass of a group with symmetric units (the
+    // column-side tests exist only in that instantiation)
+    constexpr bool SYMK = PASS == 2;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < SC_STAGES; ++s) {
@@ -433,17 +441,17 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
             // 2 band, precomputed; a pair's value may come from the tile of the
             // other orientation, within 2E of the threshold pass's value)
             float thr = -INF;
-            if (PASS == 1 && valid) thr = ut.sym ? G.ethr[gr] : __fadd_ru(unord32(G.rowthr[gr]), band);
+            if (PASS >= 1 && valid) thr = (SYMK && ut.sym) ? G.ethr[gr] : __fadd_ru(unord32(G.rowthr[gr]), band);
             // cosine fast path of pass 1: every v with fl(1 - v) <= thr has
             // v >= 1 - thr - ulp(thr)/2 >= vstar (2^-20 relative margin)
             const float vstar = !(thr < INF) ? -INF
                                              : __fsub_rd(__fsub_rd(1.0f, thr), fmaxf(fabsf(thr), 1.0f) * 0x1p-20f);
             uint32_t cnt = 0;
-            unsigned long long *cand = PASS == 1 ? cand_slots(J, G, list) : nullptr;
+            unsigned long long *cand = PASS >= 1 ? cand_slots(J, G, list) : nullptr;
             // symmetric: this row's own term in its pairs' column-side values
             // (c^_ji = rowterm_j + colterm_i - scale v) and the column-side
             // candidates this thread staged in the unit
-            const float own_ct = (PASS == 1 && ut.sym && valid) ? G.colterm[gr] : 0.0f;
+            const float own_ct = (SYMK && ut.sym && valid) ? G.colterm[gr] : 0.0f;
             uint32_t colsum = 0;
 
             for (uint32_t ct = ut.ct_begin; ct < ut.ct_end; ++ct, ++tile) {
@@ -453,13 +461,13 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                 // another unit's column side, above it they also serve the
                 // columns' rows
                 const uint32_t jb = 2 * ct + half;
-                const bool skip = PASS == 1 && ut.sym && jb < ut.rb;
-                const bool colside = PASS == 1 && ut.sym && jb > ut.rb && jb * (uint32_t)(SC_BN / 2) < n;
+                const bool skip = SYMK && ut.sym && jb < ut.rb;
+                const bool colside = SYMK && ut.sym && jb > ut.rb && jb * (uint32_t)(SC_BN / 2) < n;
                 const uint32_t c_base = ct * SC_BN + half * (SC_BN / 2);
                 // the columns' limits (lane t holds column c_base + 32 q + t),
                 // loaded while the accumulator is still being filled
                 float cthr[4] = {-INF, -INF, -INF, -INF}, cvs[4] = {INF, INF, INF, INF}, cterm[4] = {0, 0, 0, 0};
-                if (colside) {
+                if (SYMK && colside) {
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
                         const size_t gc = (size_t)J.row0 + c_base + 32 * q + lane;
@@ -528,7 +536,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                     // column j of the chunk takes this row as a candidate when
                     // c^_ji <= its limit (cosine without zero rows: the raw
                     // product against the column's v* form, a superset)
-                    if (PASS == 1 && colside) {
+                    if (SYMK && colside) {
                         const float cl_thr = ch == 0 ? cthr[0] : ch == 1 ? cthr[1] : ch == 2 ? cthr[2] : cthr[3];
                         const float cl_vs = ch == 0 ? cvs[0] : ch == 1 ? cvs[1] : ch == 2 ? cvs[2] : cvs[3];
                         const float cl_term = ch == 0 ? cterm[0] : ch == 1 ? cterm[1] : ch == 2 ? cterm[2] : cterm[3];
@@ -597,7 +605,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                     }
                     // cosine fast path: c = 1 - v is monotone in v, so a
                     // minimum of c is 1 - (the maximum of v), bit for bit
-                    const bool quick = fast_cos && full && !self_here && (PASS == 1 || !dump);
+                    const bool quick = fast_cos && full && !self_here && (PASS >= 1 || !dump);
                     if (PASS == 0) {
                         // mini-chunk minima: columns {t, t+8, t+16, t+24}
                         float m[8];
@@ -758,7 +766,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
                      "r"(SC_TMEM_COLS));
     }
-    if (PASS == 1 && threadIdx.x == 0 && G.stage_cnt) G.stage_cnt[blockIdx.x] = *s_colcnt;
+    if (SYMK && threadIdx.x == 0 && G.stage_cnt) G.stage_cnt[blockIdx.x] = *s_colcnt;
 }
 
 template <int KIND, int KP, int PASS>
@@ -766,7 +774,7 @@ static int launch_kind(const JobDev *jobs, const GroupDev &G, const CUtensorMap 
                        const CUtensorMap &tb, float *dump, uint32_t idesc, cudaStream_t s) {
     HM_TRY(ensure_dynamic_smem((const void *)screen_gemm_kernel<KIND, KP, PASS>, (int)SC_SMEM_BYTES));
     const uint32_t sms = (uint32_t)device_sm_count();
-    const uint32_t grid = PASS == 1 ? emission_grid(G) : (G.units < sms ? G.units : sms);
+    const uint32_t grid = PASS >= 1 ? emission_grid(G) : (G.units < sms ? G.units : sms);
     if (grid == 0) return HM_OK;
     // every job's K slices fit the resident A block
     const uint32_t a_res = (G.kpmax / G.kslice) <= SC_ARES_STAGES ? 1u : 0u;
@@ -794,13 +802,15 @@ template <int KIND>
 static int launch_pass(const JobDev *jobs, const GroupDev &G, uint32_t kp, const CUtensorMap &ta,
                        const CUtensorMap &tb, float *dump, uint32_t idesc, int pass, cudaStream_t s) {
     if (pass == 1) return launch_kind<KIND, 32, 1>(jobs, G, ta, tb, nullptr, idesc, s);
+    if (pass == 2) return launch_kind<KIND, 32, 2>(jobs, G, ta, tb, nullptr, idesc, s);
     if (kp == 32) return launch_kind<KIND, 32, 0>(jobs, G, ta, tb, dump, idesc, s);
     if (kp == 64) return launch_kind<KIND, 64, 0>(jobs, G, ta, tb, dump, idesc, s);
     return set_error(HM_ERR_UNSUPPORTED, "screen top-k width %u", kp);
 }
 
 // pass 0: each list's k smallest chunk minima over the column sample (-> tau1);
-// pass 1: emission of every column within tau1 + band
+// pass 1: emission of every column within tau1 + band; pass 2: the same for a
+// group with symmetric units (tiles on and above the diagonal, column side too)
 int launch_screen_gemm(const JobDev *jobs, const GroupDev &G, const GroupDev *, uint32_t kp,
                        const CUtensorMap &ta, const CUtensorMap &tb, float *dump, int pass,
                        cudaStream_t s) {
