@@ -7,9 +7,9 @@ launching stream, one full kNN + smooth-kNN run of
 
 * the plain exact binary64 path, and
 * each tensor-core screen (BF16, TF32, split-BF16) with the threshold pass
-  sampling 1/4, 1/8 and 1/16 of the columns and the symmetric emission pass
-  (tiles on and above the diagonal), and the fastest of those again with the
-  emission pass over every tile,
+  sampling 1/4, 1/8 and 1/16 of the columns (emission pass over every column
+  tile), and the fastest of those again with the symmetric emission pass
+  (tiles on and above the diagonal only),
 
 on seeded Gaussian-mixture data of that shape, checks that every screened
 result equals the plain path's bytes, and records the fastest choice.  Two
@@ -126,16 +126,16 @@ def sweep(grid_n=GRID_N, grid_d=GRID_D, grid_k=GRID_K, metrics=METRICS, verbose=
 
                     for path in SCREENS:
                         for sd in SEED_DIVS:
-                            times[f"{path}/{sd}/sym"] = measure(path, sd, 1)
+                            times[f"{path}/{sd}/full"] = measure(path, sd, 0)
                     screened = {c: t for c, t in times.items() if t is not None and c != "plain"}
                     if screened:
                         c0 = min(screened, key=screened.get)
                         p0, sd0, _ = c0.split("/")
-                        times[f"{p0}/{sd0}/full"] = measure(p0, int(sd0), 0)
+                        times[f"{p0}/{sd0}/sym"] = measure(p0, int(sd0), 1)
                     exact = all(t is not None for t in times.values())
                     valid = {c: t for c, t in times.items() if t is not None}
                     best = min(valid, key=valid.get)
-                    path, sd, form = (best.split("/") + ["8", "sym"])[:3]
+                    path, sd, form = (best.split("/") + ["8", "full"])[:3]
                     e = {"n": n, "d": d, "k": k, "metric": metric, "times_ms": times, "best": path,
                          "seed_div": int(sd), "symmetric": int(form == "sym"), "all_paths_equal_plain": exact}
                     entries.append(e)
