@@ -27,6 +27,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 from pathlib import Path
 
@@ -91,18 +92,63 @@ def workload(name, rows=None):
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """nvidia-smi samples every 200 ms during the timed region."""
+    """SM clock and clock-event reasons sampled every 5 ms during the timed
+    region by a host thread reading NVML (read-only queries); nvidia-smi at
+    its 200 ms period where NVML cannot be opened."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20,
+               "sw_power_cap": 0x4}
 
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.thread = None
+        self.samples = []
+        self.stop_flag = threading.Event()
+        self.nvml = None
+        self.handle = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.handle = self._handle(pynvml, gpu_index)
+        except Exception:  # no NVML: nvidia-smi below
+            self.nvml = None
+
+    @staticmethod
+    def _handle(pynvml, gpu_index):
+        """The NVML device behind CUDA device `gpu_index` (by PCI address, as
+        CUDA_VISIBLE_DEVICES may renumber devices)."""
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(gpu_index)
+            bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(gpu_index)
+
+    def _poll(self):
+        nv, h = self.nvml, self.handle
+        max_sm = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop_flag.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                power = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                self.samples.append((sm, max_sm, power, reasons))
+            except Exception:
+                pass
+            self.stop_flag.wait(0.005)
 
     def start(self):
+        if self.nvml is not None:
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
@@ -112,6 +158,16 @@ class ClockSampler:
             self.proc = None
 
     def stop(self) -> dict:
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            rows = self.samples
+            if not rows:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "source": "nvml"}
+            reasons = sorted({name for r in rows for name, bit in self.REASONS.items() if r[3] & bit})
+            return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                    "reasons": reasons, "samples": len(rows), "power_w_max": max(r[2] for r in rows),
+                    "source": "nvml, 5 ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -133,7 +189,8 @@ class ClockSampler:
         pw = [float(r[3]) for r in rows if r[3].strip().replace(".", "").isdigit()]
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(rows), "power_w_max": max(pw) if pw else None}
+                "samples": len(rows), "power_w_max": max(pw) if pw else None,
+                "source": "nvidia-smi, 200 ms"}
 
 
 # ---------------------------------------------------------- CPU baselines

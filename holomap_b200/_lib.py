@@ -204,6 +204,7 @@ SIGNATURES = {
     "hm_autotune_path": (_i32, [_u64, _u32, _u32, _i32]),
     "hm_tuning_override": (_i32, [_i32]),
     "hm_tuning_symmetric": (_i32, [_i32]),
+    "hm_tuning_pair": (_i32, [_i32]),
     "hm_timing_enable": (_i32, [_i32]),
     "hm_timing_read": (_i32, [_i32, _vp, _vp, _i32]),
     "hm_launch_count": (_u64, []),

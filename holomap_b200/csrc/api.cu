@@ -114,6 +114,7 @@ struct GroupPlan {
     uint64_t lists = 0, cand = 0, topk = 0, elists = 0;
     std::vector<uint4> eunits;  // emission units, largest first
     bool any_sym = false;
+    bool pair = false;  // emission pass in the 2-SM form (units of 256 rows)
     uint32_t egrid = 0, stage_cap = 0;
     size_t off_opa = 0, off_opb = 0, off_rowstat = 0, off_rowterm = 0, off_colterm = 0;
     size_t off_band = 0, off_force = 0, off_rowthr = 0, off_cand = 0, off_cnt = 0, off_topk = 0;
@@ -123,6 +124,7 @@ struct GroupPlan {
     size_t off_gdev = 0, off_job_ids = 0, off_row_starts = 0, off_unit_starts = 0, off_eunits = 0;
     GroupDev host{};
     CUtensorMap ta{}, tb{};
+    CUtensorMap tb_half{};  // 2-SM form: B in boxes of 128 rows (half a column tile)
 };
 
 }  // namespace hm
@@ -322,12 +324,17 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
             P.cand0 = Gp.cand;
             Gp.cand += P.spec.n * (uint64_t)P.elists * P.cap;
         }
-        // emission units of the group: (job slot | sym, row block, first tile,
-        // end tile | part)
+        // The emission pass takes the 2-SM form (a cluster of two CTAs per
+        // block of 256 rows, each loading half of every column tile) when no
+        // job is symmetric and every job's K slices fit the resident A block.
+        Gp.pair = tuning_pair() && !Gp.any_sym && Gp.kpmax / Gp.kslice <= SC_ARES_STAGES;
+        // emission units of the group: (job slot | sym, row block (2-SM form:
+        // block of 256 rows), first tile, end tile | part)
+        const uint32_t ubm = Gp.pair ? 2 * SC_BM : SC_BM;
         for (uint32_t gj = 0; gj < Gp.jobs.size(); ++gj) {
             const JobPlan &P = B.jobs[Gp.jobs[gj]];
-            for (uint32_t r = 0; r < P.row_blocks; ++r) {
-                const uint32_t rb = P.rb0 + r;
+            const uint32_t ub0 = P.q0 / ubm, ub1 = (P.q1 + ubm - 1) / ubm;
+            for (uint32_t rb = ub0; rb < ub1; ++rb) {
                 const uint32_t first = P.sym ? rb / 2 : 0u;
                 for (uint32_t part = 0, t0 = first; t0 < P.col_tiles; ++part, t0 += P.ept) {
                     const uint32_t t1 = std::min<uint32_t>(P.col_tiles, t0 + P.ept);
@@ -599,6 +606,7 @@ static int bind_batch(hm_batch &B, void *d_ws, size_t bytes, cudaStream_t s) {
         D.row_cnt = at<uint32_t>(ws, Gp.off_rowcnt);
         D.eunits = at<uint4>(ws, Gp.off_eunits);
         D.neunits = (uint32_t)Gp.eunits.size();
+        D.pair = Gp.pair ? 1u : 0u;
         if (Gp.any_sym) {
             D.ethr = at<float>(ws, Gp.off_ethr);
             D.evstar = at<float>(ws, Gp.off_evstar);
@@ -611,6 +619,8 @@ static int bind_batch(hm_batch &B, void *d_ws, size_t bytes, cudaStream_t s) {
         memcpy(host + Gp.off_gdev, &D, sizeof D);
         HM_TRY(make_operand_map(&Gp.ta, D.opa, Gp.rows, Gp.kpmax, Gp.elem_bytes, Gp.kslice, SC_BM));
         HM_TRY(make_operand_map(&Gp.tb, D.opb, Gp.rows, Gp.kpmax, Gp.elem_bytes, Gp.kslice, SC_BN));
+        if (Gp.pair)
+            HM_TRY(make_operand_map(&Gp.tb_half, D.opb, Gp.rows, Gp.kpmax, Gp.elem_bytes, Gp.kslice, SC_BM));
     }
 
     // written by kernels from their parameters, 3968 bytes per launch: no
@@ -662,7 +672,8 @@ static int run_batch(hm_batch &B, cudaStream_t s) {
         // column lists the scatter fills start empty
         HM_CUDA_TRY(cudaMemsetAsync(Gp.host.cand_cnt, 0, Gp.elists * sizeof(uint32_t), s));
         if (Gp.any_sym) HM_TRY(launch_emit_limits(jobs, Gp.host, Gd, s));
-        HM_TRY(launch_screen_gemm(jobs, Gp.host, Gd, Gp.kp, Gp.ta, Gp.tb, nullptr, Gp.any_sym ? 2 : 1, s));
+        HM_TRY(launch_screen_gemm(jobs, Gp.host, Gd, Gp.kp, Gp.ta, Gp.pair ? Gp.tb_half : Gp.tb, nullptr,
+                                  Gp.any_sym ? 2 : 1, s));
         if (Gp.any_sym) HM_TRY(launch_column_scatter(jobs, Gp.host, Gd, Gp.egrid, s));
         HM_TRY(launch_rerank(jobs, Gp.host, Gd, Gp.kpl, Gp.dmax, Gp.metric_mask, s));
     }

@@ -20,6 +20,7 @@ namespace hm {
 
 static thread_local uint32_t g_seed_override = 0;
 static thread_local bool g_symmetric = true;
+static thread_local bool g_pair = true;
 
 template <size_t N>
 static size_t nearest_ratio(const uint32_t (&grid)[N], double v) {
@@ -54,6 +55,8 @@ int autotune_choice(uint64_t n, uint32_t d, uint32_t k, int metric, uint32_t *se
     return (int)(e & 0xff);
 }
 
+bool tuning_pair() { return g_pair; }
+
 }  // namespace hm
 
 using namespace hm;
@@ -72,6 +75,11 @@ int hm_tuning_override(int seed_div) {
 
 int hm_tuning_symmetric(int on) {
     g_symmetric = on != 0;
+    return HM_OK;
+}
+
+int hm_tuning_pair(int on) {
+    g_pair = on != 0;
     return HM_OK;
 }
 

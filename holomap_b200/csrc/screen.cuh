@@ -37,6 +37,9 @@ constexpr int SC_BM = 128;
 constexpr int SC_BN = 256;
 constexpr int SC_SLICE_BYTES = 128;
 constexpr int SC_STAGES = 4;
+// K slices of the A block kept resident in shared memory for a whole unit
+// (96 KB: 6 slices of 128 B x 128 rows); deeper operands stream A with B
+constexpr uint32_t SC_ARES_STAGES = 6;
 constexpr int SC_EPI_WARPS = 8;  // two per TMEM lane quadrant, one per half tile
 constexpr int SC_THREADS = 64 + 32 * SC_EPI_WARPS;  // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
 
@@ -78,6 +81,9 @@ struct GroupDev {
     // largest first
     const uint4 *eunits;
     uint32_t neunits;
+    // emission pass in the 2-SM form (a cluster of two CTAs per unit, one
+    // MMA of 256 rows; eunits' y is then a block of 256 rows)
+    uint32_t pair;
     // symmetric emission: per group row (padded like colterm) the emission
     // limit tau1 + 2 band and its cosine raw-product form; the column-side
     // candidates each CTA staged (group row of the column, raw product bits

@@ -31,6 +31,8 @@
 // Every wait on an mbarrier is bounded (wall clock via %globaltimer and an
 // iteration cap): on expiry the CTA records an error code, stops issuing,
 // waits (bounded) for its own copies and MMAs, frees TMEM and returns.
+#include <atomic>
+
 #include <cuda.h>
 #include <cuda_runtime.h>
 
@@ -41,12 +43,14 @@ namespace hm {
 
 constexpr uint32_t SC_A_BYTES = SC_BM * SC_SLICE_BYTES;  // 16 KB
 constexpr uint32_t SC_B_BYTES = SC_BN * SC_SLICE_BYTES;  // 32 KB
-// A block kept in shared memory for a whole unit when its K slices fit
-// (96 KB: 6 slices of 128 B x 128 rows); otherwise A streams with B.
-constexpr uint32_t SC_ARES_STAGES = 6;
 constexpr uint32_t SC_OPND_BYTES = SC_ARES_STAGES * SC_A_BYTES + SC_STAGES * SC_B_BYTES;  // 224 KB
 constexpr uint32_t SC_SMEM_BYTES = 1024 + SC_OPND_BYTES + 256;
 constexpr uint32_t SC_TMEM_COLS = 512;
+// 2-SM form: each CTA holds half of the 256-row B tile, 16 KB per K slice,
+// in 8 stages (the same 128 KB as 4 stages of whole tiles)
+constexpr uint32_t SC_B2_BYTES = (SC_BN / 2) * SC_SLICE_BYTES;
+constexpr uint32_t SC_STAGES2 = 8;
+constexpr uint32_t SC_MAXST = SC_STAGES2;
 constexpr uint64_t SC_WAIT_LIMIT_NS = 4000000000ull;  // 4 s
 constexpr uint64_t SC_DRAIN_LIMIT_NS = 200000000ull;  // 0.2 s for copies already in flight
 constexpr uint32_t SC_WAIT_SPIN_CAP = 1u << 30;
@@ -121,6 +125,43 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map
         : "memory");
 }
 
+// The 2-SM form (a cluster of two CTAs sharing each MMA): both CTAs' loads
+// complete on the leader's (rank 0's) barrier, whose cluster address is the
+// local one with the rank bit (bit 24) cleared.
+// 2-SM copy: the bytes land in this CTA's shared memory and complete on the
+// barrier at `leader_bar` (a shared::cluster address in the pair's leader)
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap *map, uint32_t leader_bar,
+                                                 int32_t x, int32_t y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(leader_bar)
+        : "memory");
+}
+
+// arrive on a barrier given by its shared::cluster address
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cluster.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// the shared::cluster address of a shared-memory word of this CTA in CTA `rank`
+__device__ __forceinline__ uint32_t cluster_addr(uint32_t local, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+
 __device__ __forceinline__ void fence_before_sync() {
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 }
@@ -138,9 +179,24 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
            | ((uint64_t)2 << 61);             // swizzle mode: 128B
 }
 
-template <int KIND>
+template <int KIND, bool PAIR = false>
 __device__ __forceinline__ void mma_issue(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc,
                                           uint32_t idesc, uint32_t accum) {
+    if (PAIR) {
+        if (KIND == SCREEN_KIND_BF16)
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+                "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
+                : "memory");
+        else
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::2.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+                "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
+                : "memory");
+        return;
+    }
     if (KIND == SCREEN_KIND_BF16) {
         asm volatile(
             "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
@@ -156,10 +212,16 @@ __device__ __forceinline__ void mma_issue(uint32_t d_tmem, uint64_t adesc, uint6
     }
 }
 
+template <bool PAIR = false>
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                     bar)
-                 : "memory");
+    if (PAIR)  // the barrier at this offset in both CTAs of the pair
+        asm volatile(
+            "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::
+                "r"(bar), "h"((uint16_t)3)
+            : "memory");
+    else
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                     : "memory");
 }
 
 // tcgen05.ld of 32 consecutive accumulator columns of this warp's 32 lanes;
@@ -193,8 +255,10 @@ __device__ __forceinline__ void tmem_ld_wait(uint32_t (&v)[32]) {
 
 
 __device__ __forceinline__ void raise_error(volatile uint32_t *abort_flag, uint32_t *error_code,
-                                            uint32_t code) {
+                                            uint32_t code, uint32_t peer_abort = 0) {
     *abort_flag = 1;
+    if (peer_abort)  // the other CTA of a pair stops waiting too
+        asm volatile("st.shared::cluster.u32 [%0], %1;" ::"r"(peer_abort), "r"(1u) : "memory");
     atomicCAS(error_code, 0u, code);
 }
 
@@ -230,7 +294,7 @@ __device__ __forceinline__ UnitTiles unit_tiles(const JobDev *jobs, const GroupD
     return t;
 }
 
-template <int KIND, int KP, int PASS>
+template <int KIND, int KP, int PASS, bool PAIR>
 __global__ void __launch_bounds__(SC_THREADS, 1)
     screen_gemm_kernel(const __grid_constant__ CUtensorMap tma, const __grid_constant__ CUtensorMap tmb,
                        const JobDev *__restrict__ jobs, const GroupDev G, float *dump, uint32_t idesc,
@@ -240,12 +304,15 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                                                 ~(uintptr_t)1023);
     // streaming: stage s holds A at sA + s * 16 KB and B at sB + s * 32 KB;
     // resident A: the unit's A slices at smem + ks * 16 KB, B stages after them
+    // 2-SM form (a_res always): the A block resident, B half-tile stages
     uint8_t *sA = smem;
-    uint8_t *sB = a_res ? smem + SC_ARES_STAGES * SC_A_BYTES : smem + SC_STAGES * SC_A_BYTES;
+    uint8_t *sB = (PAIR || a_res) ? smem + SC_ARES_STAGES * SC_A_BYTES : smem + SC_STAGES * SC_A_BYTES;
+    constexpr uint32_t NST = PAIR ? SC_STAGES2 : SC_STAGES;  // B stages
+    constexpr uint32_t BST = PAIR ? SC_B2_BYTES : SC_B_BYTES;  // bytes of one B stage
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + SC_OPND_BYTES);
-    uint64_t *full = bars;                  // [SC_STAGES]
-    uint64_t *empty = bars + SC_STAGES;     // [SC_STAGES]
-    uint64_t *accf = bars + 2 * SC_STAGES;  // [2]
+    uint64_t *full = bars;                  // [NST]
+    uint64_t *empty = bars + SC_MAXST;      // [NST]
+    uint64_t *accf = bars + 2 * SC_MAXST;   // [2]
     uint64_t *acce = accf + 2;              // [2]
     uint64_t *afull = acce + 2;             // resident A loaded
     uint64_t *aempty = afull + 1;           // resident A consumed by the unit's MMAs
@@ -255,18 +322,25 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t nunits = PASS >= 1 ? G.neunits : G.units;
+    // 2-SM form: a cluster of two CTAs works on a unit of 256 rows (rank r
+    // owns the 128-row block 2 rb + r); rank 0 (the leader) issues the MMAs
+    const uint32_t rank = PAIR ? cluster_rank() : 0u;
+    const bool leader = rank == 0;
+    const uint32_t wid = PAIR ? blockIdx.x >> 1 : blockIdx.x;
+    const uint32_t nworkers = PAIR ? gridDim.x >> 1 : gridDim.x;
     // PASS 2 is the emission pass of a group with symmetric units (the
     // column-side tests exist only in that instantiation)
     constexpr bool SYMK = PASS == 2;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < SC_STAGES; ++s) {
+        for (uint32_t s = 0; s < NST; ++s) {
             mbar_init(smem_u32(&full[s]), 1);
             mbar_init(smem_u32(&empty[s]), 1);
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(smem_u32(&accf[b]), 1);
-            mbar_init(smem_u32(&acce[b]), SC_EPI_WARPS);
+            // the leader's accumulator is released by both CTAs' epilogues
+            mbar_init(smem_u32(&acce[b]), PAIR ? 2 * SC_EPI_WARPS : SC_EPI_WARPS);
         }
         mbar_init(smem_u32(afull), 1);
         mbar_init(smem_u32(aempty), 1);
@@ -275,15 +349,24 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 1) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
-                         smem_u32(tmem_slot)),
-                     "r"(SC_TMEM_COLS));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        if (PAIR) {
+            asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                             smem_u32(tmem_slot)),
+                         "r"(SC_TMEM_COLS));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;");
+        } else {
+            asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                             smem_u32(tmem_slot)),
+                         "r"(SC_TMEM_COLS));
+            asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+        }
     }
     fence_before_sync();
     __syncthreads();
+    if (PAIR) cluster_sync();  // both CTAs' barriers exist before either signals the other's
     fence_after_sync();
     const uint32_t tmem_base = *tmem_slot;
+    const uint32_t peer_abort = PAIR ? cluster_addr(smem_u32((const void *)abort_flag), rank ^ 1u) : 0u;
 
     if (warp == 0) {
         // ------------------------------------------------------ TMA producer
@@ -291,68 +374,97 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
             uint32_t it = 0, un = 0;
             bool ok = true;
             constexpr uint32_t kelems = SC_SLICE_BYTES / (KIND == SCREEN_KIND_BF16 ? 2 : 4);
-            for (uint32_t u = blockIdx.x; ok && u < nunits; u += gridDim.x) {
+            for (uint32_t u = wid; ok && u < nunits; u += nworkers) {
                 const UnitTiles ut = unit_tiles(jobs, G, u, PASS);
                 const JobDev &J = jobs[ut.job];
-                if (a_res) {
+                const uint32_t myrb = PAIR ? 2 * ut.rb + rank : ut.rb;  // this CTA's 128-row block
+                if (PAIR || a_res) {
                     // the previous unit's MMAs must be done with the A block
                     if (un > 0 && !mbar_wait(smem_u32(aempty), (un - 1) & 1, abort_flag)) {
-                        raise_error(abort_flag, &J.cnt->error_code, SC_ERR_PRODUCER);
+                        raise_error(abort_flag, &J.cnt->error_code, SC_ERR_PRODUCER, peer_abort);
                         ok = false;
                         break;
                     }
                     const uint32_t fb = smem_u32(afull);
-                    mbar_arrive_expect_tx(fb, J.k_stages * SC_A_BYTES);
-                    for (uint32_t ks = 0; ks < J.k_stages; ++ks)
-                        tma_load_2d(smem_u32(sA + ks * SC_A_BYTES), &tma, fb, (int32_t)(ks * kelems),
-                                    (int32_t)(J.row0 + ut.rb * SC_BM));
+                    if (!PAIR || leader) mbar_arrive_expect_tx(fb, (PAIR ? 2u : 1u) * J.k_stages * SC_A_BYTES);
+                    for (uint32_t ks = 0; ks < J.k_stages; ++ks) {
+                        if (PAIR)
+                            tma_load_2d_pair(smem_u32(sA + ks * SC_A_BYTES), &tma, cluster_addr(fb, 0), (int32_t)(ks * kelems),
+                                             (int32_t)(J.row0 + myrb * SC_BM));
+                        else
+                            tma_load_2d(smem_u32(sA + ks * SC_A_BYTES), &tma, fb, (int32_t)(ks * kelems),
+                                        (int32_t)(J.row0 + myrb * SC_BM));
+                    }
                     ++un;
                 }
                 for (uint32_t ct = ut.ct_begin; ok && ct < ut.ct_end; ++ct) {
                     for (uint32_t ks = 0; ks < J.k_stages; ++ks, ++it) {
-                        const uint32_t s = it % SC_STAGES, r = it / SC_STAGES;
+                        const uint32_t s = it % NST, r = it / NST;
                         if (!mbar_wait(smem_u32(&empty[s]), (r & 1) ^ 1, abort_flag)) {
-                            raise_error(abort_flag, &J.cnt->error_code, SC_ERR_PRODUCER);
+                            raise_error(abort_flag, &J.cnt->error_code, SC_ERR_PRODUCER, peer_abort);
                             ok = false;
                             break;
                         }
                         const uint32_t fb = smem_u32(&full[s]);
                         const int32_t kx = (int32_t)(ks * kelems);
-                        if (a_res) {
-                            mbar_arrive_expect_tx(fb, SC_B_BYTES);
+                        if (PAIR) {
+                            // both halves of the B tile complete on the leader's barrier
+                            if (leader) mbar_arrive_expect_tx(fb, 2 * SC_B2_BYTES);
+                            tma_load_2d_pair(smem_u32(sB + s * BST), &tmb, cluster_addr(fb, 0), kx,
+                                             (int32_t)(J.row0 + ct * SC_BN + rank * (SC_BN / 2)));
                         } else {
-                            mbar_arrive_expect_tx(fb, SC_A_BYTES + SC_B_BYTES);
-                            tma_load_2d(smem_u32(sA + s * SC_A_BYTES), &tma, fb, kx, (int32_t)(J.row0 + ut.rb * SC_BM));
+                            if (a_res) {
+                                mbar_arrive_expect_tx(fb, SC_B_BYTES);
+                            } else {
+                                mbar_arrive_expect_tx(fb, SC_A_BYTES + SC_B_BYTES);
+                                tma_load_2d(smem_u32(sA + s * SC_A_BYTES), &tma, fb, kx, (int32_t)(J.row0 + myrb * SC_BM));
+                            }
+                            tma_load_2d(smem_u32(sB + s * SC_B_BYTES), &tmb, fb, kx, (int32_t)(J.row0 + ct * SC_BN));
                         }
-                        tma_load_2d(smem_u32(sB + s * SC_B_BYTES), &tmb, fb, kx, (int32_t)(J.row0 + ct * SC_BN));
                     }
                 }
             }
-            // drain: the last A block must have landed before the CTA exits
-            if (a_res && un > 0 && !mbar_wait(smem_u32(afull), (un - 1) & 1, abort_flag, true))
-                raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN);
-            // drain: every issued stage must have landed before the CTA exits
-            const uint32_t issued = it;
-            for (uint32_t t = issued > SC_STAGES ? issued - SC_STAGES : 0; t < issued; ++t) {
-                const uint32_t s = t % SC_STAGES, r = t / SC_STAGES;
-                if (!mbar_wait(smem_u32(&full[s]), r & 1, abort_flag, true)) {
-                    raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN);
-                    break;
+            if (PAIR) {
+                // drain: the leader's MMAs have consumed (so both CTAs' copies
+                // have landed in) every issued stage and A block
+                const uint32_t issued = it;
+                for (uint32_t t = issued > NST ? issued - NST : 0; t < issued; ++t) {
+                    const uint32_t s = t % NST, r = t / NST;
+                    if (!mbar_wait(smem_u32(&empty[s]), r & 1, abort_flag, true)) {
+                        raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN, peer_abort);
+                        break;
+                    }
+                }
+                if (un > 0 && !mbar_wait(smem_u32(aempty), (un - 1) & 1, abort_flag, true))
+                    raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN, peer_abort);
+            } else {
+                // drain: the last A block must have landed before the CTA exits
+                if (a_res && un > 0 && !mbar_wait(smem_u32(afull), (un - 1) & 1, abort_flag, true))
+                    raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN, peer_abort);
+                // drain: every issued stage must have landed before the CTA exits
+                const uint32_t issued = it;
+                for (uint32_t t = issued > NST ? issued - NST : 0; t < issued; ++t) {
+                    const uint32_t s = t % NST, r = t / NST;
+                    if (!mbar_wait(smem_u32(&full[s]), r & 1, abort_flag, true)) {
+                        raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN, peer_abort);
+                        break;
+                    }
                 }
             }
         }
         __syncwarp();
     } else if (warp == 1) {
         // ------------------------------------------------------- MMA issuer
-        if (lane == 0) {
+        // (2-SM form: the leader's alone, for both CTAs)
+        if (lane == 0 && (!PAIR || leader)) {
             uint32_t it = 0, tile = 0, un = 0;
             bool ok = true;
-            for (uint32_t u = blockIdx.x; ok && u < nunits; u += gridDim.x) {
+            for (uint32_t u = wid; ok && u < nunits; u += nworkers) {
                 const UnitTiles ut = unit_tiles(jobs, G, u, PASS);
                 const JobDev &J = jobs[ut.job];
-                if (a_res) {
+                if (PAIR || a_res) {
                     if (!mbar_wait(smem_u32(afull), un & 1, abort_flag)) {
-                        raise_error(abort_flag, &J.cnt->error_code, SC_ERR_MMA_FULL);
+                        raise_error(abort_flag, &J.cnt->error_code, SC_ERR_MMA_FULL, peer_abort);
                         ok = false;
                         break;
                     }
@@ -361,44 +473,44 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                 for (uint32_t ct = ut.ct_begin; ok && ct < ut.ct_end; ++ct, ++tile) {
                     const uint32_t buf = tile & 1, use = tile >> 1;
                     if (!mbar_wait(smem_u32(&acce[buf]), (use & 1) ^ 1, abort_flag)) {
-                        raise_error(abort_flag, &J.cnt->error_code, SC_ERR_MMA_ACC);
+                        raise_error(abort_flag, &J.cnt->error_code, SC_ERR_MMA_ACC, peer_abort);
                         ok = false;
                         break;
                     }
                     fence_after_sync();
                     const uint32_t d_tmem = tmem_base + buf * SC_BN;
                     for (uint32_t ks = 0; ks < J.k_stages; ++ks, ++it) {
-                        const uint32_t s = it % SC_STAGES, r = it / SC_STAGES;
+                        const uint32_t s = it % NST, r = it / NST;
                         if (!mbar_wait(smem_u32(&full[s]), r & 1, abort_flag)) {
-                            raise_error(abort_flag, &J.cnt->error_code, SC_ERR_MMA_FULL);
+                            raise_error(abort_flag, &J.cnt->error_code, SC_ERR_MMA_FULL, peer_abort);
                             ok = false;
                             break;
                         }
                         fence_after_sync();
-                        const uint32_t a0 = smem_u32(sA + (a_res ? ks : s) * SC_A_BYTES);
-                        const uint32_t b0 = smem_u32(sB + s * SC_B_BYTES);
+                        const uint32_t a0 = smem_u32(sA + ((PAIR || a_res) ? ks : s) * SC_A_BYTES);
+                        const uint32_t b0 = smem_u32(sB + s * BST);
 #pragma unroll
                         for (uint32_t kk = 0; kk < SC_SLICE_BYTES / 32; ++kk)
-                            mma_issue<KIND>(d_tmem, smem_desc(a0 + kk * 32), smem_desc(b0 + kk * 32),
-                                            idesc, (ks | kk) != 0);
-                        mma_commit(smem_u32(&empty[s]));
+                            mma_issue<KIND, PAIR>(d_tmem, smem_desc(a0 + kk * 32), smem_desc(b0 + kk * 32),
+                                                  idesc, (ks | kk) != 0);
+                        mma_commit<PAIR>(smem_u32(&empty[s]));
                     }
                     if (!ok) break;
-                    mma_commit(smem_u32(&accf[buf]));
+                    mma_commit<PAIR>(smem_u32(&accf[buf]));
                 }
-                if (ok && a_res) {
-                    mma_commit(smem_u32(aempty));  // the A block is free once these MMAs finish
+                if (ok && (PAIR || a_res)) {
+                    mma_commit<PAIR>(smem_u32(aempty));  // the A block is free once these MMAs finish
                     ++un;
                 }
             }
             // drain: the last commits must have landed before TMEM is freed
             if (it > 0) {
-                const uint32_t s = (it - 1) % SC_STAGES, r = (it - 1) / SC_STAGES;
+                const uint32_t s = (it - 1) % NST, r = (it - 1) / NST;
                 if (!mbar_wait(smem_u32(&empty[s]), r & 1, abort_flag, true))
-                    raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN);
+                    raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN, peer_abort);
             }
-            if (a_res && un > 0 && !mbar_wait(smem_u32(aempty), (un - 1) & 1, abort_flag, true))
-                raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN);
+            if ((PAIR || a_res) && un > 0 && !mbar_wait(smem_u32(aempty), (un - 1) & 1, abort_flag, true))
+                raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN, peer_abort);
         }
         __syncwarp();
     } else {
@@ -411,11 +523,12 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         const float INF = __int_as_float(0x7f800000);
         uint32_t tile = 0;
         bool ok = true;
-        for (uint32_t u = blockIdx.x; ok && u < nunits; u += gridDim.x) {
+        for (uint32_t u = wid; ok && u < nunits; u += nworkers) {
             const UnitTiles ut = unit_tiles(jobs, G, u, PASS);
             const JobDev &J = jobs[ut.job];
             const uint32_t n = J.n;
-            const uint32_t row = ut.rb * SC_BM + row_in_tile;  // job-local
+            const uint32_t myrb = PAIR ? 2 * ut.rb + rank : ut.rb;  // this CTA's 128-row block
+            const uint32_t row = myrb * SC_BM + row_in_tile;  // job-local
             const bool valid = row >= J.q0 && row < J.q1;
             const size_t gr = (size_t)J.row0 + row;              // group row
             // cosine rows compare 1 - v directly (every column term is 1 when
@@ -461,8 +574,8 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                 // another unit's column side, above it they also serve the
                 // columns' rows
                 const uint32_t jb = 2 * ct + half;
-                const bool skip = SYMK && ut.sym && jb < ut.rb;
-                const bool colside = SYMK && ut.sym && jb > ut.rb && jb * (uint32_t)(SC_BN / 2) < n;
+                const bool skip = SYMK && ut.sym && jb < myrb;
+                const bool colside = SYMK && ut.sym && jb > myrb && jb * (uint32_t)(SC_BN / 2) < n;
                 const uint32_t c_base = ct * SC_BN + half * (SC_BN / 2);
                 // the columns' limits (lane t holds column c_base + 32 q + t),
                 // loaded while the accumulator is still being filled
@@ -478,14 +591,19 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                 }
                 const bool got = mbar_wait(smem_u32(&accf[buf]), use & 1, abort_flag);
                 if (!__all_sync(0xffffffffu, got)) {
-                    raise_error(abort_flag, &J.cnt->error_code, SC_ERR_EPILOGUE);
+                    raise_error(abort_flag, &J.cnt->error_code, SC_ERR_EPILOGUE, peer_abort);
                     ok = false;
                     break;
                 }
                 fence_after_sync();
                 if (skip) {
                     __syncwarp();
-                    if (lane == 0) mbar_arrive(smem_u32(&acce[buf]));
+                    if (lane == 0) {
+                        if (PAIR)
+                            mbar_arrive_cluster(cluster_addr(smem_u32(&acce[buf]), 0));
+                        else
+                            mbar_arrive(smem_u32(&acce[buf]));
+                    }
                     continue;
                 }
                 if (PASS == 0 && valid) {
@@ -494,7 +612,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                     tglob = fminf(tglob, unord32(tnext));
                     tnext = *(volatile const uint32_t *)(G.rowthr + gr);
                 }
-                const bool diag = (ct * SC_BN < ut.rb * SC_BM + SC_BM) && (ut.rb * SC_BM < ct * SC_BN + SC_BN);
+                const bool diag = (ct * SC_BN < myrb * SC_BM + SC_BM) && (myrb * SC_BM < ct * SC_BN + SC_BN);
                 const uint32_t t_base = tmem_base + ((quad * 32) << 16) + buf * SC_BN + half * (SC_BN / 2);
                 // one chunk = 32 columns; the accumulator registers are
                 // overwritten in place by the screened values
@@ -740,7 +858,12 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                 }
                 fence_before_sync();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(smem_u32(&acce[buf]));
+                if (lane == 0) {
+                    if (PAIR)
+                        mbar_arrive_cluster(cluster_addr(smem_u32(&acce[buf]), 0));
+                    else
+                        mbar_arrive(smem_u32(&acce[buf]));
+                }
             }
             if (!ok) break;
             if (PASS == 0) {
@@ -761,25 +884,91 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
 
     fence_before_sync();
     __syncthreads();
+    if (PAIR) cluster_sync();  // neither CTA leaves while the other may still signal it
     if (warp == 1) {
         fence_after_sync();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
-                     "r"(SC_TMEM_COLS));
+        if (PAIR)
+            asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                         "r"(SC_TMEM_COLS));
+        else
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
+                         "r"(SC_TMEM_COLS));
     }
     if (SYMK && threadIdx.x == 0 && G.stage_cnt) G.stage_cnt[blockIdx.x] = *s_colcnt;
+}
+
+// clusters of two screen CTAs the device can hold at once (per device,
+// computed on first use; 0 until then)
+static uint32_t pair_slots(const void *func) {
+    static std::atomic<int> cache[64];  // clusters + 1
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
+    const int hit = cache[dev].load(std::memory_order_relaxed);
+    if (hit > 0) return (uint32_t)(hit - 1);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * (uint32_t)device_sm_count(), 1, 1);
+    cfg.blockDim = dim3(SC_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = SC_SMEM_BYTES;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = 2;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    if (cudaOccupancyMaxActiveClusters(&clusters, func, &cfg) != cudaSuccess || clusters < 1) {
+        (void)cudaGetLastError();
+        return 0;
+    }
+    cache[dev].store(clusters + 1, std::memory_order_relaxed);
+    return (uint32_t)clusters;
+}
+
+// the emission pass in the 2-SM form: clusters of two, the A block resident
+// in each CTA, one MMA of M = 256 per K step
+template <int KIND>
+static int launch_pair(const JobDev *jobs, const GroupDev &G, const CUtensorMap &ta, const CUtensorMap &tb,
+                       uint32_t idesc, cudaStream_t s) {
+    const void *func = (const void *)screen_gemm_kernel<KIND, 32, 1, true>;
+    HM_TRY(ensure_dynamic_smem(func, (int)SC_SMEM_BYTES));
+    const uint32_t slots = pair_slots(func);
+    if (slots == 0) return set_error(HM_ERR_CUDA, "no room for a cluster of two screen CTAs");
+    const uint32_t clusters = G.neunits < slots ? G.neunits : slots;
+    if (clusters == 0) return HM_OK;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * clusters, 1, 1);
+    cfg.blockDim = dim3(SC_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = SC_SMEM_BYTES;
+    cfg.stream = s;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeClusterDimension;
+    attr.val.clusterDim.x = 2;
+    attr.val.clusterDim.y = 1;
+    attr.val.clusterDim.z = 1;
+    cfg.attrs = &attr;
+    cfg.numAttrs = 1;
+    const uint32_t pidesc = (idesc & ~(0x1fu << 24)) | (((uint32_t)(2 * SC_BM) >> 4) << 24);  // M = 256
+    HM_CUDA_TRY(cudaLaunchKernelEx(&cfg, screen_gemm_kernel<KIND, 32, 1, true>, ta, tb, jobs, G,
+                                   (float *)nullptr, pidesc, 1u));
+    count_launch();
+    return HM_OK;
 }
 
 template <int KIND, int KP, int PASS>
 static int launch_kind(const JobDev *jobs, const GroupDev &G, const CUtensorMap &ta,
                        const CUtensorMap &tb, float *dump, uint32_t idesc, cudaStream_t s) {
-    HM_TRY(ensure_dynamic_smem((const void *)screen_gemm_kernel<KIND, KP, PASS>, (int)SC_SMEM_BYTES));
+    if constexpr (PASS == 1 && KP == 32) {
+        if (G.pair) return launch_pair<KIND>(jobs, G, ta, tb, idesc, s);
+    }
+    HM_TRY(ensure_dynamic_smem((const void *)screen_gemm_kernel<KIND, KP, PASS, false>, (int)SC_SMEM_BYTES));
     const uint32_t sms = (uint32_t)device_sm_count();
     const uint32_t grid = PASS >= 1 ? emission_grid(G) : (G.units < sms ? G.units : sms);
     if (grid == 0) return HM_OK;
     // every job's K slices fit the resident A block
     const uint32_t a_res = (G.kpmax / G.kslice) <= SC_ARES_STAGES ? 1u : 0u;
-    screen_gemm_kernel<KIND, KP, PASS><<<grid, SC_THREADS, SC_SMEM_BYTES, s>>>(ta, tb, jobs, G, dump, idesc,
-                                                                               a_res);
+    screen_gemm_kernel<KIND, KP, PASS, false><<<grid, SC_THREADS, SC_SMEM_BYTES, s>>>(ta, tb, jobs, G, dump,
+                                                                                      idesc, a_res);
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();
     return HM_OK;

@@ -398,6 +398,12 @@ HM_API int hm_tuning_override(int seed_div);
  * rows only).  Same results; on = 1 (the default) restores the symmetric
  * form. */
 HM_API int hm_tuning_symmetric(int on);
+/* Sweep and test hook (no reference counterpart): with on = 0, screened plans
+ * made on this thread run the emission pass with one CTA per 128-row block
+ * instead of the 2-SM form (a cluster of two CTAs sharing one 256-row MMA,
+ * each CTA loading half of every column tile).  Same results; on = 1 (the
+ * default) restores the 2-SM form where a group can take it. */
+HM_API int hm_tuning_pair(int on);
 
 /* ----------------------------------------------------------------------------
  * Instrumentation (no reference counterpart; the reference has no timers on

@@ -152,3 +152,27 @@ def test_full_and_symmetric_emission_agree_with_the_oracle(oracle, path, metric)
         assert_same_bytes(knn.dists, od, f"sym={sym} dists")
         assert_same_bytes(sm.sigmas, osig, f"sym={sym} sigma")
         assert_same_bytes(sm.rhos, orho, f"sym={sym} rho")
+
+
+@pytest.mark.parametrize("path", PATHS)
+@pytest.mark.parametrize("n", [200, 1000, 2600])
+def test_pair_and_single_cta_emission_agree_with_the_oracle(oracle, path, n):
+    """The emission pass in the 2-SM form (the default: a cluster of two CTAs
+    shares one 256-row MMA, each loading half of every column tile) and with
+    one CTA per 128-row block (hm_tuning_pair(0)) return the oracle's bytes,
+    including a last 256-row block that ends inside its first half (n = 200,
+    1000) and one whose second half lies past every row (n = 2600)."""
+    lib = hm.lib()
+    x = edge_case("duplicates", n, 40, seed=n)
+    oi, od = oracle.exact_knn(x, 15, "euclidean")
+    osig, orho = oracle.smooth_knn(od, 15)
+    for pair in (0, 1):
+        assert lib.hm_tuning_pair(pair) == 0
+        try:
+            knn, sm = hm.knn_smooth(x, 40, 15, "euclidean", path)
+        finally:
+            lib.hm_tuning_pair(1)
+        assert_same_bytes(knn.indices, oi, f"pair={pair} indices")
+        assert_same_bytes(knn.dists, od, f"pair={pair} dists")
+        assert_same_bytes(sm.sigmas, osig, f"pair={pair} sigma")
+        assert_same_bytes(sm.rhos, orho, f"pair={pair} rho")
