@@ -8,8 +8,9 @@ launching stream, one full kNN + smooth-kNN run of
 * the plain exact binary64 path, and
 * each tensor-core screen (BF16, TF32, split-BF16) with the threshold pass
   sampling 1/4, 1/8 and 1/16 of the columns (emission pass over every column
-  tile), and the fastest of those again with the symmetric emission pass
-  (tiles on and above the diagonal only),
+  tile, in the 2-SM form where it applies), and the fastest of those again
+  with one CTA per 128-row block instead of the 2-SM form and with the
+  symmetric emission pass (tiles on and above the diagonal only),
 
 on seeded Gaussian-mixture data of that shape, checks that every screened
 result equals the plain path's bytes, and records the fastest choice.  Two
@@ -52,16 +53,17 @@ SEED_DIVS = [4, 8, 16]
 PATH_CODE = {"plain": 1, "screen_bf16": 2, "screen_tf32": 3, "screen_bf16x3": 4}
 
 
-def hand_rule(n: int, d: int, k: int, metric: str) -> tuple[str, int, int]:
+def hand_rule(n: int, d: int, k: int, metric: str) -> tuple[str, int, int, int]:
     """The choice used before any measurement exists (and the shape of the
     table when the sweep has not run): plain below 512 points, split-BF16 up
     to d = 256, then BF16 (cosine) or TF32 (euclidean); an eighth sampled;
-    the emission pass over every column tile."""
+    the emission pass over every column tile in the 2-SM form.  Returns
+    (path, seed_div, symmetric, pair)."""
     if n < 512:
-        return "plain", 8, 0
+        return "plain", 8, 0, 1
     if d <= 256:
-        return "screen_bf16x3", 8, 0
-    return ("screen_bf16" if metric == "cosine" else "screen_tf32"), 8, 0
+        return "screen_bf16x3", 8, 0, 1
+    return ("screen_bf16" if metric == "cosine" else "screen_tf32"), 8, 0, 1
 
 
 def _pool(d: int, n: int, seed: int) -> np.ndarray:
@@ -109,9 +111,10 @@ def sweep(grid_n=GRID_N, grid_d=GRID_D, grid_k=GRID_K, metrics=METRICS, verbose=
                     ref = (plain.idx.cpu().numpy(), plain.dist.cpu().numpy().view(np.uint32),
                            plain.sigma.cpu().numpy().view(np.uint32))
                     del plain
-                    def measure(path, sd, sym):
+                    def measure(path, sd, sym, pair=1):
                         _lib.check(lib.hm_tuning_override(sd))
                         _lib.check(lib.hm_tuning_symmetric(sym))
+                        _lib.check(lib.hm_tuning_pair(pair))
                         try:
                             p = DeviceKnnProblem(n, d, k, metric, path)
                             t = _time_run(p, x, 5)
@@ -122,6 +125,7 @@ def sweep(grid_n=GRID_N, grid_d=GRID_D, grid_k=GRID_K, metrics=METRICS, verbose=
                         finally:
                             _lib.check(lib.hm_tuning_override(0))
                             _lib.check(lib.hm_tuning_symmetric(1))
+                            _lib.check(lib.hm_tuning_pair(1))
                         return t if same else None
 
                     for path in SCREENS:
@@ -131,13 +135,15 @@ def sweep(grid_n=GRID_N, grid_d=GRID_D, grid_k=GRID_K, metrics=METRICS, verbose=
                     if screened:
                         c0 = min(screened, key=screened.get)
                         p0, sd0, _ = c0.split("/")
+                        times[f"{p0}/{sd0}/single"] = measure(p0, int(sd0), 0, 0)
                         times[f"{p0}/{sd0}/sym"] = measure(p0, int(sd0), 1)
                     exact = all(t is not None for t in times.values())
                     valid = {c: t for c, t in times.items() if t is not None}
                     best = min(valid, key=valid.get)
                     path, sd, form = (best.split("/") + ["8", "full"])[:3]
                     e = {"n": n, "d": d, "k": k, "metric": metric, "times_ms": times, "best": path,
-                         "seed_div": int(sd), "symmetric": int(form == "sym"), "all_paths_equal_plain": exact}
+                         "seed_div": int(sd), "symmetric": int(form == "sym"), "pair": int(form != "single"),
+                         "all_paths_equal_plain": exact}
                     entries.append(e)
                     if verbose:
                         print(f"{metric:9s} d={d:4d} k={k:2d} n={n:6d}  best {best:18s} "
@@ -158,13 +164,14 @@ def sweep(grid_n=GRID_N, grid_d=GRID_D, grid_k=GRID_K, metrics=METRICS, verbose=
 
 
 def table_from(doc: dict | None) -> tuple[dict, list, list, list]:
-    """(choice[(metric, k, d, n)] = (path, seed_div, symmetric), grid n, d, k)."""
+    """(choice[(metric, k, d, n)] = (path, seed_div, symmetric, pair), grid n, d, k)."""
     if doc is None:
         gn, gd, gk = GRID_N, GRID_D, GRID_K
         choice = {(m, k, d, n): hand_rule(n, d, k, m) for m in METRICS for k in gk for d in gd for n in gn}
         return choice, gn, gd, gk
     g = doc["grid"]
-    choice = {(e["metric"], e["k"], e["d"], e["n"]): (e["best"], e["seed_div"], e.get("symmetric", 1))
+    choice = {(e["metric"], e["k"], e["d"], e["n"]): (e["best"], e["seed_div"], e.get("symmetric", 1),
+                                                      e.get("pair", 1))
               for e in doc["entries"]}
     return choice, g["n"], g["d"], g["k"]
 
@@ -181,9 +188,9 @@ def describe(n: int, d: int, k: int, metric: str) -> dict:
     doc = json.loads(JSON_PATH.read_text()) if JSON_PATH.exists() else None
     choice, gn, gd, gk = table_from(doc)
     key = (metric, _nearest(gk, k), _nearest(gd, d), _nearest(gn, n))
-    path, sd, sym = choice[key]
+    path, sd, sym, pair = choice[key]
     out = {"grid_point": {"metric": key[0], "k": key[1], "d": key[2], "n": key[3]},
-           "choice": path, "seed_div": sd, "symmetric_emission": bool(sym),
+           "choice": path, "seed_div": sd, "symmetric_emission": bool(sym), "two_sm_emission": bool(pair),
            "table": f"measured {doc['measured']} on {doc['device']}" if doc else "hand rule (no measurement)"}
     if doc:
         for e in doc["entries"]:
@@ -199,7 +206,7 @@ def emit_inc(doc: dict | None, path: Path = INC_PATH) -> None:
         "// autotune_table.inc -- generated by holomap_b200/autotune.py from",
         "// holomap_b200/autotune_table.json; do not edit by hand.",
         f"// Source: {src}.",
-        "// kTune[metric][k][d][n] = path | seed_div << 8 | symmetric << 15 at the grid",
+        "// kTune[metric][k][d][n] = path | pair << 4 | seed_div << 8 | symmetric << 15 at the grid",
         "// points below",
         "// (metric 0 euclidean, 1 cosine).",
         "#pragma once",
@@ -215,8 +222,8 @@ def emit_inc(doc: dict | None, path: Path = INC_PATH) -> None:
             for d in gd:
                 row = []
                 for n in gn:
-                    p, sd, sym = choice[(m, k, d, n)]
-                    row.append(str(PATH_CODE[p] | (int(sd) << 8) | (int(sym) << 15)))
+                    p, sd, sym, pair = choice[(m, k, d, n)]
+                    row.append(str(PATH_CODE[p] | (int(pair) << 4) | (int(sd) << 8) | (int(sym) << 15)))
                 lines.append("            {" + ", ".join(row) + "},")
             lines.append("        },")
         lines.append("    },")

@@ -115,6 +115,7 @@ struct GroupPlan {
     std::vector<uint4> eunits;  // emission units, largest first
     bool any_sym = false;
     bool pair = false;  // emission pass in the 2-SM form (units of 256 rows)
+    bool pair_vetoed = false;  // the autotuner table prefers one CTA per row block for a job
     uint32_t egrid = 0, stage_cap = 0;
     size_t off_opa = 0, off_opb = 0, off_rowstat = 0, off_rowterm = 0, off_colterm = 0;
     size_t off_band = 0, off_force = 0, off_rowthr = 0, off_cand = 0, off_cnt = 0, off_topk = 0;
@@ -281,15 +282,13 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
             // table's choice for the shape), at least 2048 (all of them for
             // small jobs), spread over the parts
             uint32_t seed_div = 8;
-            bool sym_ok = true;
-            autotune_choice(P.spec.n, P.spec.d, P.spec.k, P.spec.metric, &seed_div, &sym_ok);
+            bool sym_ok = true, pair_ok = true;
+            autotune_choice(P.spec.n, P.spec.d, P.spec.k, P.spec.metric, &seed_div, &sym_ok, &pair_ok);
+            if (!pair_ok) Gp.pair_vetoed = true;
             const uint64_t seed_cols = std::max<uint64_t>(P.spec.n / std::max<uint32_t>(seed_div, 1), 2048);
             P.seed_tiles = std::min<uint32_t>(
                 P.part_tiles, (uint32_t)((seed_cols + (uint64_t)SC_BN * P.parts - 1) / ((uint64_t)SC_BN * P.parts)));
             P.seed_tiles = std::max<uint32_t>(P.seed_tiles, 1);
-            const double per_list = (double)P.spec.n / (2.0 * P.parts);
-            const double expect = 1.5 * P.spec.k * (2.0 + std::log(std::fmax(1.0, per_list / P.spec.k)));
-            P.cap = std::min<uint32_t>(std::max<uint32_t>(pow2ceil((uint32_t)expect), 128), 4096);
             P.row0 = Gp.rows;
             Gp.rows += (uint32_t)round_up(P.spec.n, 32);  // rows of each job start 32-aligned
             P.unit0 = Gp.units;
@@ -303,22 +302,31 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
             // two column tiles takes the symmetric form: row block rb walks
             // the column tiles from the one holding its own diagonal block
             // (rb / 2) to the end, in parts of ept tiles; the rows of the
-            // blocks above the diagonal get their candidates as columns.  Its
-            // candidate lists per row: two per part, then the column list,
-            // which takes two lists' room.
+            // blocks above the diagonal get their candidates as columns.
             P.sym = sym_ok && P.q0 == 0 && P.q1 == P.spec.n && P.col_tiles >= 2;
             if (P.sym) {
                 uint64_t tiles = 0;
                 for (uint32_t rb = 0; rb < P.row_blocks; ++rb) tiles += P.col_tiles - rb / 2;
                 P.ept = (uint32_t)std::max<uint64_t>(4, (tiles + 4ull * G - 1) / (4ull * G));
                 P.ept = std::max<uint32_t>(P.ept, (P.col_tiles + 7) / 8);  // at most 8 parts: 18 lists
-                const uint32_t eparts = (P.col_tiles + P.ept - 1) / P.ept;
-                P.elists = 2 * eparts + 2;
                 Gp.any_sym = true;
             } else {
                 P.ept = P.part_tiles;
-                P.elists = 2 * P.parts;
             }
+        }
+        // Candidate lists per row: a group with symmetric jobs runs the
+        // symmetric emission pass (two lists per column part, and for a
+        // symmetric job the column list, which takes two lists' room);
+        // otherwise the full pass writes SC_FULL_LISTS lists per part.  The
+        // cap of a list grows with the columns it covers.
+        for (uint32_t j : Gp.jobs) {
+            JobPlan &P = B.jobs[j];
+            const uint32_t eparts = (P.col_tiles + P.ept - 1) / P.ept;
+            const uint32_t per_part = Gp.any_sym ? 2u : (uint32_t)SC_FULL_LISTS;
+            P.elists = per_part * eparts + (P.sym ? 2u : 0u);
+            const double per_list = (double)P.spec.n / ((double)per_part * eparts);
+            const double expect = 1.5 * P.spec.k * (2.0 + std::log(std::fmax(1.0, per_list / P.spec.k)));
+            P.cap = std::min<uint32_t>(std::max<uint32_t>(pow2ceil((uint32_t)expect), 128), 4096);
             P.eslot0 = Gp.elists;
             Gp.elists += P.spec.n * (uint64_t)P.elists;
             P.cand0 = Gp.cand;
@@ -326,8 +334,9 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
         }
         // The emission pass takes the 2-SM form (a cluster of two CTAs per
         // block of 256 rows, each loading half of every column tile) when no
-        // job is symmetric and every job's K slices fit the resident A block.
-        Gp.pair = tuning_pair() && !Gp.any_sym && Gp.kpmax / Gp.kslice <= SC_ARES_STAGES;
+        // job is symmetric, every job's K slices fit the resident A block and
+        // the autotuner table prefers it for every job.
+        Gp.pair = tuning_pair() && !Gp.pair_vetoed && !Gp.any_sym && Gp.kpmax / Gp.kslice <= SC_ARES_STAGES;
         // emission units of the group: (job slot | sym, row block (2-SM form:
         // block of 256 rows), first tile, end tile | part)
         const uint32_t ubm = Gp.pair ? 2 * SC_BM : SC_BM;

@@ -43,16 +43,19 @@ static uint16_t table_entry(uint64_t n, uint32_t d, uint32_t k, int metric) {
     return kTune[metric == HM_METRIC_COSINE ? 1 : 0][ik][id][in];
 }
 
-int autotune_choice(uint64_t n, uint32_t d, uint32_t k, int metric, uint32_t *seed_div, bool *symmetric) {
+int autotune_choice(uint64_t n, uint32_t d, uint32_t k, int metric, uint32_t *seed_div, bool *symmetric,
+                    bool *pair) {
     if (metric == HM_METRIC_MANHATTAN || k > 64 || d > 2048) {
         if (seed_div) *seed_div = 8;
         if (symmetric) *symmetric = true;
+        if (pair) *pair = true;
         return HM_PATH_PLAIN;
     }
     const uint16_t e = table_entry(n, d, k, metric);
     if (seed_div) *seed_div = g_seed_override ? g_seed_override : (uint32_t)((e >> 8) & 0x7f);
     if (symmetric) *symmetric = g_symmetric && (e >> 15) != 0;
-    return (int)(e & 0xff);
+    if (pair) *pair = ((e >> 4) & 1) != 0;
+    return (int)(e & 0xf);
 }
 
 bool tuning_pair() { return g_pair; }
@@ -64,7 +67,7 @@ using namespace hm;
 extern "C" {
 
 int hm_autotune_path(uint64_t n, uint32_t d, uint32_t k, int metric) {
-    return autotune_choice(n, d, k, metric, nullptr, nullptr);
+    return autotune_choice(n, d, k, metric, nullptr, nullptr, nullptr);
 }
 
 int hm_tuning_override(int seed_div) {

@@ -40,8 +40,17 @@ constexpr int SC_STAGES = 4;
 // K slices of the A block kept resident in shared memory for a whole unit
 // (96 KB: 6 slices of 128 B x 128 rows); deeper operands stream A with B
 constexpr uint32_t SC_ARES_STAGES = 6;
-constexpr int SC_EPI_WARPS = 8;  // two per TMEM lane quadrant, one per half tile
-constexpr int SC_THREADS = 64 + 32 * SC_EPI_WARPS;  // warp 0 TMA, warp 1 MMA, warps 2-9 epilogue
+// Epilogue warps per CTA: warp 0 issues the TMA loads, warp 1 the MMAs, the
+// rest read the accumulator, (warp & 3) naming their TMEM lane quadrant (32
+// query rows) and (warp - 2) / 4 their segment of the tile's 256 columns.
+// The threshold and symmetric emission passes take 8 (two segments of 128
+// columns, the threshold pass's sorted arrays need the registers); the full
+// emission pass takes 16 (four segments of 64 columns: twice the warps to
+// hide the latency of the per-row tests, each writing its own candidate
+// list, so a row has four lists per column part).
+__host__ __device__ constexpr int sc_epi_warps(int pass) { return pass == 1 ? 16 : 8; }
+__host__ __device__ constexpr int sc_threads(int pass) { return 64 + 32 * sc_epi_warps(pass); }
+constexpr int SC_FULL_LISTS = 4;  // candidate lists per row and column part of the full emission pass
 
 enum ScreenKind { SCREEN_KIND_BF16 = 0, SCREEN_KIND_TF32 = 1 };
 

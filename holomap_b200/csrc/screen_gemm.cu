@@ -2,15 +2,20 @@
 // accumulators, fused with the per-row thresholds and the candidate emission,
 // so the N x N similarity matrix never leaves the SM.
 //
-// One CTA per SM (persistent), 10 warps:
+// One CTA per SM (persistent), 10 warps (18 in the full emission pass):
 //   warp 0     TMA producer: the unit's 128-row A block stays resident in
 //              shared memory when its K slices fit 96 KB (else it streams
 //              with B), 256-row B slices per stage (128-byte K slices, 128B
 //              swizzle, 4-stage mbarrier ring; every CTA loads its own tiles),
 //   warp 1     allocates 512 TMEM columns (two 128 x 256 fp32 accumulators)
 //              and issues tcgen05.mma (one thread) + tcgen05.commit,
-//   warps 2-9  epilogue: each thread owns one query row (its TMEM lane) and
-//              one half of every tile's 256 columns, read 32 columns at a time.
+//   warps 2-   epilogue: each thread owns one query row (its TMEM lane) and
+//              one segment of every tile's 256 columns (half; a quarter in
+//              the full emission pass), read 32 columns at a time.
+// The full emission pass can also run in the 2-SM form: a cluster of two
+// CTAs shares each 256 x 256 tile (one tcgen05.mma.cta_group::2 of M = 256
+// issued by the leader CTA), each CTA holding its own 128 rows of A and
+// loading half of the column tile into an 8-stage ring.
 // Two launches per group (template PASS):
 //   0  threshold pass over a sample of each part's columns: per list, the k
 //      smallest minima of column chunks, sorted in registers and shared
@@ -92,8 +97,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
 // Bounded wait for the phase of parity `parity` to complete.  Gives up when
 // another role has raised the abort flag (unless draining) or after the
 // time / iteration limits.
-__device__ __noinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile uint32_t *abort_flag,
-                                       bool draining = false) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile uint32_t *abort_flag,
+                                          bool draining = false) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer_ns();
     const uint64_t limit = draining ? SC_DRAIN_LIMIT_NS : SC_WAIT_LIMIT_NS;
@@ -295,7 +300,7 @@ __device__ __forceinline__ UnitTiles unit_tiles(const JobDev *jobs, const GroupD
 }
 
 template <int KIND, int KP, int PASS, bool PAIR>
-__global__ void __launch_bounds__(SC_THREADS, 1)
+__global__ void __launch_bounds__(sc_threads(PASS), 1)
     screen_gemm_kernel(const __grid_constant__ CUtensorMap tma, const __grid_constant__ CUtensorMap tmb,
                        const JobDev *__restrict__ jobs, const GroupDev G, float *dump, uint32_t idesc,
                        uint32_t a_res) {
@@ -331,6 +336,9 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
     // PASS 2 is the emission pass of a group with symmetric units (the
     // column-side tests exist only in that instantiation)
     constexpr bool SYMK = PASS == 2;
+    constexpr uint32_t EW = sc_epi_warps(PASS);   // epilogue warps
+    constexpr uint32_t NSEG = EW / 4;             // column segments per tile (= lists per part)
+    constexpr uint32_t SEGW = SC_BN / NSEG;       // columns per segment
 
     if (threadIdx.x == 0) {
         for (uint32_t s = 0; s < NST; ++s) {
@@ -340,7 +348,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         for (int b = 0; b < 2; ++b) {
             mbar_init(smem_u32(&accf[b]), 1);
             // the leader's accumulator is released by both CTAs' epilogues
-            mbar_init(smem_u32(&acce[b]), PAIR ? 2 * SC_EPI_WARPS : SC_EPI_WARPS);
+            mbar_init(smem_u32(&acce[b]), PAIR ? 2 * EW : EW);
         }
         mbar_init(smem_u32(afull), 1);
         mbar_init(smem_u32(aempty), 1);
@@ -515,10 +523,10 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
         __syncwarp();
     } else {
         // --------------------------------------------------------- epilogue
-        // warps 2..9: quadrant (warp & 3) of the TMEM lanes = 32 query rows,
-        // half (warp - 2) / 4 of the tile's 256 columns
+        // warps 2..EW+1: quadrant (warp & 3) of the TMEM lanes = 32 query
+        // rows, segment (warp - 2) / 4 of the tile's 256 columns
         const uint32_t quad = (uint32_t)(warp & 3);
-        const uint32_t half = (uint32_t)(warp - 2) >> 2;
+        const uint32_t seg = (uint32_t)(warp - 2) >> 2;
         const uint32_t row_in_tile = quad * 32 + lane;
         const float INF = __int_as_float(0x7f800000);
         uint32_t tile = 0;
@@ -538,9 +546,9 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
             const float rowterm = valid ? G.rowterm[gr] : 0.0f;
             const float scale = J.scale;
             // pass 0: the row's threshold-pass list (its k-array); pass 1: its
-            // candidate list for this column part and half
-            const size_t list = PASS == 0 ? list_index(J, valid ? row : 0, ut.part * 2 + half)
-                                          : cand_list(J, valid ? row : 0, ut.part * 2 + half);
+            // candidate list for this column part and segment
+            const size_t list = PASS == 0 ? list_index(J, valid ? row : 0, ut.part * NSEG + seg)
+                                          : cand_list(J, valid ? row : 0, ut.part * NSEG + seg);
             const float *colterm = G.colterm + J.row0;
             // pass 0: the k smallest mini-chunk minima seen (ascending;
             // arr[KP-1] is the list's k-th) and the row's shared k-th
@@ -573,10 +581,10 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                 // the job; below the row block's diagonal its pairs belong to
                 // another unit's column side, above it they also serve the
                 // columns' rows
-                const uint32_t jb = 2 * ct + half;
+                const uint32_t jb = 2 * ct + seg;  // (NSEG = 2 here)
                 const bool skip = SYMK && ut.sym && jb < myrb;
                 const bool colside = SYMK && ut.sym && jb > myrb && jb * (uint32_t)(SC_BN / 2) < n;
-                const uint32_t c_base = ct * SC_BN + half * (SC_BN / 2);
+                const uint32_t c_base = ct * SC_BN + seg * SEGW;
                 // the columns' limits (lane t holds column c_base + 32 q + t),
                 // loaded while the accumulator is still being filled
                 float cthr[4] = {-INF, -INF, -INF, -INF}, cvs[4] = {INF, INF, INF, INF}, cterm[4] = {0, 0, 0, 0};
@@ -613,7 +621,7 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                     tnext = *(volatile const uint32_t *)(G.rowthr + gr);
                 }
                 const bool diag = (ct * SC_BN < myrb * SC_BM + SC_BM) && (myrb * SC_BM < ct * SC_BN + SC_BN);
-                const uint32_t t_base = tmem_base + ((quad * 32) << 16) + buf * SC_BN + half * (SC_BN / 2);
+                const uint32_t t_base = tmem_base + ((quad * 32) << 16) + buf * SC_BN + seg * SEGW;
                 // one chunk = 32 columns; the accumulator registers are
                 // overwritten in place by the screened values
                 auto process = [&](uint32_t (&v)[32], uint32_t ch) {
@@ -844,17 +852,31 @@ __global__ void __launch_bounds__(SC_THREADS, 1)
                         }
                     }
                 };
-                uint32_t va[32], vb[32];
-                tmem_ld32_issue(t_base, va);
-                tmem_ld_wait(va);
+                if constexpr (EW >= 16) {
+                    // four warps per scheduler hide the load latency: one
+                    // chunk of registers
+                    uint32_t va[32];
 #pragma unroll 1
-                for (uint32_t ch = 0; ch < SC_BN / 64; ch += 2) {
-                    tmem_ld32_issue(t_base + (ch + 1) * 32, vb);
-                    process(va, ch);
-                    tmem_ld_wait(vb);
-                    if (ch + 2 < SC_BN / 64) tmem_ld32_issue(t_base + (ch + 2) * 32, va);
-                    process(vb, ch + 1);
-                    if (ch + 2 < SC_BN / 64) tmem_ld_wait(va);
+                    for (uint32_t ch = 0; ch < SEGW / 32; ++ch) {
+                        tmem_ld32_issue(t_base + ch * 32, va);
+                        tmem_ld_wait(va);
+                        process(va, ch);
+                    }
+                } else {
+                    // two warps per scheduler: the next chunk loads while
+                    // this one is processed
+                    uint32_t va[32], vb[32];
+                    tmem_ld32_issue(t_base, va);
+                    tmem_ld_wait(va);
+#pragma unroll 1
+                    for (uint32_t ch = 0; ch < SEGW / 32; ch += 2) {
+                        tmem_ld32_issue(t_base + (ch + 1) * 32, vb);
+                        process(va, ch);
+                        tmem_ld_wait(vb);
+                        if (ch + 2 < SEGW / 32) tmem_ld32_issue(t_base + (ch + 2) * 32, va);
+                        process(vb, ch + 1);
+                        if (ch + 2 < SEGW / 32) tmem_ld_wait(va);
+                    }
                 }
                 fence_before_sync();
                 __syncwarp();
@@ -907,7 +929,7 @@ static uint32_t pair_slots(const void *func) {
     if (hit > 0) return (uint32_t)(hit - 1);
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(2 * (uint32_t)device_sm_count(), 1, 1);
-    cfg.blockDim = dim3(SC_THREADS, 1, 1);
+    cfg.blockDim = dim3(sc_threads(1), 1, 1);
     cfg.dynamicSmemBytes = SC_SMEM_BYTES;
     cudaLaunchAttribute attr;
     attr.id = cudaLaunchAttributeClusterDimension;
@@ -938,7 +960,7 @@ static int launch_pair(const JobDev *jobs, const GroupDev &G, const CUtensorMap 
     if (clusters == 0) return HM_OK;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(2 * clusters, 1, 1);
-    cfg.blockDim = dim3(SC_THREADS, 1, 1);
+    cfg.blockDim = dim3(sc_threads(1), 1, 1);
     cfg.dynamicSmemBytes = SC_SMEM_BYTES;
     cfg.stream = s;
     cudaLaunchAttribute attr;
@@ -967,7 +989,7 @@ static int launch_kind(const JobDev *jobs, const GroupDev &G, const CUtensorMap 
     if (grid == 0) return HM_OK;
     // every job's K slices fit the resident A block
     const uint32_t a_res = (G.kpmax / G.kslice) <= SC_ARES_STAGES ? 1u : 0u;
-    screen_gemm_kernel<KIND, KP, PASS, false><<<grid, SC_THREADS, SC_SMEM_BYTES, s>>>(ta, tb, jobs, G, dump,
+    screen_gemm_kernel<KIND, KP, PASS, false><<<grid, sc_threads(PASS), SC_SMEM_BYTES, s>>>(ta, tb, jobs, G, dump,
                                                                                       idesc, a_res);
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();

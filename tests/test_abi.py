@@ -113,7 +113,7 @@ def test_autotune_table_is_the_committed_measurement():
     from holomap_b200 import autotune
     doc = _autotune_doc()
     choice, gn, gd, gk = autotune.table_from(doc)
-    for (metric, k, d, n), (path, _, _) in choice.items():
+    for (metric, k, d, n), (path, *_) in choice.items():
         assert hm.autotune_path(n, d, k, metric) == hm.KnnPath.parse(path), (metric, k, d, n)
     import tempfile
     from pathlib import Path
