@@ -12,9 +12,14 @@ launching stream, one full kNN + smooth-kNN run of
   with one CTA per 128-row block instead of the 2-SM form and with the
   symmetric emission pass (tiles on and above the diagonal only),
 
-on seeded Gaussian-mixture data of that shape, checks that every screened
-result equals the plain path's bytes, and records the fastest choice.  Two
-files are written:
+on seeded data of that shape, checks that every screened result equals the
+plain path's bytes, and records the fastest choice.  Euclidean points are
+Gaussian mixtures (3-20 clusters); cosine points have the shape of text or
+image embeddings (a decaying spectrum, N(0, diag(i^-1.2)), a shared offset,
+unit norm).  Cosine data made of a few very tight clusters far from the
+origin is the screens' hard case: neighbour gaps far below the BF16 band
+send most rows to the exact fallback, where TF32 or split-BF16 is faster.
+Two files are written:
 
 * ``holomap_b200/autotune_table.json`` -- every measurement, the choice per
   grid point, and the device and command that produced them;
@@ -66,9 +71,12 @@ def hand_rule(n: int, d: int, k: int, metric: str) -> tuple[str, int, int, int]:
     return ("screen_bf16" if metric == "cosine" else "screen_tf32"), 8, 0, 1
 
 
-def _pool(d: int, n: int, seed: int) -> np.ndarray:
-    from .synth import _rng, gaussian_mixture
-    g = _rng(900000 + 10 * d + seed)
+def _pool(d: int, n: int, metric: str) -> np.ndarray:
+    from .synth import _rng, embedding_like, gaussian_mixture
+    if metric == "cosine":
+        g = _rng(900001 + 10 * d)
+        return np.ascontiguousarray(embedding_like(g, n, d).astype(np.float32))
+    g = _rng(900000 + 10 * d)
     clusters = int(g.integers(3, 21))
     return np.ascontiguousarray(gaussian_mixture(g, n, d, clusters, 4.0, 0.3, 3.0).astype(np.float32))
 
@@ -99,7 +107,7 @@ def sweep(grid_n=GRID_N, grid_d=GRID_D, grid_k=GRID_K, metrics=METRICS, verbose=
     t_start = time.time()
     for metric in metrics:
         for d in grid_d:
-            pool = _pool(d, max(grid_n), 0 if metric == "euclidean" else 1)
+            pool = _pool(d, max(grid_n), metric)
             xpool = torch.from_numpy(pool).cuda()
             for k in grid_k:
                 for n in grid_n:
@@ -155,7 +163,8 @@ def sweep(grid_n=GRID_N, grid_d=GRID_D, grid_k=GRID_K, metrics=METRICS, verbose=
         "command": "python -m holomap_b200.autotune",
         "timing": "median of CUDA-event times of full kNN + smooth-kNN runs on device-resident "
                   "inputs (one warm-up run first)",
-        "data": "seeded Gaussian mixtures (3-20 clusters, centres N(0, 16 I), sigma U[0.3, 3]); "
+        "data": "euclidean: seeded Gaussian mixtures (3-20 clusters, centres N(0, 16 I), sigma U[0.3, 3]); "
+                "cosine: embedding-shaped rows (N(0, diag(i^-1.2)) plus an offset of norm 0.3, unit norm); "
                 "prefixes of one 50,000-point pool per (d, metric)",
         "sweep_seconds": round(time.time() - t_start, 1),
         "grid": {"n": list(grid_n), "d": list(grid_d), "k": list(grid_k), "metric": list(metrics)},

@@ -36,7 +36,7 @@ def nvcc() -> str:
 
 
 def _headers_mtime() -> float:
-    files = list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    files = list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.inc")) + list(INCLUDE.glob("*.h"))
     return max((f.stat().st_mtime for f in files), default=0.0)
 
 

@@ -80,6 +80,17 @@ def dups_20k(n: int = 20000, d: int = 128, seed: int = 2) -> Workload:
     return Workload("dups_20k", np.ascontiguousarray(x), 15, "euclidean")
 
 
+def embedding_like(g: np.random.Generator, n: int, d: int) -> np.ndarray:
+    """Rows with an embedding model's shape: N(0, diag(i^-1.2)) plus a shared
+    offset of norm 0.3, L2-normalised (float64)."""
+    lam = np.arange(1, d + 1, dtype=np.float64) ** -1.2
+    z = g.normal(0.0, 1.0, size=(n, d)) * np.sqrt(lam)
+    off = g.normal(0.0, 1.0, size=d)
+    z += 0.3 * off / np.linalg.norm(off)
+    z /= np.linalg.norm(z, axis=1, keepdims=True)
+    return z
+
+
 def embed_50k(n: int = 50000, d: int = 384, seed: int = 3) -> Workload:
     g = _rng(seed)
     lam = np.arange(1, d + 1, dtype=np.float64) ** -1.2
