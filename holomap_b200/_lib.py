@@ -202,6 +202,7 @@ SIGNATURES = {
     "hm_last_error": (ctypes.c_char_p, []),
     "hm_abi_version": (_i32, []),
     "hm_autotune_path": (_i32, [_u64, _u32, _u32, _i32]),
+    "hm_autotune_path_batched": (_i32, [_u64, _u32, _u32, _i32]),
     "hm_tuning_override": (_i32, [_i32]),
     "hm_tuning_symmetric": (_i32, [_i32]),
     "hm_tuning_pair": (_i32, [_i32]),
@@ -439,5 +440,8 @@ def workspace_bytes(n: int, d: int, k: int, metric="euclidean", path="auto") -> 
     return b
 
 
-def autotune_path(n: int, d: int, k: int, metric="euclidean") -> KnnPath:
-    return KnnPath(lib().hm_autotune_path(n, d, k, int(Metric.parse(metric))))
+def autotune_path(n: int, d: int, k: int, metric="euclidean", batched: bool = False) -> KnnPath:
+    """The path HM_PATH_AUTO takes for a problem alone (or, batched=True, for a
+    job planned in a batch of several)."""
+    f = lib().hm_autotune_path_batched if batched else lib().hm_autotune_path
+    return KnnPath(f(n, d, k, int(Metric.parse(metric))))

@@ -13,7 +13,10 @@ launching stream, one full kNN + smooth-kNN run of
   symmetric emission pass (tiles on and above the diagonal only),
 
 on seeded data of that shape, checks that every screened result equals the
-plain path's bytes, and records the fastest choice.  Euclidean points are
+plain path's bytes, and records the fastest choice.  Up to 8192 points it
+also times each path on a batch of 32 jobs of that shape (one CUDA graph per
+batch, windows of the same pool), where the screens' fixed per-call costs are
+shared: jobs planned in a batch take that choice.  Euclidean points are
 Gaussian mixtures (3-20 clusters); cosine points have the shape of text or
 image embeddings (a decaying spectrum, N(0, diag(i^-1.2)), a shared offset,
 unit norm).  Cosine data made of a few very tight clusters far from the
@@ -55,6 +58,8 @@ GRID_K = [15, 30]
 METRICS = ["euclidean", "cosine"]
 SCREENS = ["screen_bf16", "screen_tf32", "screen_bf16x3"]
 SEED_DIVS = [4, 8, 16]
+BATCH_JOBS = 32
+BATCH_MAX_N = 8192
 PATH_CODE = {"plain": 1, "screen_bf16": 2, "screen_tf32": 3, "screen_bf16x3": 4}
 
 
@@ -95,6 +100,49 @@ def _time_run(prob, x, reps: int) -> float:
         e1.synchronize()
         ms.append(e0.elapsed_time(e1))
     return statistics.median(ms)
+
+
+def _time_batch(batch, reps: int) -> float:
+    import torch
+    s = torch.cuda.current_stream()
+    batch.run(s, graph=True)  # warm: captures the batch's graph
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        batch.run(s, graph=True)
+        e1.record(s)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    return statistics.median(ms)
+
+
+def _batch_measure(xpool, n: int, k: int, metric: str, seed_div: dict, lib) -> dict:
+    """Per-batch times of BATCH_JOBS jobs of one shape on each path (None
+    where a screened batch's bytes differ from the plain batch's)."""
+    from . import _lib
+    from .device import DeviceBatch
+    span = xpool.shape[0] - n
+    xs = [xpool[(j * 1543) % max(span, 1):][:n].contiguous() for j in range(BATCH_JOBS)]
+    times, ref = {}, None
+    for path in ["plain"] + SCREENS:
+        _lib.check(lib.hm_tuning_override(seed_div.get(path, 8)))
+        try:
+            b = DeviceBatch([(x, k, metric, path) for x in xs])
+            t = _time_batch(b, 5)
+            got = [b.result(j) for j in range(BATCH_JOBS)]
+            del b
+        finally:
+            _lib.check(lib.hm_tuning_override(0))
+        if ref is None:
+            ref = got
+            times[path] = t
+        else:
+            same = all(np.array_equal(a.view(np.uint32), r.view(np.uint32))
+                       for g, rr in zip(got, ref) for a, r in zip(g, rr))
+            times[path] = t if same else None
+    return times
 
 
 def sweep(grid_n=GRID_N, grid_d=GRID_D, grid_k=GRID_K, metrics=METRICS, verbose=True) -> dict:
@@ -152,10 +200,24 @@ def sweep(grid_n=GRID_N, grid_d=GRID_D, grid_k=GRID_K, metrics=METRICS, verbose=
                     e = {"n": n, "d": d, "k": k, "metric": metric, "times_ms": times, "best": path,
                          "seed_div": int(sd), "symmetric": int(form == "sym"), "pair": int(form != "single"),
                          "all_paths_equal_plain": exact}
+                    if n <= BATCH_MAX_N:
+                        # each screen at its fastest single-job sample
+                        sds = {}
+                        for c, t in valid.items():
+                            pth, *rest = c.split("/")
+                            if rest and rest[1] == "full" and (pth not in sds or t < valid[f"{pth}/{sds[pth]}/full"]):
+                                sds[pth] = int(rest[0])
+                        bt = _batch_measure(xpool, n, k, metric, sds, lib)
+                        bvalid = {c: t for c, t in bt.items() if t is not None}
+                        bbest = min(bvalid, key=bvalid.get)
+                        e.update({"batch_jobs": BATCH_JOBS, "batch_times_ms": bt, "batch_best": bbest,
+                                  "batch_seed_div": sds.get(bbest, 8),
+                                  "all_paths_equal_plain": exact and all(t is not None for t in bt.values())})
                     entries.append(e)
                     if verbose:
+                        extra = f"  batch {e['batch_best']}" if "batch_best" in e else ""
                         print(f"{metric:9s} d={d:4d} k={k:2d} n={n:6d}  best {best:18s} "
-                              f"{valid[best]:9.3f} ms  (plain {times['plain']:9.3f} ms)", flush=True)
+                              f"{valid[best]:9.3f} ms  (plain {times['plain']:9.3f} ms){extra}", flush=True)
     props = torch.cuda.get_device_properties(0)
     return {
         "device": props.name, "sms": props.multi_processor_count,
@@ -172,17 +234,25 @@ def sweep(grid_n=GRID_N, grid_d=GRID_D, grid_k=GRID_K, metrics=METRICS, verbose=
     }
 
 
-def table_from(doc: dict | None) -> tuple[dict, list, list, list]:
-    """(choice[(metric, k, d, n)] = (path, seed_div, symmetric, pair), grid n, d, k)."""
+def table_from(doc: dict | None) -> tuple[dict, dict, list, list, list]:
+    """(choice, batch_choice, grid n, d, k); choice[(metric, k, d, n)] =
+    (path, seed_div, symmetric, pair) for a problem alone, batch_choice the
+    same for a job planned in a batch (the single choice where no batch was
+    measured)."""
     if doc is None:
         gn, gd, gk = GRID_N, GRID_D, GRID_K
         choice = {(m, k, d, n): hand_rule(n, d, k, m) for m in METRICS for k in gk for d in gd for n in gn}
-        return choice, gn, gd, gk
+        return choice, dict(choice), gn, gd, gk
     g = doc["grid"]
-    choice = {(e["metric"], e["k"], e["d"], e["n"]): (e["best"], e["seed_div"], e.get("symmetric", 1),
-                                                      e.get("pair", 1))
-              for e in doc["entries"]}
-    return choice, g["n"], g["d"], g["k"]
+    choice, batch = {}, {}
+    for e in doc["entries"]:
+        key = (e["metric"], e["k"], e["d"], e["n"])
+        choice[key] = (e["best"], e["seed_div"], e.get("symmetric", 1), e.get("pair", 1))
+        if "batch_best" in e:
+            batch[key] = (e["batch_best"], e.get("batch_seed_div", 8), 0, 1)
+        else:
+            batch[key] = choice[key]
+    return choice, batch, g["n"], g["d"], g["k"]
 
 
 def _nearest(grid, v) -> int:
@@ -195,11 +265,12 @@ def describe(n: int, d: int, k: int, metric: str) -> dict:
     if metric == "manhattan" or k > 64 or d > 2048:
         return {"choice": "plain", "reason": "no screen applies"}
     doc = json.loads(JSON_PATH.read_text()) if JSON_PATH.exists() else None
-    choice, gn, gd, gk = table_from(doc)
+    choice, batch, gn, gd, gk = table_from(doc)
     key = (metric, _nearest(gk, k), _nearest(gd, d), _nearest(gn, n))
     path, sd, sym, pair = choice[key]
     out = {"grid_point": {"metric": key[0], "k": key[1], "d": key[2], "n": key[3]},
            "choice": path, "seed_div": sd, "symmetric_emission": bool(sym), "two_sm_emission": bool(pair),
+           "batch_choice": batch[key][0],
            "table": f"measured {doc['measured']} on {doc['device']}" if doc else "hand rule (no measurement)"}
     if doc:
         for e in doc["entries"]:
@@ -209,34 +280,35 @@ def describe(n: int, d: int, k: int, metric: str) -> dict:
 
 
 def emit_inc(doc: dict | None, path: Path = INC_PATH) -> None:
-    choice, gn, gd, gk = table_from(doc)
+    choice, batch, gn, gd, gk = table_from(doc)
     src = doc["measured"] + " on " + doc["device"] if doc else "no measurement yet (the hand rule)"
     lines = [
         "// autotune_table.inc -- generated by holomap_b200/autotune.py from",
         "// holomap_b200/autotune_table.json; do not edit by hand.",
         f"// Source: {src}.",
         "// kTune[metric][k][d][n] = path | pair << 4 | seed_div << 8 | symmetric << 15 at the grid",
-        "// points below",
-        "// (metric 0 euclidean, 1 cosine).",
+        "// points below, for a problem alone; kTuneBatch the same for a job planned",
+        "// in a batch of several (metric 0 euclidean, 1 cosine).",
         "#pragma once",
         f"static const uint32_t kTuneN[{len(gn)}] = {{{', '.join(map(str, gn))}}};",
         f"static const uint32_t kTuneD[{len(gd)}] = {{{', '.join(map(str, gd))}}};",
         f"static const uint32_t kTuneK[{len(gk)}] = {{{', '.join(map(str, gk))}}};",
-        f"static const uint16_t kTune[2][{len(gk)}][{len(gd)}][{len(gn)}] = {{",
     ]
-    for m in METRICS:
-        lines.append("    {")
-        for k in gk:
-            lines.append("        {")
-            for d in gd:
-                row = []
-                for n in gn:
-                    p, sd, sym, pair = choice[(m, k, d, n)]
-                    row.append(str(PATH_CODE[p] | (int(pair) << 4) | (int(sd) << 8) | (int(sym) << 15)))
-                lines.append("            {" + ", ".join(row) + "},")
-            lines.append("        },")
-        lines.append("    },")
-    lines.append("};")
+    for name, table in (("kTune", choice), ("kTuneBatch", batch)):
+        lines.append(f"static const uint16_t {name}[2][{len(gk)}][{len(gd)}][{len(gn)}] = {{")
+        for m in METRICS:
+            lines.append("    {")
+            for k in gk:
+                lines.append("        {")
+                for d in gd:
+                    row = []
+                    for n in gn:
+                        p, sd, sym, pair = table[(m, k, d, n)]
+                        row.append(str(PATH_CODE[p] | (int(pair) << 4) | (int(sd) << 8) | (int(sym) << 15)))
+                    lines.append("            {" + ", ".join(row) + "},")
+                lines.append("        },")
+            lines.append("    },")
+        lines.append("};")
     path.write_text("\n".join(lines) + "\n")
 
 

@@ -186,7 +186,8 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
         const hm_job &s = P.spec;
         HM_TRY(validate_shape(s.n, s.d, s.k, s.metric));
         int path = s.path;
-        if (path == HM_PATH_AUTO) path = hm_autotune_path(s.n, s.d, s.k, s.metric);
+        if (path == HM_PATH_AUTO)
+            path = autotune_choice(s.n, s.d, s.k, s.metric, nullptr, nullptr, nullptr, njobs > 1);
         if (path < HM_PATH_PLAIN || path > HM_PATH_SCREEN_BF16X3)
             return set_error(HM_ERR_INVALID, "unknown path %d", s.path);
         if (path != HM_PATH_PLAIN && !screen_capable(s.d, s.k, s.metric))
@@ -283,7 +284,8 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
             // small jobs), spread over the parts
             uint32_t seed_div = 8;
             bool sym_ok = true, pair_ok = true;
-            autotune_choice(P.spec.n, P.spec.d, P.spec.k, P.spec.metric, &seed_div, &sym_ok, &pair_ok);
+            autotune_choice(P.spec.n, P.spec.d, P.spec.k, P.spec.metric, &seed_div, &sym_ok, &pair_ok,
+                            njobs > 1);
             if (!pair_ok) Gp.pair_vetoed = true;
             const uint64_t seed_cols = std::max<uint64_t>(P.spec.n / std::max<uint32_t>(seed_div, 1), 2048);
             P.seed_tiles = std::min<uint32_t>(

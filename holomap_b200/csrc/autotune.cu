@@ -7,8 +7,11 @@
 // plain path and the three screens (each with 1/4, 1/8 or 1/16 of the columns
 // sampled), all of which return the same bytes.  A problem takes the choice of
 // the nearest grid point (n by ratio, d by ratio, k by the nearer of the
-// measured k), including whether the emission pass takes the symmetric form.  Where no screen applies (manhattan, k > 64, d > 2048) the path
-// is plain.
+// measured k), including whether the emission pass takes the symmetric or
+// the 2-SM form.  Where no screen applies (manhattan, k > 64, d > 2048) the
+// path is plain.  A job planned in a batch of several takes the batch table:
+// the same grid measured as batches of jobs of that shape, where the
+// screens' fixed costs are shared and small jobs favour them.
 #include <cuda_runtime.h>
 
 #include <cmath>
@@ -36,22 +39,23 @@ static size_t nearest_ratio(const uint32_t (&grid)[N], double v) {
     return best;
 }
 
-static uint16_t table_entry(uint64_t n, uint32_t d, uint32_t k, int metric) {
+static uint16_t table_entry(uint64_t n, uint32_t d, uint32_t k, int metric, bool batched) {
     const size_t in = nearest_ratio(kTuneN, (double)(n ? n : 1));
     const size_t id = nearest_ratio(kTuneD, (double)(d ? d : 1));
     const size_t ik = nearest_ratio(kTuneK, (double)(k ? k : 1));
-    return kTune[metric == HM_METRIC_COSINE ? 1 : 0][ik][id][in];
+    const int m = metric == HM_METRIC_COSINE ? 1 : 0;
+    return batched ? kTuneBatch[m][ik][id][in] : kTune[m][ik][id][in];
 }
 
 int autotune_choice(uint64_t n, uint32_t d, uint32_t k, int metric, uint32_t *seed_div, bool *symmetric,
-                    bool *pair) {
+                    bool *pair, bool batched) {
     if (metric == HM_METRIC_MANHATTAN || k > 64 || d > 2048) {
         if (seed_div) *seed_div = 8;
         if (symmetric) *symmetric = true;
         if (pair) *pair = true;
         return HM_PATH_PLAIN;
     }
-    const uint16_t e = table_entry(n, d, k, metric);
+    const uint16_t e = table_entry(n, d, k, metric, batched);
     if (seed_div) *seed_div = g_seed_override ? g_seed_override : (uint32_t)((e >> 8) & 0x7f);
     if (symmetric) *symmetric = g_symmetric && (e >> 15) != 0;
     if (pair) *pair = ((e >> 4) & 1) != 0;
@@ -67,7 +71,11 @@ using namespace hm;
 extern "C" {
 
 int hm_autotune_path(uint64_t n, uint32_t d, uint32_t k, int metric) {
-    return autotune_choice(n, d, k, metric, nullptr, nullptr, nullptr);
+    return autotune_choice(n, d, k, metric, nullptr, nullptr, nullptr, false);
+}
+
+int hm_autotune_path_batched(uint64_t n, uint32_t d, uint32_t k, int metric) {
+    return autotune_choice(n, d, k, metric, nullptr, nullptr, nullptr, true);
 }
 
 int hm_tuning_override(int seed_div) {

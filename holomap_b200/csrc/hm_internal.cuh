@@ -221,7 +221,7 @@ int kpl_for_k(uint32_t k);  // 1, 2, 4, 8 or 0 if k > 256
 // (symmetric) whether its emission pass takes the symmetric form (never when
 // hm_tuning_symmetric(0) is in force on this thread).
 int autotune_choice(uint64_t n, uint32_t d, uint32_t k, int metric, uint32_t *seed_div, bool *symmetric,
-                    bool *pair);
+                    bool *pair, bool batched);
 // Whether screened plans made on this thread may run the emission pass in
 // the 2-SM form (hm_tuning_pair).
 bool tuning_pair();

@@ -16,14 +16,12 @@
 //      the screen cannot bound (zero vectors under cosine), are appended to the
 //      overflow list for the exact plain path.
 //   2. exact distances: the survivors of the warp's rows are taken as one flat
-//      sequence and processed 64 at a time (a slice never spans more than 4
-//      rows), two candidates per lane (pairs lane and 32 + lane: two
-//      independent binary64 chains whose steps interleave, so each hides the
-//      other's add latency).  The candidate rows are staged through shared
-//      memory 16 dimensions at a time by cp.async with coalesced 64-byte
-//      reads (4 lanes per candidate row; a 2-stage pipeline), the query
-//      rows' chunks beside them, converted once to binary64; each chain
-//      accumulates its pair exactly as the reference does
+//      sequence and processed 32 at a time (a slice never spans more than 4
+//      rows), one candidate per lane.  The candidate rows are staged through
+//      shared memory 32 dimensions at a time by cp.async with coalesced
+//      128-byte reads (8 lanes per candidate row; a 2-stage pipeline), the
+//      query rows' chunks beside them, converted once to binary64; each lane
+//      then accumulates its pair exactly as the reference does
 //      (src/metric.rs:42-53 euclidean, :58-70 cosine: binary64, dimension
 //      order, no contraction; self forced to 0 as in src/knn.rs:38-39) and
 //      overwrites its survivor's slot with the (distance bits, index) key.
@@ -102,22 +100,20 @@ constexpr int RR_ROWS = 8;        // group rows per warp of the exact phase
 constexpr int RR_WARPS = 4;       // warps per block of the exact phase
 constexpr int RR_CBUF = 512;      // emitted candidates a warp stages in shared memory
 constexpr int RS_WARPS = 8;       // rows (warps) per block of the select and top-k phases
-constexpr int RR_STAGES = 2;      // chunks in flight (11.4 KB of shared memory per warp)
-constexpr int RR_NC = 2;          // candidate pairs per lane: independent binary64 chains
-constexpr int RR_SLICE = 32 * RR_NC;  // pairs per slice
-constexpr int RR_CH = 16;         // dimensions per chunk
-constexpr int RR_XJ_STRIDE = 20;  // floats per staged candidate chunk (80 B: 16-byte aligned rows;
-                                  // eight consecutive lanes' 16-byte reads hit distinct banks)
+constexpr int RR_STAGES = 2;      // chunks in flight (11.5 KB of shared memory per warp)
+constexpr int RR_CH = 32;         // dimensions per chunk
+constexpr int RR_XJ_STRIDE = 36;  // floats per staged candidate chunk (144 B: 16-byte aligned rows
+                                  // whose 16-byte reads by 32 lanes need the minimum 4 wavefronts)
 constexpr int RR_QROWS = 4;       // query rows per slice
-constexpr int RR_XI_STRIDE = 20;  // doubles per converted query-row chunk (rows 8 banks apart)
+constexpr int RR_XI_STRIDE = 36;  // doubles per converted query-row chunk (rows 8 banks apart)
 
 // Shared memory of one warp of the exact phase: the chunk pipeline.
 struct RrWarpSmem {
     struct {
-        float xj[RR_STAGES][RR_SLICE][RR_XJ_STRIDE];
-        float xi[RR_STAGES][RR_QROWS][RR_CH];
+        float xj[RR_STAGES][32][RR_XJ_STRIDE];
+        float xi[RR_STAGES][RR_QROWS][32];
         double xid[RR_QROWS][RR_XI_STRIDE];
-        uint32_t cj[RR_SLICE];
+        uint32_t cj[32];
     } ex;
 };
 
@@ -402,65 +398,44 @@ __device__ __forceinline__ void exact_pairs(const JobDev &J, const GroupDev &G, 
     // 16-byte staging when every candidate chunk starts 16-byte aligned
     const bool vec = (d & 3u) == 0 && (reinterpret_cast<uintptr_t>(x) & 15u) == 0;
     const uint32_t nch = (d + RR_CH - 1) / RR_CH;
-    const uint32_t sub = (uint32_t)lane & 3u;   // 16-byte piece of a candidate chunk (vector path)
-    const uint32_t qd = (uint32_t)lane & 15u;   // dimension of a query chunk this lane copies
-    const uint32_t qa = (uint32_t)lane >> 4;    // first query row it copies (and qa + 2)
 
     for (uint32_t s = 0; s < total;) {
         // rows of the slice: the first is the row holding pair s; a slice
-        // ends at RR_SLICE pairs, at the total, or where a fifth row would begin
+        // ends at 32 pairs, at the total, or where a fifth row would begin
         const uint32_t r_s = __popc(__ballot_sync(0xffffffffu, lane < RR_ROWS && incl <= s));
-        uint32_t end = min(s + (uint32_t)RR_SLICE, total);
+        uint32_t end = min(s + 32, total);
         if (r_s + RR_QROWS < RR_ROWS) end = min(end, __shfl_sync(0xffffffffu, excl, r_s + RR_QROWS));
-        // the slice's row starts relative to pair s
-        uint32_t e_q[RR_QROWS];
+        const uint32_t p = s + lane;
+        const bool active = p < end;
+        uint32_t ri = 0;  // the lane's row, relative to r_s
 #pragma unroll
         for (uint32_t q = 1; q < RR_QROWS; ++q) {
             const uint32_t e = __shfl_sync(0xffffffffu, excl, min(r_s + q, (uint32_t)RR_ROWS - 1));
-            e_q[q] = r_s + q < RR_ROWS ? e : 0xffffffffu;
+            if (r_s + q < RR_ROWS && p >= e) ri = q;
         }
-        // chain c of this lane: pair s + 32 c + lane, of row r_s + ri[c]
-        uint32_t ri[RR_NC], jc[RR_NC], rowc[RR_NC];
-        bool act[RR_NC];
-        unsigned long long *slot[RR_NC];
-#pragma unroll
-        for (int c = 0; c < RR_NC; ++c) {
-            const uint32_t p = s + 32 * c + lane;
-            act[c] = p < end;
-            ri[c] = 0;
-#pragma unroll
-            for (uint32_t q = 1; q < RR_QROWS; ++q)
-                if (p >= e_q[q]) ri[c] = q;
-        }
-        const uint32_t span = end - s;  // 1..RR_SLICE pairs
-        const uint32_t last0 = __shfl_sync(0xffffffffu, ri[0], min(span, 32u) - 1);
-        const uint32_t last1 = __shfl_sync(0xffffffffu, ri[RR_NC - 1], span > 32 ? span - 33 : 0u);
-        const uint32_t nr = (span > 32 ? last1 : last0) + 1;  // query rows staged for this slice
-#pragma unroll
-        for (int c = 0; c < RR_NC; ++c) {
-            const uint32_t my_excl = __shfl_sync(0xffffffffu, excl, r_s + ri[c]);
-            rowc[c] = gr0 + r_s + ri[c] - J.row0;  // job-local
-            // idle chains (p >= end) may name a padding row: they read nothing
-            slot[c] = row_region(J, G, rowc[c]) + (s + 32 * c + lane - my_excl);
-            jc[c] = act[c] ? (uint32_t)*slot[c] : 0u;
-        }
-        const uint32_t j0 = __shfl_sync(0xffffffffu, jc[0], 0);
-#pragma unroll
-        for (int c = 0; c < RR_NC; ++c) {
-            if (!act[c]) jc[c] = j0;  // idle chains stage a valid row (pair s's)
-            sm.ex.cj[32 * c + lane] = jc[c];
-        }
+        const uint32_t last = __shfl_sync(0xffffffffu, ri, min(end - s, 32u) - 1);
+        const uint32_t nr = last + 1;  // query rows staged for this slice
+        const uint32_t my_excl = __shfl_sync(0xffffffffu, excl, r_s + ri);
+        const uint32_t row = gr0 + r_s + ri - J.row0;  // job-local
+        // idle lanes (p >= end) may name a padding row: they read nothing
+        unsigned long long *slot = row_region(J, G, row) + (p - my_excl);
+        uint32_t j = 0;
+        if (active) j = (uint32_t)*slot;
+        const uint32_t j0 = __shfl_sync(0xffffffffu, j, 0);
+        if (!active) j = j0;  // idle lanes stage a valid row (lane 0's)
+        sm.ex.cj[lane] = j;
         __syncwarp();
 
         // the rows this lane copies from, fixed for the slice: candidate
-        // 8 i + lane / 4 (16-byte pieces, vector path) and query rows qa, qa + 2
+        // 4 i + lane / 8 (16-byte pieces, vector path) and query row a
+        const uint32_t sub = (uint32_t)lane & 7u;
         const float *cp[8];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) cp[i] = x + (size_t)sm.ex.cj[8 * i + ((uint32_t)lane >> 2)] * d + 4 * sub;
-        const float *qp[2];
+        for (int i = 0; i < 8; ++i) cp[i] = x + (size_t)sm.ex.cj[4 * i + ((uint32_t)lane >> 3)] * d + 4 * sub;
+        const float *qp[RR_QROWS];
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
-            qp[h] = x + (size_t)(gr0 + r_s + min(qa + 2 * h, nr - 1) - J.row0) * d + qd;
+        for (int a = 0; a < RR_QROWS; ++a)
+            qp[a] = x + (size_t)(gr0 + r_s + min((uint32_t)a, nr - 1) - J.row0) * d + lane;
 
         auto issue = [&](uint32_t c, uint32_t st) {
             const uint32_t dim0 = c * RR_CH;
@@ -468,94 +443,67 @@ __device__ __forceinline__ void exact_pairs(const JobDev &J, const GroupDev &G, 
                 const bool in = dim0 + 4 * sub < d;  // d % 4 == 0: a piece is all in or all out
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
-                    const uint32_t cand = 8 * i + ((uint32_t)lane >> 2);
+                    const uint32_t cand = 4 * i + ((uint32_t)lane >> 3);
                     cp_async16(&sm.ex.xj[st][cand][4 * sub], in ? cp[i] + dim0 : cp[i], in ? 16u : 0u);
                 }
             } else {
-                const uint32_t dp = dim0 + qd;
+                const uint32_t dp = dim0 + (uint32_t)lane;
                 const uint32_t bytes = dp < d ? 4u : 0u;
-                for (uint32_t i = 0; i < RR_SLICE / 2; ++i) {
-                    const uint32_t cand = 2 * i + ((uint32_t)lane >> 4);
+                for (uint32_t cand = 0; cand < 32; ++cand) {
                     const float *src = x + (size_t)sm.ex.cj[cand] * d + (bytes ? dp : 0u);
-                    cp_async4(&sm.ex.xj[st][cand][qd], src, bytes);
+                    cp_async4(&sm.ex.xj[st][cand][lane], src, bytes);
                 }
             }
-            const bool qin = dim0 + qd < d;
+            const bool qin = dim0 + (uint32_t)lane < d;
 #pragma unroll
-            for (int h = 0; h < 2; ++h)
-                if (qa + 2 * h < nr)
-                    cp_async4(&sm.ex.xi[st][qa + 2 * h][qd], qin ? qp[h] + dim0 : qp[h] - qd, qin ? 4u : 0u);
+            for (int a = 0; a < RR_QROWS; ++a)
+                if ((uint32_t)a < nr) cp_async4(&sm.ex.xi[st][a][lane], qin ? qp[a] + dim0 : qp[a] - lane, qin ? 4u : 0u);
         };
 
         for (uint32_t c = 0; c + 1 < RR_STAGES; ++c) {
             if (c < nch) issue(c, c);
             cp_async_commit();
         }
-        double acc[RR_NC];
-#pragma unroll
-        for (int c = 0; c < RR_NC; ++c) acc[c] = 0.0;
+        double acc = 0.0;
         for (uint32_t c = 0; c < nch; ++c) {
             if (c + RR_STAGES - 1 < nch) issue(c + RR_STAGES - 1, (c + RR_STAGES - 1) % RR_STAGES);
             cp_async_commit();  // possibly empty: keeps the group count uniform
             cp_async_wait<RR_STAGES - 1>();
             __syncwarp();
             const uint32_t st = c % RR_STAGES;
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-                if (qa + 2 * h < nr) sm.ex.xid[qa + 2 * h][qd] = (double)sm.ex.xi[st][qa + 2 * h][qd];
+            for (uint32_t a = 0; a < nr; ++a) sm.ex.xid[a][lane] = (double)sm.ex.xi[st][a][lane];
             __syncwarp();
-            const double *xv[RR_NC];
-            const float *yv[RR_NC];
-#pragma unroll
-            for (int h = 0; h < RR_NC; ++h) {
-                xv[h] = sm.ex.xid[ri[h]];
-                yv[h] = sm.ex.xj[st][32 * h + lane];
-            }
+            const double *xiv = sm.ex.xid[ri];
+            const float *xjv = sm.ex.xj[st][lane];
             const uint32_t tmax = min((uint32_t)RR_CH, d - c * RR_CH);
             if (tmax == RR_CH) {
-                // each chain adds its dimensions in order; the chains interleave
 #pragma unroll
                 for (int q = 0; q < RR_CH / 4; ++q) {
-                    float4 y[RR_NC];
-                    double2 a0[RR_NC], a1[RR_NC];
-#pragma unroll
-                    for (int h = 0; h < RR_NC; ++h) {
-                        y[h] = *reinterpret_cast<const float4 *>(yv[h] + 4 * q);
-                        a0[h] = *reinterpret_cast<const double2 *>(xv[h] + 4 * q);
-                        a1[h] = *reinterpret_cast<const double2 *>(xv[h] + 4 * q + 2);
-                    }
-#pragma unroll
-                    for (int h = 0; h < RR_NC; ++h) acc[h] = step<METRIC>(acc[h], a0[h].x, (double)y[h].x);
-#pragma unroll
-                    for (int h = 0; h < RR_NC; ++h) acc[h] = step<METRIC>(acc[h], a0[h].y, (double)y[h].y);
-#pragma unroll
-                    for (int h = 0; h < RR_NC; ++h) acc[h] = step<METRIC>(acc[h], a1[h].x, (double)y[h].z);
-#pragma unroll
-                    for (int h = 0; h < RR_NC; ++h) acc[h] = step<METRIC>(acc[h], a1[h].y, (double)y[h].w);
+                    const float4 y = *reinterpret_cast<const float4 *>(xjv + 4 * q);
+                    const double2 a0 = *reinterpret_cast<const double2 *>(xiv + 4 * q);
+                    const double2 a1 = *reinterpret_cast<const double2 *>(xiv + 4 * q + 2);
+                    acc = step<METRIC>(acc, a0.x, (double)y.x);
+                    acc = step<METRIC>(acc, a0.y, (double)y.y);
+                    acc = step<METRIC>(acc, a1.x, (double)y.z);
+                    acc = step<METRIC>(acc, a1.y, (double)y.w);
                 }
             } else {
-                for (uint32_t t = 0; t < tmax; ++t) {
-#pragma unroll
-                    for (int h = 0; h < RR_NC; ++h) acc[h] = step<METRIC>(acc[h], xv[h][t], (double)yv[h][t]);
-                }
+                for (uint32_t t = 0; t < tmax; ++t) acc = step<METRIC>(acc, xiv[t], (double)xjv[t]);
             }
             __syncwarp();
         }
-#pragma unroll
-        for (int c = 0; c < RR_NC; ++c) {
-            if (!act[c]) continue;
-            const uint32_t row = rowc[c], j = jc[c];
+        if (active) {
             float dist;
             if (j == row) {
                 dist = 0.0f;  // src/knn.rs:38-39
             } else if (METRIC == HM_METRIC_EUCLIDEAN) {
-                dist = __double2float_rn(__dsqrt_rn(acc[c]));
+                dist = __double2float_rn(__dsqrt_rn(acc));
             } else {
-                const double q = __ddiv_rn(acc[c], __dmul_rn(J.rnorm[row], J.rnorm[j]));
+                const double q = __ddiv_rn(acc, __dmul_rn(J.rnorm[row], J.rnorm[j]));
                 const double r = __dsub_rn(1.0, q);
                 dist = (r > 0.0) ? __double2float_rn(r) : 0.0f;
             }
-            *slot[c] = make_key(dist, j);
+            *slot = make_key(dist, j);
         }
         __syncwarp();
         s = end;

@@ -387,6 +387,10 @@ HM_API int hm_abi_version(void);
  * holomap_b200/autotune.py (holomap_b200/autotune_table.json); plain where
  * no screen applies (manhattan, k > 64, d > 2048). */
 HM_API int hm_autotune_path(uint64_t n, uint32_t d, uint32_t k, int metric);
+/* The same for a job planned in a batch of several (hm_batch_*, the serving
+ * context's batches): the table measured on batches of jobs of each shape,
+ * where the screens' fixed per-call costs are shared. */
+HM_API int hm_autotune_path_batched(uint64_t n, uint32_t d, uint32_t k, int metric);
 /* Autotuner sweep hook (no reference counterpart): while seed_div is nonzero,
  * screened plans made on this thread sample 1/seed_div of the columns in the
  * screen's threshold pass instead of the table's fraction; 0 restores the

@@ -112,9 +112,11 @@ def test_autotune_table_is_the_committed_measurement():
     it), and the generated table is current."""
     from holomap_b200 import autotune
     doc = _autotune_doc()
-    choice, gn, gd, gk = autotune.table_from(doc)
+    choice, batch, gn, gd, gk = autotune.table_from(doc)
     for (metric, k, d, n), (path, *_) in choice.items():
         assert hm.autotune_path(n, d, k, metric) == hm.KnnPath.parse(path), (metric, k, d, n)
+    for (metric, k, d, n), (path, *_) in batch.items():
+        assert hm.autotune_path(n, d, k, metric, batched=True) == hm.KnnPath.parse(path), (metric, k, d, n)
     import tempfile
     from pathlib import Path
     with tempfile.TemporaryDirectory() as t:
