@@ -563,6 +563,7 @@ static int bind_batch(hm_batch &B, void *d_ws, size_t bytes, cudaStream_t s) {
         J.csum = P.group >= 0 ? at<double>(ws, P.off_csum) : nullptr;
         J.ovf_list = P.group >= 0 ? at<uint32_t>(ws, P.off_ovf) : nullptr;
         J.cnt = at<JobCounters>(ws, B.off_counters) + j;
+        J.out = J.cnt;
         at<JobDev>(host, B.off_jobs)[j] = J;
         row_starts[j + 1] = row_starts[j] + J.n;
     }
@@ -1032,6 +1033,7 @@ int hm_smooth_knn_device(const float *d_dists, uint64_t n, uint32_t k, float *d_
     J.rho = d_rho;
     J.target = std::log2((double)k);  // src/smooth_knn.rs:25 (platform log2)
     J.cnt = reinterpret_cast<JobCounters *>(w + align256(sizeof(JobDev)));
+    J.out = J.cnt;
     J.zero_rows = reinterpret_cast<uint32_t *>(w + align256(sizeof(JobDev)) + align256(sizeof(JobCounters)));
     JobDev *jd = reinterpret_cast<JobDev *>(w);
     write_smooth_job_kernel<<<1, 32, 0, s>>>(jd, J);
@@ -1068,6 +1070,7 @@ int hm_smooth_knn_rows_device(const float *d_dists, uint64_t n, uint32_t k, uint
     J.rho = d_rho - row_begin;
     J.target = std::log2((double)k);  // src/smooth_knn.rs:25 (platform log2)
     J.cnt = reinterpret_cast<JobCounters *>(w + align256(sizeof(JobDev)));
+    J.out = J.cnt;
     J.zero_rows = reinterpret_cast<uint32_t *>(w + align256(sizeof(JobDev)) + align256(sizeof(JobCounters)));
     JobDev *jd = reinterpret_cast<JobDev *>(w);
     write_smooth_job_kernel<<<1, 32, 0, s>>>(jd, J);

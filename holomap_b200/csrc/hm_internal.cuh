@@ -164,6 +164,9 @@ struct JobCounters {
     unsigned long long emitted;     // candidates the screen wrote
     uint32_t band_max_bits;  // widest keep band (binary32 bits)
     uint32_t error_code;     // nonzero if a bounded wait gave up
+    uint32_t escalate;       // 1: the job's screen was too coarse for its data; its
+                             // split-BF16 copy produced the rows (see JobDev::gate)
+    uint32_t escalate_rows;  // rows whose band exceeded the escalation share of tau1
     // screen prep maxima (non-negative doubles as bits): |u|, |e|, |r|,
     // |A row|, |B row|, |u|^2, largest centred |x - mu|^2; then zero rows
     unsigned long long maxb[8];
@@ -200,8 +203,26 @@ struct JobDev {
     double *mu, *csum;           // euclidean column mean and its partial sums
     uint32_t csum_blocks, csum_rows;
     uint32_t *ovf_list;          // n (job-local rows)
-    JobCounters *cnt;
+    JobCounters *cnt;            // the job's working counters (screen prep maxima)
+    JobCounters *out;            // where its reported counts go (the original's for a copy)
+    // Escalation: a job screened in BF16 or TF32 may carry a split-BF16 copy
+    // (a second job entry on the same points and outputs).  After its
+    // threshold pass a kernel decides, from the rows' bands against their
+    // thresholds, whether the coarse screen would keep most of the dataset;
+    // then the copy runs and the original's remaining kernels step aside.
+    // gate: the original's escalate flag (null: always active); the job runs
+    // while *gate == gate_on (the original 0, the copy 1).
+    const uint32_t *gate;
+    uint32_t gate_on;
+    uint32_t escalation;         // the original: 1 if it has a copy to hand over to
 };
+
+// Whether a job's kernels run: always, unless it takes part in an
+// escalation and its side is not the one the flag selects.  The flag is
+// written once, between launches (never while a kernel reading it runs).
+__device__ __forceinline__ bool job_active(const JobDev &J) {
+    return !J.gate || *(volatile const uint32_t *)J.gate == J.gate_on;
+}
 
 // Host-side decomposition of an all-rows / item / group index into its job:
 // `starts` holds njobs + 1 ascending offsets.

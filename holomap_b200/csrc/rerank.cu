@@ -244,7 +244,7 @@ __device__ __forceinline__ uint32_t select_row(const JobDev &J, const GroupDev &
     const bool ovf = __any_sync(0xffffffffu, G.force[gr] != 0 || ((uint32_t)lane < lists && myc > list_cap(J, lane)));
     if (ovf) {
         if (lane == 0) {
-            const uint32_t at = atomicAdd(&J.cnt->ovf_count, 1u);
+            const uint32_t at = atomicAdd(&J.out->ovf_count, 1u);
             J.ovf_list[at] = row;
         }
         return 0;
@@ -373,8 +373,8 @@ __global__ void __launch_bounds__(RS_WARPS * 32, 4) rr_select_kernel(const JobDe
             mx = max(mx, s_kept[w]);
         }
         if (sum) {
-            atomicAdd(&J.cnt->candidates, (unsigned long long)sum);
-            atomicMax(&J.cnt->max_row, mx);
+            atomicAdd(&J.out->candidates, (unsigned long long)sum);
+            atomicMax(&J.out->max_row, mx);
         }
     }
 }

@@ -246,6 +246,23 @@ __device__ __forceinline__ void tmem_ld32_issue(uint32_t taddr, uint32_t (&v)[32
         : "r"(taddr));
 }
 
+__device__ __forceinline__ void tmem_ld16_issue(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32"
+        " {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
+          "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
+          "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld_wait16(uint32_t (&v)[16]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]),
+                   "+r"(v[6]), "+r"(v[7]), "+r"(v[8]), "+r"(v[9]), "+r"(v[10]), "+r"(v[11]),
+                   "+r"(v[12]), "+r"(v[13]), "+r"(v[14]), "+r"(v[15])
+                 :
+                 : "memory");
+}
 __device__ __forceinline__ void tmem_ld_wait(uint32_t (&v)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;"
                  : "+r"(v[0]), "+r"(v[1]), "+r"(v[2]), "+r"(v[3]), "+r"(v[4]), "+r"(v[5]),
@@ -389,7 +406,7 @@ __global__ void __launch_bounds__(sc_threads(PASS), 1)
                 if (PAIR || a_res) {
                     // the previous unit's MMAs must be done with the A block
                     if (un > 0 && !mbar_wait(smem_u32(aempty), (un - 1) & 1, abort_flag)) {
-                        raise_error(abort_flag, &J.cnt->error_code, SC_ERR_PRODUCER, peer_abort);
+                        raise_error(abort_flag, &J.out->error_code, SC_ERR_PRODUCER, peer_abort);
                         ok = false;
                         break;
                     }
@@ -409,7 +426,7 @@ __global__ void __launch_bounds__(sc_threads(PASS), 1)
                     for (uint32_t ks = 0; ks < J.k_stages; ++ks, ++it) {
                         const uint32_t s = it % NST, r = it / NST;
                         if (!mbar_wait(smem_u32(&empty[s]), (r & 1) ^ 1, abort_flag)) {
-                            raise_error(abort_flag, &J.cnt->error_code, SC_ERR_PRODUCER, peer_abort);
+                            raise_error(abort_flag, &J.out->error_code, SC_ERR_PRODUCER, peer_abort);
                             ok = false;
                             break;
                         }
@@ -439,22 +456,22 @@ __global__ void __launch_bounds__(sc_threads(PASS), 1)
                 for (uint32_t t = issued > NST ? issued - NST : 0; t < issued; ++t) {
                     const uint32_t s = t % NST, r = t / NST;
                     if (!mbar_wait(smem_u32(&empty[s]), r & 1, abort_flag, true)) {
-                        raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN, peer_abort);
+                        raise_error(abort_flag, &jobs[G.job_ids[0]].out->error_code, SC_ERR_DRAIN, peer_abort);
                         break;
                     }
                 }
                 if (un > 0 && !mbar_wait(smem_u32(aempty), (un - 1) & 1, abort_flag, true))
-                    raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN, peer_abort);
+                    raise_error(abort_flag, &jobs[G.job_ids[0]].out->error_code, SC_ERR_DRAIN, peer_abort);
             } else {
                 // drain: the last A block must have landed before the CTA exits
                 if (a_res && un > 0 && !mbar_wait(smem_u32(afull), (un - 1) & 1, abort_flag, true))
-                    raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN, peer_abort);
+                    raise_error(abort_flag, &jobs[G.job_ids[0]].out->error_code, SC_ERR_DRAIN, peer_abort);
                 // drain: every issued stage must have landed before the CTA exits
                 const uint32_t issued = it;
                 for (uint32_t t = issued > NST ? issued - NST : 0; t < issued; ++t) {
                     const uint32_t s = t % NST, r = t / NST;
                     if (!mbar_wait(smem_u32(&full[s]), r & 1, abort_flag, true)) {
-                        raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN, peer_abort);
+                        raise_error(abort_flag, &jobs[G.job_ids[0]].out->error_code, SC_ERR_DRAIN, peer_abort);
                         break;
                     }
                 }
@@ -472,7 +489,7 @@ __global__ void __launch_bounds__(sc_threads(PASS), 1)
                 const JobDev &J = jobs[ut.job];
                 if (PAIR || a_res) {
                     if (!mbar_wait(smem_u32(afull), un & 1, abort_flag)) {
-                        raise_error(abort_flag, &J.cnt->error_code, SC_ERR_MMA_FULL, peer_abort);
+                        raise_error(abort_flag, &J.out->error_code, SC_ERR_MMA_FULL, peer_abort);
                         ok = false;
                         break;
                     }
@@ -481,7 +498,7 @@ __global__ void __launch_bounds__(sc_threads(PASS), 1)
                 for (uint32_t ct = ut.ct_begin; ok && ct < ut.ct_end; ++ct, ++tile) {
                     const uint32_t buf = tile & 1, use = tile >> 1;
                     if (!mbar_wait(smem_u32(&acce[buf]), (use & 1) ^ 1, abort_flag)) {
-                        raise_error(abort_flag, &J.cnt->error_code, SC_ERR_MMA_ACC, peer_abort);
+                        raise_error(abort_flag, &J.out->error_code, SC_ERR_MMA_ACC, peer_abort);
                         ok = false;
                         break;
                     }
@@ -490,7 +507,7 @@ __global__ void __launch_bounds__(sc_threads(PASS), 1)
                     for (uint32_t ks = 0; ks < J.k_stages; ++ks, ++it) {
                         const uint32_t s = it % NST, r = it / NST;
                         if (!mbar_wait(smem_u32(&full[s]), r & 1, abort_flag)) {
-                            raise_error(abort_flag, &J.cnt->error_code, SC_ERR_MMA_FULL, peer_abort);
+                            raise_error(abort_flag, &J.out->error_code, SC_ERR_MMA_FULL, peer_abort);
                             ok = false;
                             break;
                         }
@@ -515,10 +532,10 @@ __global__ void __launch_bounds__(sc_threads(PASS), 1)
             if (it > 0) {
                 const uint32_t s = (it - 1) % NST, r = (it - 1) / NST;
                 if (!mbar_wait(smem_u32(&empty[s]), r & 1, abort_flag, true))
-                    raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN, peer_abort);
+                    raise_error(abort_flag, &jobs[G.job_ids[0]].out->error_code, SC_ERR_DRAIN, peer_abort);
             }
             if ((PAIR || a_res) && un > 0 && !mbar_wait(smem_u32(aempty), (un - 1) & 1, abort_flag, true))
-                raise_error(abort_flag, &jobs[G.job_ids[0]].cnt->error_code, SC_ERR_DRAIN, peer_abort);
+                raise_error(abort_flag, &jobs[G.job_ids[0]].out->error_code, SC_ERR_DRAIN, peer_abort);
         }
         __syncwarp();
     } else {
@@ -599,7 +616,7 @@ __global__ void __launch_bounds__(sc_threads(PASS), 1)
                 }
                 const bool got = mbar_wait(smem_u32(&accf[buf]), use & 1, abort_flag);
                 if (!__all_sync(0xffffffffu, got)) {
-                    raise_error(abort_flag, &J.cnt->error_code, SC_ERR_EPILOGUE, peer_abort);
+                    raise_error(abort_flag, &J.out->error_code, SC_ERR_EPILOGUE, peer_abort);
                     ok = false;
                     break;
                 }
@@ -853,14 +870,109 @@ __global__ void __launch_bounds__(sc_threads(PASS), 1)
                     }
                 };
                 if constexpr (EW >= 16) {
-                    // four warps per scheduler hide the load latency: one
-                    // chunk of registers
-                    uint32_t va[32];
+                    // the full emission pass (96 registers a thread): 16-column
+                    // loads, the next in flight while this one is tested
+                    const uint32_t cap = J.cap;
+                    auto emit16 = [&](uint32_t (&v)[16], uint32_t j0) {
+                        float (&c)[16] = reinterpret_cast<float (&)[16]>(v);
+                        const bool full = j0 + 16 <= n;
+                        const bool self_here = diag && (row - j0 < 16u);
+                        auto put = [&](uint32_t pm, int g, bool raw) {
+                            while (pm) {
+                                const int e = __ffs(pm) - 1;
+                                pm &= pm - 1;
+                                const float a0 = (e & 1) ? c[8 * g + 1] : c[8 * g];
+                                const float a1 = (e & 1) ? c[8 * g + 3] : c[8 * g + 2];
+                                const float a2 = (e & 1) ? c[8 * g + 5] : c[8 * g + 4];
+                                const float a3 = (e & 1) ? c[8 * g + 7] : c[8 * g + 6];
+                                const float b0 = (e & 2) ? a1 : a0, b1 = (e & 2) ? a3 : a2;
+                                float x = (e & 4) ? b1 : b0;
+                                if (raw) x = __fsub_rn(1.0f, x);
+                                if (cnt < cap)
+                                    cand[cnt] = ((unsigned long long)__float_as_uint(x) << 32) | (j0 + 8 * g + e);
+                                ++cnt;
+                            }
+                        };
+                        if (fast_cos && full && !self_here) {
+                            // c = 1 - v <= thr  <=>  v >= vstar (a superset)
+                            float gm[2];
+#pragma unroll
+                            for (int g = 0; g < 2; ++g) {
+                                float x = c[8 * g];
+#pragma unroll
+                                for (int e = 1; e < 8; ++e) x = fmaxf(x, c[8 * g + e]);
+                                gm[g] = x;
+                            }
+                            if (valid && fmaxf(gm[0], gm[1]) >= vstar) {
+#pragma unroll
+                                for (int g = 0; g < 2; ++g) {
+                                    if (gm[g] >= vstar) {
+                                        uint32_t pm = 0;
+#pragma unroll
+                                        for (int e = 0; e < 8; ++e) pm |= (c[8 * g + e] >= vstar) ? (1u << e) : 0u;
+                                        put(pm, g, true);
+                                    }
+                                }
+                            }
+                            return;
+                        }
+                        // exact screened values (columns past n: +inf; the row itself: 0)
+                        if (fast_cos) {
+#pragma unroll
+                            for (int t = 0; t < 16; ++t) c[t] = __fsub_rn(1.0f, c[t]);
+                        } else {
+                            const float4 *ctp = reinterpret_cast<const float4 *>(colterm + j0);
+#pragma unroll
+                            for (int q = 0; q < 4; ++q) {
+                                const float4 cq = __ldg(ctp + q);
+                                const float cs[4] = {cq.x, cq.y, cq.z, cq.w};
+#pragma unroll
+                                for (int e = 0; e < 4; ++e)
+                                    c[4 * q + e] = __fsub_rn(__fadd_rn(rowterm, cs[e]), __fmul_rn(scale, c[4 * q + e]));
+                            }
+                        }
+                        if (!full) {
+#pragma unroll
+                            for (int t = 0; t < 16; ++t)
+                                if (j0 + t >= n) c[t] = INF;
+                        }
+                        if (self_here) {
+#pragma unroll
+                            for (int t = 0; t < 16; ++t)
+                                if (j0 + t == row) c[t] = 0.0f;
+                        }
+                        float gm[2];
+#pragma unroll
+                        for (int g = 0; g < 2; ++g) {
+                            float x = c[8 * g];
+#pragma unroll
+                            for (int e = 1; e < 8; ++e) x = fminf(x, c[8 * g + e]);
+                            gm[g] = x;
+                        }
+                        if (valid && !(fminf(gm[0], gm[1]) > thr)) {
+#pragma unroll
+                            for (int g = 0; g < 2; ++g) {
+                                if (!(gm[g] > thr)) {
+                                    uint32_t pm = 0;
+#pragma unroll
+                                    for (int e = 0; e < 8; ++e)
+                                        pm |= (!(c[8 * g + e] > thr) && j0 + 8 * g + e < n) ? (1u << e) : 0u;
+                                    put(pm, g, false);
+                                }
+                            }
+                        }
+                    };
+                    uint32_t va[16], vb[16];
+                    tmem_ld16_issue(t_base, va);
+                    tmem_ld_wait16(va);
 #pragma unroll 1
-                    for (uint32_t ch = 0; ch < SEGW / 32; ++ch) {
-                        tmem_ld32_issue(t_base + ch * 32, va);
-                        tmem_ld_wait(va);
-                        process(va, ch);
+                    for (uint32_t ch = 0; ch < SEGW / 16; ch += 2) {
+                        tmem_ld16_issue(t_base + (ch + 1) * 16, vb);
+                        emit16(va, c_base + ch * 16);
+                        tmem_ld_wait16(vb);
+                        if (ch + 2 < SEGW / 16) tmem_ld16_issue(t_base + (ch + 2) * 16, va);
+                        emit16(vb, c_base + (ch + 1) * 16);
+                        if (ch + 2 < SEGW / 16) tmem_ld_wait16(va);
                     }
                 } else {
                     // two warps per scheduler: the next chunk loads while
@@ -899,7 +1011,7 @@ __global__ void __launch_bounds__(sc_threads(PASS), 1)
             } else {
                 if (valid) G.cand_cnt[list] = cnt;
                 const uint32_t e = __reduce_add_sync(0xffffffffu, (valid ? cnt : 0u) + colsum);
-                if (lane == 0 && e) atomicAdd(&J.cnt->emitted, (unsigned long long)e);
+                if (lane == 0 && e) atomicAdd(&J.out->emitted, (unsigned long long)e);
             }
         }
     }

@@ -299,7 +299,7 @@ __global__ void band_kernel(const JobDev *__restrict__ jobs, const GroupDev *__r
     uint32_t bits = 0;
     if (real) bits = band_of_row(J, G, gr);
     bits = __reduce_max_sync(0xffffffffu, bits);  // non-negative floats order like their bits
-    if ((threadIdx.x & 31) == 0 && bits) atomicMax(&J.cnt->band_max_bits, bits);
+    if ((threadIdx.x & 31) == 0 && bits) atomicMax(&J.out->band_max_bits, bits);
 }
 
 
