@@ -206,6 +206,7 @@ SIGNATURES = {
     "hm_tuning_override": (_i32, [_i32]),
     "hm_tuning_symmetric": (_i32, [_i32]),
     "hm_tuning_pair": (_i32, [_i32]),
+    "hm_tuning_escalation": (_i32, [_i32]),
     "hm_timing_enable": (_i32, [_i32]),
     "hm_timing_read": (_i32, [_i32, _vp, _vp, _i32]),
     "hm_launch_count": (_u64, []),

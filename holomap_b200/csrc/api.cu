@@ -102,6 +102,8 @@ struct JobPlan {
     bool sym = false;
     uint32_t ept = 0, elists = 0;
     uint64_t eslot0 = 0;
+    // escalation: the job's split-BF16 copy (clone), or the job a copy is of
+    int clone = -1, clone_of = -1;
 };
 
 struct GroupPlan {
@@ -116,6 +118,7 @@ struct GroupPlan {
     bool any_sym = false;
     bool pair = false;  // emission pass in the 2-SM form (units of 256 rows)
     bool pair_vetoed = false;  // the autotuner table prefers one CTA per row block for a job
+    bool any_escalation = false;  // a job of the group has a split-BF16 escalation copy
     uint32_t egrid = 0, stage_cap = 0;
     size_t off_opa = 0, off_opb = 0, off_rowstat = 0, off_rowterm = 0, off_colterm = 0;
     size_t off_band = 0, off_force = 0, off_rowthr = 0, off_cand = 0, off_cnt = 0, off_topk = 0;
@@ -131,7 +134,8 @@ struct GroupPlan {
 }  // namespace hm
 
 struct hm_batch {
-    std::vector<hm::JobPlan> jobs;
+    std::vector<hm::JobPlan> jobs;  // the caller's jobs, then their escalation copies
+    uint32_t user_jobs = 0;
     hm::GroupPlan groups[3];  // bf16, tf32, split bf16
     uint32_t all_rows = 0, kmax = 0, kpl_all = 1, kpl_plain[3] = {1, 1, 1}, kpl_fb[3] = {1, 1, 1};
     std::vector<uint2> items[3];       // exact-path work per metric
@@ -166,11 +170,48 @@ static int group_of_path(int path) {
 
 // `ranges` (optional): 2 per job, the job's query rows [begin, end); every
 // point stays a column.  NULL: all rows.
-static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const uint64_t *ranges = nullptr) {
-    if (njobs == 0) return set_error(HM_ERR_INVALID, "empty batch");
-    if (njobs > (1u << 16)) return set_error(HM_ERR_UNSUPPORTED, "more than 65536 jobs");
+static int plan_batch(const hm_job *user_specs, uint32_t user_jobs, hm_batch &B,
+                      const uint64_t *user_ranges = nullptr) {
+    if (user_jobs == 0) return set_error(HM_ERR_INVALID, "empty batch");
+    if (user_jobs > (1u << 16)) return set_error(HM_ERR_UNSUPPORTED, "more than 65536 jobs");
     const uint32_t G = (uint32_t)sm_count();
+    const bool batched = user_jobs > 1;
+    // Escalation copies: a job left to the autotuner whose choice is the BF16
+    // or TF32 screen also gets a split-BF16 copy on the same points and
+    // outputs (no smooth-kNN of its own), appended after the caller's jobs;
+    // on the device one of the two finishes the job.
+    std::vector<hm_job> ext(user_specs, user_specs + user_jobs);
+    std::vector<uint64_t> ext_ranges;
+    if (user_ranges) ext_ranges.assign(user_ranges, user_ranges + 2 * (size_t)user_jobs);
+    std::vector<uint32_t> clone_src;
+    if (tuning_escalation()) {
+        for (uint32_t j = 0; j < user_jobs; ++j) {
+            const hm_job &s = user_specs[j];
+            if (s.path != HM_PATH_AUTO || validate_shape(s.n, s.d, s.k, s.metric) != HM_OK) continue;
+            const int p = autotune_choice(s.n, s.d, s.k, s.metric, nullptr, nullptr, nullptr, batched);
+            if (p != HM_PATH_SCREEN_BF16 && p != HM_PATH_SCREEN_TF32) continue;
+            hm_job c = s;
+            c.path = HM_PATH_SCREEN_BF16X3;
+            c.sigma_out = nullptr;
+            c.rho_out = nullptr;
+            ext.push_back(c);
+            if (user_ranges) {
+                ext_ranges.push_back(user_ranges[2 * j]);
+                ext_ranges.push_back(user_ranges[2 * j + 1]);
+            }
+            clone_src.push_back(j);
+        }
+        clear_error();
+    }
+    const hm_job *specs = ext.data();
+    const uint64_t *ranges = user_ranges ? ext_ranges.data() : nullptr;
+    const uint32_t njobs = (uint32_t)ext.size();
+    B.user_jobs = user_jobs;
     B.jobs.assign(njobs, JobPlan{});
+    for (uint32_t c = 0; c < (uint32_t)clone_src.size(); ++c) {
+        B.jobs[clone_src[c]].clone = (int)(user_jobs + c);
+        B.jobs[user_jobs + c].clone_of = (int)clone_src[c];
+    }
     for (int g = 0; g < 3; ++g) B.groups[g] = GroupPlan{};
     B.groups[0].kind = SCREEN_KIND_BF16;
     B.groups[1].kind = SCREEN_KIND_TF32;
@@ -187,7 +228,7 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
         HM_TRY(validate_shape(s.n, s.d, s.k, s.metric));
         int path = s.path;
         if (path == HM_PATH_AUTO)
-            path = autotune_choice(s.n, s.d, s.k, s.metric, nullptr, nullptr, nullptr, njobs > 1);
+            path = autotune_choice(s.n, s.d, s.k, s.metric, nullptr, nullptr, nullptr, batched);
         if (path < HM_PATH_PLAIN || path > HM_PATH_SCREEN_BF16X3)
             return set_error(HM_ERR_INVALID, "unknown path %d", s.path);
         if (path != HM_PATH_PLAIN && !screen_capable(s.d, s.k, s.metric))
@@ -285,7 +326,9 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
             uint32_t seed_div = 8;
             bool sym_ok = true, pair_ok = true;
             autotune_choice(P.spec.n, P.spec.d, P.spec.k, P.spec.metric, &seed_div, &sym_ok, &pair_ok,
-                            njobs > 1);
+                            batched);
+            if (P.clone >= 0 || P.clone_of >= 0) sym_ok = false;  // an escalation pair runs the full pass
+            if (P.clone >= 0) Gp.any_escalation = true;
             if (!pair_ok) Gp.pair_vetoed = true;
             const uint64_t seed_cols = std::max<uint64_t>(P.spec.n / std::max<uint32_t>(seed_div, 1), 2048);
             P.seed_tiles = std::min<uint32_t>(
@@ -329,6 +372,10 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
             const double per_list = (double)P.spec.n / ((double)per_part * eparts);
             const double expect = 1.5 * P.spec.k * (2.0 + std::log(std::fmax(1.0, per_list / P.spec.k)));
             P.cap = std::min<uint32_t>(std::max<uint32_t>(pow2ceil((uint32_t)expect), 128), 4096);
+            // an escalation copy runs only where the coarse screen kept most of
+            // the dataset, and its band is about 2^-16 of the norms: the
+            // smallest lists suffice (an overflowing row takes the exact path)
+            if (P.clone_of >= 0) P.cap = 128;
             P.eslot0 = Gp.elists;
             Gp.elists += P.spec.n * (uint64_t)P.elists;
             P.cand0 = Gp.cand;
@@ -380,7 +427,9 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
             for (uint32_t gi = P.q0 / PL_BM; gi < g_end; ++gi)
                 for (uint32_t sp = 0; sp < P.splits; ++sp) B.items[m].push_back(make_uint2(j, gi << 6 | sp));
             B.kpl_plain[m] = std::max<uint32_t>(B.kpl_plain[m], (uint32_t)kpl_for_k(P.spec.k));
-        } else {
+        } else if (P.clone_of < 0) {
+            // (an escalation copy's fallback rows are the original's: same
+            // points, outputs and row list)
             B.fb_jobs[m].push_back(j);
             B.kpl_fb[m] = std::max<uint32_t>(B.kpl_fb[m], (uint32_t)kpl_for_k(P.spec.k));
         }
@@ -437,6 +486,18 @@ static int plan_batch(const hm_job *specs, uint32_t njobs, hm_batch &B, const ui
     for (uint32_t j = 0; j < njobs; ++j) {
         JobPlan &P = B.jobs[j];
         const uint64_t n = P.spec.n;
+        if (P.clone_of >= 0) {
+            // an escalation copy shares its original's norms, binary64 rows
+            // and overflow list (only one of the two reaches them)
+            const JobPlan &O = B.jobs[P.clone_of];
+            P.off_x64 = O.off_x64;
+            P.off_rnorm = O.off_rnorm;
+            P.off_zero_rows = O.off_zero_rows;
+            P.off_ovf = O.off_ovf;
+            P.off_mu = take((size_t)P.spec.d * sizeof(double));
+            P.off_csum = take((size_t)64 * P.spec.d * sizeof(double));
+            continue;
+        }
         P.off_x64 = take((size_t)P.n_pad * P.ldd * sizeof(double));  // exact path or fallback rows
         P.off_rnorm = take((size_t)P.n_pad * sizeof(double));
         P.off_zero_rows = take(n * sizeof(uint32_t));
@@ -564,6 +625,15 @@ static int bind_batch(hm_batch &B, void *d_ws, size_t bytes, cudaStream_t s) {
         J.ovf_list = P.group >= 0 ? at<uint32_t>(ws, P.off_ovf) : nullptr;
         J.cnt = at<JobCounters>(ws, B.off_counters) + j;
         J.out = J.cnt;
+        if (P.clone >= 0) {
+            J.gate = &J.cnt->escalate;
+            J.gate_on = 0;
+            J.escalation = 1;
+        } else if (P.clone_of >= 0) {
+            J.out = at<JobCounters>(ws, B.off_counters) + P.clone_of;
+            J.gate = &J.out->escalate;
+            J.gate_on = 1;
+        }
         at<JobDev>(host, B.off_jobs)[j] = J;
         row_starts[j + 1] = row_starts[j] + J.n;
     }
@@ -680,6 +750,7 @@ static int run_batch(hm_batch &B, cudaStream_t s) {
         HM_TRY(launch_screen_band(jobs, Gp.host, Gd, s));
         HM_TRY(launch_screen_gemm(jobs, Gp.host, Gd, Gp.kp, Gp.ta, Gp.tb, debug_dump_pointer(), 0, s));
         HM_TRY(launch_screen_threshold(jobs, Gp.host, Gd, Gp.kpl, s));
+        if (Gp.any_escalation) HM_TRY(launch_escalation(jobs, Gp.host, Gd, s));
         // lists no unit writes (parts a row block does not have) and the
         // column lists the scatter fills start empty
         HM_CUDA_TRY(cudaMemsetAsync(Gp.host.cand_cnt, 0, Gp.elists * sizeof(uint32_t), s));
@@ -717,7 +788,9 @@ static int run_batch(hm_batch &B, cudaStream_t s) {
 
 static void stats_from_counters(const hm_batch &B, uint32_t j, const JobCounters &c, hm_stats *st) {
     memset(st, 0, sizeof *st);
-    const JobPlan &P = B.jobs[j];
+    // an escalated job reports its split-BF16 copy's path (the copy's counts
+    // went to the job's own counters)
+    const JobPlan &P = (c.escalate && B.jobs[j].clone >= 0) ? B.jobs[B.jobs[j].clone] : B.jobs[j];
     st->path_used = P.path;
     st->col_splits = P.splits;
     st->zero_rho_rows = c.zero_count;
@@ -833,6 +906,19 @@ static hm_job one_job(const float *data, uint64_t n, uint32_t d, uint32_t k, int
     return j;
 }
 
+// Replaces a planned job's buffers (the plan only depended on which were
+// present) and those of its escalation copy, which shares the points and the
+// kNN outputs but never the smooth-kNN ones.
+static void set_job_buffers(hm_batch &B, uint32_t j, const hm_job &spec) {
+    B.jobs[j].spec = spec;
+    const int c = B.jobs[j].clone;
+    if (c < 0) return;
+    hm_job &cs = B.jobs[c].spec;
+    cs.data = spec.data;
+    cs.idx_out = spec.idx_out;
+    cs.dist_out = spec.dist_out;
+}
+
 static int host_pipeline(const float *data, uint64_t n, uint32_t d, uint32_t k, int metric,
                          int path, uint32_t *idx_out, float *dist_out, float *sigma_out,
                          float *rho_out, hm_stats *stats) {
@@ -859,9 +945,9 @@ static int host_pipeline(const float *data, uint64_t n, uint32_t d, uint32_t k, 
             HM_TRY(A.get(&d_rho, n * sizeof(float)));
         }
         HM_TRY(A.get(&ws, B.total));
-        B.jobs[0].spec = one_job(static_cast<float *>(d_data), n, d, k, metric, path,
-                                 static_cast<uint32_t *>(d_idx), static_cast<float *>(d_dist),
-                                 static_cast<float *>(d_sigma), static_cast<float *>(d_rho));
+        set_job_buffers(B, 0, one_job(static_cast<float *>(d_data), n, d, k, metric, path,
+                                      static_cast<uint32_t *>(d_idx), static_cast<float *>(d_dist),
+                                      static_cast<float *>(d_sigma), static_cast<float *>(d_rho)));
         HM_CUDA_TRY(cudaMemcpyAsync(d_data, data, n * d * sizeof(float), cudaMemcpyHostToDevice, s));
         HM_CUDA_TRY(cudaEventRecord(ctx->ev0, s));
         HM_TRY(bind_batch(B, ws, B.total, s));
@@ -1170,7 +1256,7 @@ int hm_batch_graph_launch(hm_batch *batch, void *stream) {
 int hm_batch_job_stats(const hm_batch *batch, uint32_t job, hm_stats *stats) {
     clear_error();
     if (!batch || !stats || !batch->ws) return set_error(HM_ERR_INVALID, "unbound batch or NULL stats");
-    if (job >= batch->jobs.size()) return set_error(HM_ERR_INVALID, "job %u out of range", job);
+    if (job >= batch->user_jobs) return set_error(HM_ERR_INVALID, "job %u out of range", job);
     JobCounters c{};
     HM_CUDA_TRY(cudaMemcpy(&c, batch->ws + batch->off_counters + job * sizeof(JobCounters), sizeof c,
                            cudaMemcpyDeviceToHost));
@@ -1179,7 +1265,7 @@ int hm_batch_job_stats(const hm_batch *batch, uint32_t job, hm_stats *stats) {
 }
 
 int hm_batch_job_path(const hm_batch *batch, uint32_t job) {
-    if (!batch || job >= batch->jobs.size()) return set_error(HM_ERR_INVALID, "job out of range");
+    if (!batch || job >= batch->user_jobs) return set_error(HM_ERR_INVALID, "job out of range");
     return batch->jobs[job].path;
 }
 

@@ -24,6 +24,7 @@ namespace hm {
 static thread_local uint32_t g_seed_override = 0;
 static thread_local bool g_symmetric = true;
 static thread_local bool g_pair = true;
+static thread_local bool g_escalation = true;
 
 template <size_t N>
 static size_t nearest_ratio(const uint32_t (&grid)[N], double v) {
@@ -63,6 +64,7 @@ int autotune_choice(uint64_t n, uint32_t d, uint32_t k, int metric, uint32_t *se
 }
 
 bool tuning_pair() { return g_pair; }
+bool tuning_escalation() { return g_escalation; }
 
 }  // namespace hm
 
@@ -91,6 +93,11 @@ int hm_tuning_symmetric(int on) {
 
 int hm_tuning_pair(int on) {
     g_pair = on != 0;
+    return HM_OK;
+}
+
+int hm_tuning_escalation(int on) {
+    g_escalation = on != 0;
     return HM_OK;
 }
 

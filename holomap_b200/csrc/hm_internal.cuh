@@ -246,6 +246,9 @@ int autotune_choice(uint64_t n, uint32_t d, uint32_t k, int metric, uint32_t *se
 // Whether screened plans made on this thread may run the emission pass in
 // the 2-SM form (hm_tuning_pair).
 bool tuning_pair();
+// Whether jobs left to the autotuner on the BF16 or TF32 screen carry a
+// split-BF16 escalation copy (hm_tuning_escalation).
+bool tuning_escalation();
 
 // ------------------------------------------------------------- plain path
 constexpr int PL_BM = 32;     // rows per CTA (8 warps x 4 rows)

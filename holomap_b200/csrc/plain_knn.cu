@@ -55,6 +55,8 @@ __global__ void __launch_bounds__(256) prep_jobs_kernel(const JobDev *__restrict
     const size_t stride = (size_t)nb * blockDim.x;
     const size_t t0 = (size_t)lb * blockDim.x + threadIdx.x;
     if (mode == PREP_X64_EXACT && J.path != HM_PATH_PLAIN) return;
+    // (an escalated job's fallback rows come from its copy's rerank: the
+    // original's row list and count, so no activity check here)
     if (mode == PREP_X64_FALLBACK && (J.path == HM_PATH_PLAIN || J.cnt->ovf_count == 0)) return;
     const size_t total = (size_t)J.n_pad * J.ldd;
     for (size_t t = t0; t < total; t += stride) {
@@ -82,9 +84,10 @@ __global__ void __launch_bounds__(NRM_WARPS * 32) check_norms_kernel(const JobDe
     const uint32_t ar0 = (blockIdx.x * NRM_WARPS + warp) * 32;
     if (ar0 >= rows) return;
     const uint32_t ar = ar0 + lane;
-    const bool mine = ar < rows;
-    const uint32_t jb = mine ? (row_starts ? find_job(row_starts, njobs, ar) : 0u) : 0u;
+    const uint32_t jb = ar < rows ? (row_starts ? find_job(row_starts, njobs, ar) : 0u) : 0u;
     const JobDev &J = jobs[jb];
+    // (an escalation copy's rows are its original's: checked there)
+    const bool mine = ar < rows && job_active(J);
     const uint32_t row = mine ? ar - J.arow0 : 0u;
     const uint32_t d = mine ? J.d : 0u;
     const float *xrow = J.x + (size_t)row * d;

@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(RS_WARPS * 32, 4) rr_select_kernel(const JobDe
     uint32_t c = 0;
     if (gr < G.rows) {
         const uint32_t row = gr - J.row0;
-        if (row < J.n && row >= J.q0 && row < J.q1) c = select_row<KPL>(J, G, gr, row, sm, lane);
+        if (row < J.n && row >= J.q0 && row < J.q1 && job_active(J)) c = select_row<KPL>(J, G, gr, row, sm, lane);
         if (lane == 0) G.row_cnt[gr] = c;
     }
     if (lane == 0) s_kept[warp] = c;
@@ -674,7 +674,7 @@ __global__ void __launch_bounds__(256) threshold_kernel(const JobDev *__restrict
     if (gr >= G.rows) return;
     const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
     const uint32_t row = gr - J.row0;
-    if (row < J.q0 || row >= J.q1) return;
+    if (row < J.q0 || row >= J.q1 || !job_active(J)) return;
     const uint32_t k = J.k, lists = 2 * J.parts;
     const size_t l0 = list_index(J, row, 0);
     // the row's lists' arrays are contiguous: lists x k values
@@ -697,6 +697,56 @@ __global__ void __launch_bounds__(256) threshold_kernel(const JobDev *__restrict
         }
     }
     if (lane == 0) G.rowthr[gr] = sel.tau == KEY_NONE ? ord32(__int_as_float(0x7f800000)) : (uint32_t)(sel.tau >> 32);
+}
+
+// Escalation decision (jobs with a split-BF16 copy), after the threshold
+// pass.  A row whose keep band exceeds half of its threshold tau1 (an upper
+// bound of its k-th screened value) would keep a share of the dataset set by
+// the screen's rounding, not by its neighbours; when more than a tenth of a
+// job's rows do, the job hands over to its copy.  Both outcomes return the
+// same bytes; the choice is only about time.
+constexpr float ESC_BAND_SHARE = 0.5f;
+constexpr uint32_t ESC_ROWS_DIV = 10;
+
+__global__ void __launch_bounds__(256) escalate_count_kernel(const JobDev *__restrict__ jobs,
+                                                             const GroupDev *__restrict__ Gp) {
+    const GroupDev &G = *Gp;
+    const uint32_t gr = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gr - (threadIdx.x & 31) >= G.rows) return;  // whole warps: 32 rows of one job
+    const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr - (threadIdx.x & 31))]];
+    if (!J.escalation) return;
+    const uint32_t row = gr - J.row0;
+    bool wide = false;
+    if (gr < G.rows && row < J.n && row >= J.q0 && row < J.q1 && !G.force[gr]) {
+        const float tau1 = unord32(G.rowthr[gr]);
+        wide = G.band[gr] > ESC_BAND_SHARE * tau1;
+    }
+    const uint32_t c = __popc(__ballot_sync(0xffffffffu, wide));
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(&J.cnt->escalate_rows, c);
+}
+
+__global__ void escalate_decide_kernel(const JobDev *__restrict__ jobs, const GroupDev *__restrict__ Gp) {
+    const GroupDev &G = *Gp;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= G.njobs) return;
+    const JobDev &J = jobs[G.job_ids[t]];
+    if (!J.escalation) return;
+    if ((unsigned long long)J.cnt->escalate_rows * ESC_ROWS_DIV > (unsigned long long)(J.q1 - J.q0)) {
+        J.cnt->escalate = 1;
+        J.cnt->band_max_bits = 0;  // the copy reports its own band
+    }
+}
+
+int launch_escalation(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, cudaStream_t s) {
+    if (G.rows == 0) return HM_OK;
+    ScopedKernelTimer timer(HM_KCLASS_SELECT, s);
+    escalate_count_kernel<<<(G.rows + 255) / 256, 256, 0, s>>>(jobs, Gd);
+    HM_CUDA_TRY(cudaGetLastError());
+    count_launch();
+    escalate_decide_kernel<<<(G.njobs + 127) / 128, 128, 0, s>>>(jobs, Gd);
+    HM_CUDA_TRY(cudaGetLastError());
+    count_launch();
+    return HM_OK;
 }
 
 int launch_screen_threshold(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t kpl,

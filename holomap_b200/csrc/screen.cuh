@@ -139,6 +139,9 @@ int launch_rerank(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uin
 // column-side candidates moved from the CTAs' staging into the rows' column
 // lists after it (grid: the emission pass's CTAs)
 int launch_emit_limits(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, cudaStream_t s);
+// After the threshold pass of a group holding jobs with an escalation copy:
+// sets each such job's escalate flag (JobCounters::escalate).
+int launch_escalation(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, cudaStream_t s);
 int launch_column_scatter(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd, uint32_t ctas,
                           cudaStream_t s);
 // the emission pass's grid (one CTA per SM, at most one per unit)

@@ -402,6 +402,7 @@ __global__ void __launch_bounds__(sc_threads(PASS), 1)
             for (uint32_t u = wid; ok && u < nunits; u += nworkers) {
                 const UnitTiles ut = unit_tiles(jobs, G, u, PASS);
                 const JobDev &J = jobs[ut.job];
+                if (!job_active(J)) continue;  // every role skips the same units
                 const uint32_t myrb = PAIR ? 2 * ut.rb + rank : ut.rb;  // this CTA's 128-row block
                 if (PAIR || a_res) {
                     // the previous unit's MMAs must be done with the A block
@@ -487,6 +488,7 @@ __global__ void __launch_bounds__(sc_threads(PASS), 1)
             for (uint32_t u = wid; ok && u < nunits; u += nworkers) {
                 const UnitTiles ut = unit_tiles(jobs, G, u, PASS);
                 const JobDev &J = jobs[ut.job];
+                if (!job_active(J)) continue;
                 if (PAIR || a_res) {
                     if (!mbar_wait(smem_u32(afull), un & 1, abort_flag)) {
                         raise_error(abort_flag, &J.out->error_code, SC_ERR_MMA_FULL, peer_abort);
@@ -551,6 +553,7 @@ __global__ void __launch_bounds__(sc_threads(PASS), 1)
         for (uint32_t u = wid; ok && u < nunits; u += nworkers) {
             const UnitTiles ut = unit_tiles(jobs, G, u, PASS);
             const JobDev &J = jobs[ut.job];
+            if (!job_active(J)) continue;
             const uint32_t n = J.n;
             const uint32_t myrb = PAIR ? 2 * ut.rb + rank : ut.rb;  // this CTA's 128-row block
             const uint32_t row = myrb * SC_BM + row_in_tile;  // job-local

@@ -38,7 +38,7 @@ constexpr uint32_t CSUM_BLOCKS = 64;  // column-sum partial blocks per euclidean
 __global__ void colsum_partial_kernel(const JobDev *__restrict__ jobs, const GroupDev *__restrict__ G) {
     const uint32_t g = blockIdx.x / CSUM_BLOCKS, b = blockIdx.x % CSUM_BLOCKS;
     const JobDev &J = jobs[G->job_ids[g]];
-    if (J.metric != HM_METRIC_EUCLIDEAN) return;
+    if (J.metric != HM_METRIC_EUCLIDEAN || !job_active(J)) return;
     const uint32_t per = (J.n + CSUM_BLOCKS - 1) / CSUM_BLOCKS;
     const uint32_t r0 = b * per, r1 = min(J.n, r0 + per);
     for (uint32_t c = threadIdx.x; c < J.d; c += blockDim.x) {
@@ -50,7 +50,7 @@ __global__ void colsum_partial_kernel(const JobDev *__restrict__ jobs, const Gro
 
 __global__ void colmean_kernel(const JobDev *__restrict__ jobs, const GroupDev *__restrict__ G) {
     const JobDev &J = jobs[G->job_ids[blockIdx.x]];
-    if (J.metric != HM_METRIC_EUCLIDEAN) return;
+    if (J.metric != HM_METRIC_EUCLIDEAN || !job_active(J)) return;
     for (uint32_t c = threadIdx.x; c < J.d; c += blockDim.x) {
         double s = 0.0;
         for (uint32_t b = 0; b < CSUM_BLOCKS; ++b) s += J.csum[(size_t)b * J.d + c];
@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(256) centred_norm_max_kernel(const JobDev *__r
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t gr0 = blockIdx.x * 32;
     const JobDev &J = jobs[G->job_ids[find_job(G->row_starts, G->njobs, gr0)]];
-    if (J.metric != HM_METRIC_EUCLIDEAN) return;  // uniform over the block
+    if (J.metric != HM_METRIC_EUCLIDEAN || !job_active(J)) return;  // uniform over the block
     double m = 0.0;
     for (uint32_t r = 0; r < 4; ++r) {
         const uint32_t row = gr0 + warp * 4 + r - J.row0;
@@ -122,6 +122,7 @@ __global__ void __launch_bounds__(256) operand_kernel(const JobDev *__restrict__
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint32_t gr0 = blockIdx.x * 32;
     const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr0)]];
+    if (!job_active(J)) return;  // uniform over the block (32 rows of one job)
     unsigned long long *maxb = J.cnt->maxb;
     double wmax[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     unsigned long long wzero = 0;
@@ -295,6 +296,7 @@ __global__ void band_kernel(const JobDev *__restrict__ jobs, const GroupDev *__r
     const uint32_t gr = blockIdx.x * blockDim.x + threadIdx.x;
     if (gr - (threadIdx.x & 31) >= G.rows) return;  // whole warps
     const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
+    if (!job_active(J)) return;  // uniform over the warp (32 rows of one job)
     const bool real = gr < G.rows && gr - J.row0 < J.n;  // not padding between jobs
     uint32_t bits = 0;
     if (real) bits = band_of_row(J, G, gr);

@@ -408,6 +408,15 @@ HM_API int hm_tuning_symmetric(int on);
  * each CTA loading half of every column tile).  Same results; on = 1 (the
  * default) restores the 2-SM form where a group can take it. */
 HM_API int hm_tuning_pair(int on);
+/* Test hook (no reference counterpart): with on = 0, jobs planned on this
+ * thread with HM_PATH_AUTO carry no escalation copy.  By default a job the
+ * autotuner sends to the BF16 or TF32 screen also carries a split-BF16 copy:
+ * after the threshold pass the device compares each row's keep band with its
+ * threshold, and when the coarse screen would keep a large share of the
+ * dataset for more than a tenth of the rows (points in clusters far tighter
+ * than its rounding), the copy screens the job instead.  Same results either
+ * way; hm_stats.path_used then reports HM_PATH_SCREEN_BF16X3. */
+HM_API int hm_tuning_escalation(int on);
 
 /* ----------------------------------------------------------------------------
  * Instrumentation (no reference counterpart; the reference has no timers on

@@ -176,3 +176,78 @@ def test_pair_and_single_cta_emission_agree_with_the_oracle(oracle, path, n):
         assert_same_bytes(knn.dists, od, f"pair={pair} dists")
         assert_same_bytes(sm.sigmas, osig, f"pair={pair} sigma")
         assert_same_bytes(sm.rhos, orho, f"pair={pair} rho")
+
+
+def _tight_clusters(n, d, seed, sigma=0.05):
+    """Eight clusters far tighter than a BF16 or TF32 operand's rounding
+    relative to their distance from the origin (the coarse screens' hard case)."""
+    g = np.random.default_rng(seed)
+    centres = g.normal(0.0, 4.0, size=(8, d))
+    labels = g.integers(0, 8, size=n)
+    return np.ascontiguousarray((centres[labels] + g.normal(0.0, sigma, size=(n, d))).astype(np.float32))
+
+
+@pytest.mark.parametrize("metric", ["cosine", "euclidean"])
+def test_auto_escalates_on_clusters_tighter_than_the_screen(metric):
+    """A job left to the autotuner, whose choice here is the BF16 (cosine) or
+    TF32 (euclidean) screen, hands over to its split-BF16 copy when the
+    coarse screen's band swamps the rows' thresholds; the bytes equal the
+    plain path's either way (escalation off: the coarse screen's own, slow
+    but exact, result)."""
+    lib = hm.lib()
+    n, d, k = 4096, 384, 15
+    x = _tight_clusters(n, d, seed=7)
+    assert hm.autotune_path(n, d, k, metric) in (hm.KnnPath.SCREEN_BF16, hm.KnnPath.SCREEN_TF32)
+    plain, psm = hm.knn_smooth(x, d, k, metric, "plain")
+    st = hm.HmStats()
+    knn, sm = hm.knn_smooth(x, d, k, metric, "auto", stats=st)
+    assert st.path_used == int(hm.KnnPath.SCREEN_BF16X3), st.path_used
+    for a, b, what in ((knn.indices, plain.indices, "indices"), (knn.dists, plain.dists, "dists"),
+                       (sm.sigmas, psm.sigmas, "sigma"), (sm.rhos, psm.rhos, "rho")):
+        assert_same_bytes(a, b, f"escalated {what}")
+    assert lib.hm_tuning_escalation(0) == 0
+    try:
+        st0 = hm.HmStats()
+        knn0, sm0 = hm.knn_smooth(x, d, k, metric, "auto", stats=st0)
+    finally:
+        lib.hm_tuning_escalation(1)
+    assert st0.path_used == int(hm.autotune_path(n, d, k, metric))
+    assert_same_bytes(knn0.indices, plain.indices, "coarse indices")
+    assert_same_bytes(knn0.dists, plain.dists, "coarse dists")
+
+
+def test_auto_keeps_the_coarse_screen_on_embedding_shaped_data():
+    """Embedding-shaped data (the autotuner's cosine family) keeps the BF16
+    screen: its band is a few percent of the rows' thresholds."""
+    from holomap_b200.synth import embed_50k
+    wl = embed_50k(n=8192)
+    assert hm.autotune_path(wl.n, wl.d, wl.k, wl.metric) == hm.KnnPath.SCREEN_BF16
+    plain, _ = hm.knn_smooth(wl.data, wl.d, wl.k, wl.metric, "plain")
+    st = hm.HmStats()
+    knn, _ = hm.knn_smooth(wl.data, wl.d, wl.k, wl.metric, "auto", stats=st)
+    assert st.path_used == int(hm.KnnPath.SCREEN_BF16)
+    assert_same_bytes(knn.indices, plain.indices, "indices")
+    assert_same_bytes(knn.dists, plain.dists, "dists")
+
+
+def test_batch_escalates_only_the_job_that_needs_it():
+    """In one batch, the tightly clustered job escalates and the
+    embedding-shaped one does not; both return the plain path's bytes."""
+    import torch
+    from holomap_b200.device import DeviceBatch
+    from holomap_b200.synth import embed_50k
+    a = _tight_clusters(4096, 384, seed=3)
+    b = embed_50k(n=4096).data
+    batch = DeviceBatch([(torch.from_numpy(a).cuda(), 15, "cosine"), (torch.from_numpy(b).cuda(), 30, "cosine")])
+    batch.run()
+    torch.cuda.synchronize()
+    for j, (x, k) in enumerate(((a, 15), (b, 30))):
+        plain, psm = hm.knn_smooth(x, 384, k, "cosine", "plain")
+        idx, dist, sig, rho = batch.result(j)
+        assert_same_bytes(idx.reshape(-1), plain.indices, f"job {j} indices")
+        assert_same_bytes(dist.reshape(-1), plain.dists, f"job {j} dists")
+        assert_same_bytes(sig, psm.sigmas, f"job {j} sigma")
+        assert_same_bytes(rho, psm.rhos, f"job {j} rho")
+    paths = [batch.stats(j).path_used for j in range(2)]
+    assert paths[0] == int(hm.KnnPath.SCREEN_BF16X3), paths
+    assert paths[1] != int(hm.KnnPath.SCREEN_BF16X3), paths
