@@ -60,6 +60,15 @@ SCREENS = ["screen_bf16", "screen_tf32", "screen_bf16x3"]
 SEED_DIVS = [4, 8, 16]
 BATCH_JOBS = 32
 BATCH_MAX_N = 8192
+# Up to this d a screened job planned in a batch takes the split-BF16 screen
+# whatever screen won its shape's batch: a batch of mixed shapes then shares
+# one screen launch (three formats cost three pipelines of launches), and
+# split-BF16's band (about 2^-16 of the norms) needs no escalation copy.
+# Measured on batch_256 (256 datasets, d in {16, 50, 128}): 25,300 graphs/s
+# with each job on its shape's batch winner (TF32 for 139 jobs, split-BF16 for
+# 72) against 35,900 with every screened job on split-BF16; at these d the
+# per-shape batch times of TF32 and split-BF16 are within a few percent.
+BATCH_SHARED_MAX_D = 256
 PATH_CODE = {"plain": 1, "screen_bf16": 2, "screen_tf32": 3, "screen_bf16x3": 4}
 
 
@@ -234,6 +243,13 @@ def sweep(grid_n=GRID_N, grid_d=GRID_D, grid_k=GRID_K, metrics=METRICS, verbose=
     }
 
 
+def _best_seed_div(e: dict, path: str) -> int:
+    """The fastest measured threshold sample of a path at a grid point."""
+    t = {c: v for c, v in e["times_ms"].items() if v is not None and c.startswith(path + "/")
+         and c.endswith("/full")}
+    return int(min(t, key=t.get).split("/")[1]) if t else 8
+
+
 def table_from(doc: dict | None) -> tuple[dict, dict, list, list, list]:
     """(choice, batch_choice, grid n, d, k); choice[(metric, k, d, n)] =
     (path, seed_div, symmetric, pair) for a problem alone, batch_choice the
@@ -249,7 +265,13 @@ def table_from(doc: dict | None) -> tuple[dict, dict, list, list, list]:
         key = (e["metric"], e["k"], e["d"], e["n"])
         choice[key] = (e["best"], e["seed_div"], e.get("symmetric", 1), e.get("pair", 1))
         if "batch_best" in e:
-            batch[key] = (e["batch_best"], e.get("batch_seed_div", 8), 0, 1)
+            bp, bsd = e["batch_best"], e.get("batch_seed_div", 8)
+            if bp != "plain" and e["d"] <= BATCH_SHARED_MAX_D and bp != "screen_bf16x3":
+                # a mixed batch shares one split-BF16 screen launch (see
+                # BATCH_SHARED_MAX_D)
+                bp = "screen_bf16x3"
+                bsd = _best_seed_div(e, bp)
+            batch[key] = (bp, bsd, 0, 1)
         else:
             batch[key] = choice[key]
     return choice, batch, g["n"], g["d"], g["k"]
