@@ -110,24 +110,28 @@ __device__ __forceinline__ uint32_t to_tf32_bits(double v, double *rounded) {
     return b;
 }
 
+// Group rows per operand_kernel block (one per warp: the rows' loads and
+// binary64 sums are latency-bound, so more warps in flight pay; a divisor of
+// 32, so a block's rows are of one job, whose rows start 32-aligned).
+constexpr uint32_t OP_ROWS = 8;
+
 // Operand row(s), binary64 error statistics, additive terms of the screen
-// epilogue, and the row's shared threshold.  A block covers 32 group rows of
-// one job (a job's rows start 32-aligned), a warp 4 of them; the job's maxima
-// take one atomic per block.
+// epilogue, and the row's shared threshold.  A block covers OP_ROWS group
+// rows of one job; the job's maxima take one atomic per block.
 __global__ void __launch_bounds__(256) operand_kernel(const JobDev *__restrict__ jobs,
                                                      const GroupDev *__restrict__ Gp) {
     __shared__ double s_max[8][6];
     __shared__ unsigned long long s_zero[8];
     const GroupDev &G = *Gp;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t gr0 = blockIdx.x * 32;
+    const uint32_t gr0 = blockIdx.x * OP_ROWS;
     const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr0)]];
-    if (!job_active(J)) return;  // uniform over the block (32 rows of one job)
+    if (!job_active(J)) return;  // uniform over the block (its rows are of one job)
     unsigned long long *maxb = J.cnt->maxb;
     double wmax[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     unsigned long long wzero = 0;
-    for (uint32_t wr = 0; wr < 4; ++wr) {
-        const uint32_t gr = gr0 + warp * 4 + wr;
+    for (uint32_t wr = 0; wr < OP_ROWS / 8; ++wr) {
+        const uint32_t gr = gr0 + warp * (OP_ROWS / 8) + wr;
         const uint32_t row = gr - J.row0;
         if (row >= J.n) {  // padding between jobs: zero operands (read only as masked rows/columns)
             for (uint32_t t = lane; t < G.kpmax; t += 32) {
@@ -312,7 +316,7 @@ int launch_screen_prep(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd
     colmean_kernel<<<G.njobs, 128, 0, s>>>(jobs, Gd);
     // G.rows is a multiple of 32: 32 group rows per block
     centred_norm_max_kernel<<<G.rows / 32, 256, 0, s>>>(jobs, Gd);
-    operand_kernel<<<G.rows / 32, 256, 0, s>>>(jobs, Gd);
+    operand_kernel<<<G.rows / OP_ROWS, 256, 0, s>>>(jobs, Gd);
     HM_CUDA_TRY(cudaGetLastError());
     count_launch(4);
     return HM_OK;
