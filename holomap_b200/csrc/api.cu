@@ -95,7 +95,7 @@ struct JobPlan {
     size_t off_mu = 0, off_csum = 0;
     int group = -1;
     uint32_t row0 = 0, unit0 = 0, kp1 = 0, k_stages = 0, row_blocks = 0, col_tiles = 0;
-    uint32_t parts = 1, part_tiles = 0, cap = 0, seed_tiles = 0;
+    uint32_t parts = 1, part_tiles = 0, cap = 0, seed_tiles = 0, tlists = 2;
     uint64_t slot0 = 0, cand0 = 0, topk0 = 0;
     // emission pass: symmetric (tiles on and above the diagonal), its column
     // parts per row block of ept tiles, candidate lists per row
@@ -339,7 +339,9 @@ static int plan_batch(const hm_job *user_specs, uint32_t user_jobs, hm_batch &B,
             P.unit0 = Gp.units;
             Gp.units += P.row_blocks * P.parts;
             P.slot0 = Gp.lists;
-            const uint64_t lists = P.spec.n * 2ull * P.parts;
+            // threshold-pass lists: one per epilogue segment and column part
+            P.tlists = (uint32_t)sc_epi_warps(0, (int)Gp.kp) / 4;
+            const uint64_t lists = P.spec.n * (uint64_t)P.tlists * P.parts;
             Gp.lists += lists;
             P.topk0 = Gp.topk;
             Gp.topk += lists * P.spec.k;
@@ -614,6 +616,7 @@ static int bind_batch(hm_batch &B, void *d_ws, size_t bytes, cudaStream_t s) {
         J.seed_tiles = P.seed_tiles;
         J.cap = P.cap;
         J.slot0 = P.slot0;
+        J.tlists = P.tlists;
         J.cand0 = P.cand0;
         J.topk0 = P.topk0;
         J.elists = P.elists;

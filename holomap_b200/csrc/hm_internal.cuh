@@ -192,7 +192,8 @@ struct JobDev {
     // screened path
     uint32_t group, row0, unit0, kp1, k_stages, row_blocks, col_tiles, parts, part_tiles, cap;
     uint32_t seed_tiles;         // leading column tiles of each part in the threshold pass
-    unsigned long long slot0;    // first threshold-pass list (2 * parts lists per row)
+    unsigned long long slot0;    // first threshold-pass list (tlists * parts lists per row)
+    uint32_t tlists;             // threshold-pass lists per column part (its epilogue segments)
     unsigned long long topk0;    // first k-array entry: list l's is [topk0 + (l - slot0) * k, +k)
     // candidate lists of the emission pass: elists per row (two per column
     // part; with the symmetric emission one more, the row's column list, last)

@@ -675,7 +675,7 @@ __global__ void __launch_bounds__(256) threshold_kernel(const JobDev *__restrict
     const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
     const uint32_t row = gr - J.row0;
     if (row < J.q0 || row >= J.q1 || !job_active(J)) return;
-    const uint32_t k = J.k, lists = 2 * J.parts;
+    const uint32_t k = J.k, lists = J.tlists * J.parts;
     const size_t l0 = list_index(J, row, 0);
     // the row's lists' arrays are contiguous: lists x k values
     const float *base = G.topk + J.topk0 + (l0 - J.slot0) * k;

@@ -43,13 +43,16 @@ constexpr uint32_t SC_ARES_STAGES = 6;
 // Epilogue warps per CTA: warp 0 issues the TMA loads, warp 1 the MMAs, the
 // rest read the accumulator, (warp & 3) naming their TMEM lane quadrant (32
 // query rows) and (warp - 2) / 4 their segment of the tile's 256 columns.
-// The threshold and symmetric emission passes take 8 (two segments of 128
-// columns, the threshold pass's sorted arrays need the registers); the full
-// emission pass takes 16 (four segments of 64 columns: twice the warps to
-// hide the latency of the per-row tests, each writing its own candidate
-// list, so a row has four lists per column part).
-__host__ __device__ constexpr int sc_epi_warps(int pass) { return pass == 1 ? 16 : 8; }
-__host__ __device__ constexpr int sc_threads(int pass) { return 64 + 32 * sc_epi_warps(pass); }
+// The full emission pass takes 16 (four segments of 64 columns: twice the
+// warps to hide the latency of the per-row tests; each warp writes its own
+// list, so a row has four lists per column part); the threshold pass (its
+// sorted arrays need the registers) and the symmetric emission pass take 8
+// (two segments of 128 columns).  A 16-warp threshold pass for k <= 32
+// (96 registers, some spilled, four k-arrays per part) measured slower.
+__host__ __device__ constexpr int sc_epi_warps(int pass, int kp = 32) {
+    return (pass == 1 && kp > 0) ? 16 : 8;
+}
+__host__ __device__ constexpr int sc_threads(int pass, int kp = 32) { return 64 + 32 * sc_epi_warps(pass, kp); }
 constexpr int SC_FULL_LISTS = 4;  // candidate lists per row and column part of the full emission pass
 
 enum ScreenKind { SCREEN_KIND_BF16 = 0, SCREEN_KIND_TF32 = 1 };
@@ -112,9 +115,9 @@ __device__ __forceinline__ float unord32(uint32_t o) {
     return __uint_as_float((o & 0x80000000u) ? (o & 0x7fffffffu) : ~o);
 }
 
-// Row i's threshold-pass list s (s < 2 * parts) of job J (its k-array).
+// Row i's threshold-pass list s (s < tlists * parts) of job J (its k-array).
 __device__ __forceinline__ size_t list_index(const JobDev &J, uint32_t i, uint32_t s) {
-    return (size_t)J.slot0 + (size_t)i * 2 * J.parts + s;
+    return (size_t)J.slot0 + (size_t)i * J.tlists * J.parts + s;
 }
 
 // Row i's candidate list s (s < elists) of job J: its count is

@@ -317,7 +317,7 @@ __device__ __forceinline__ UnitTiles unit_tiles(const JobDev *jobs, const GroupD
 }
 
 template <int KIND, int KP, int PASS, bool PAIR>
-__global__ void __launch_bounds__(sc_threads(PASS), 1)
+__global__ void __launch_bounds__(sc_threads(PASS, KP), 1)
     screen_gemm_kernel(const __grid_constant__ CUtensorMap tma, const __grid_constant__ CUtensorMap tmb,
                        const JobDev *__restrict__ jobs, const GroupDev G, float *dump, uint32_t idesc,
                        uint32_t a_res) {
@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(sc_threads(PASS), 1)
     // PASS 2 is the emission pass of a group with symmetric units (the
     // column-side tests exist only in that instantiation)
     constexpr bool SYMK = PASS == 2;
-    constexpr uint32_t EW = sc_epi_warps(PASS);   // epilogue warps
+    constexpr uint32_t EW = sc_epi_warps(PASS, KP);  // epilogue warps
     constexpr uint32_t NSEG = EW / 4;             // column segments per tile (= lists per part)
     constexpr uint32_t SEGW = SC_BN / NSEG;       // columns per segment
 
@@ -1104,7 +1104,7 @@ static int launch_kind(const JobDev *jobs, const GroupDev &G, const CUtensorMap 
     if (grid == 0) return HM_OK;
     // every job's K slices fit the resident A block
     const uint32_t a_res = (G.kpmax / G.kslice) <= SC_ARES_STAGES ? 1u : 0u;
-    screen_gemm_kernel<KIND, KP, PASS, false><<<grid, sc_threads(PASS), SC_SMEM_BYTES, s>>>(ta, tb, jobs, G, dump,
+    screen_gemm_kernel<KIND, KP, PASS, false><<<grid, sc_threads(PASS, KP), SC_SMEM_BYTES, s>>>(ta, tb, jobs, G, dump,
                                                                                       idesc, a_res);
     HM_CUDA_TRY(cudaGetLastError());
     count_launch();
