@@ -77,3 +77,25 @@ def test_smooth_rows_equal_rows_of_the_whole_calibration(oracle, k):
     for b, e in [(5, 5), (10, 3), (0, n + 1)]:
         assert lib.hm_smooth_knn_rows_device(dt.data_ptr(), n, k, b, e, sig.data_ptr(), rho.data_ptr(),
                                              wp, stream) == hm.HM_ERR_INVALID
+
+
+def test_row_ranges_of_an_escalating_job():
+    """Row ranges of a job left to the autotuner whose points are clusters far
+    tighter than the coarse screen's rounding (the range job carries its
+    split-BF16 escalation copy): the rows of the whole plain graph."""
+    import torch
+    from holomap_b200.shard import rows_cuda
+    g = np.random.default_rng(17)
+    n, d, k = 4096, 384, 15
+    centres = g.normal(0.0, 4.0, size=(8, d))
+    x = np.ascontiguousarray((centres[g.integers(0, 8, size=n)] + g.normal(0.0, 0.05, size=(n, d)))
+                             .astype(np.float32))
+    plain, _ = hm.knn_smooth(x, d, k, "cosine", "plain")
+    pi = plain.indices.reshape(n, k)
+    pd = plain.dists.reshape(n, k)
+    xt = torch.from_numpy(x).cuda()
+    for b, e in [(0, n), (100, 1300), (2048, 4096)]:
+        idx, dist = rows_cuda(xt, k, "cosine", "auto", b, e)
+        torch.cuda.synchronize()
+        assert_same_bytes(idx.cpu().numpy().view(np.uint32), pi[b:e], f"rows [{b},{e}) indices")
+        assert_same_bytes(dist.cpu().numpy(), pd[b:e], f"rows [{b},{e}) dists")

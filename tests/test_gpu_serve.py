@@ -128,3 +128,29 @@ def test_invalid_request_fails_alone_in_its_batch():
     for x, t in zip(good, [tickets[0], tickets[1], tickets[3]]):
         alone = hm.exact_knn(x, 12, 15, "cosine")
         assert_same_bytes(t.indices.reshape(-1), alone.indices, "batch mate of a failing request")
+
+
+def test_served_tight_clusters_escalate_and_match_the_plain_path():
+    """Requests whose points form clusters far tighter than the BF16/TF32
+    operands' rounding, batched with ordinary ones: each returns the plain
+    path's bytes (the coarse screen hands its rows to the split-BF16 copy
+    on the device)."""
+    g = np.random.default_rng(41)
+
+    def tight(n, d):
+        centres = g.normal(0.0, 4.0, size=(6, d))
+        labels = g.integers(0, 6, size=n)
+        return np.ascontiguousarray((centres[labels] + g.normal(0.0, 0.05, size=(n, d))).astype(np.float32))
+
+    reqs = [(tight(3000, 384), 15, "cosine"), (edge_case("gauss", 2500, 300, seed=4), 15, "cosine"),
+            (tight(2600, 384), 30, "euclidean"), (tight(2048, 300), 15, "cosine")]
+    with Server(max_batch_jobs=4, max_inflight=2) as srv:
+        tickets = [srv.submit(x, k, m) for x, k, m in reqs]
+        for t in tickets:
+            srv.wait(t)
+    for j, ((x, k, metric), t) in enumerate(zip(reqs, tickets)):
+        plain, psm = hm.knn_smooth(x, x.shape[1], k, metric, "plain")
+        assert_same_bytes(t.indices.reshape(-1), plain.indices, f"request {j} indices")
+        assert_same_bytes(t.dists.reshape(-1), plain.dists, f"request {j} dists")
+        assert_same_bytes(t.sigmas, psm.sigmas, f"request {j} sigma")
+        assert_same_bytes(t.rhos, psm.rhos, f"request {j} rho")
