@@ -2,16 +2,18 @@
 // exact rerank of the screen's candidates.
 //
 // threshold: one warp per row merges the k smallest mini-chunk minima of the
-// row's lists into tau1, the k-th smallest of their union.  Every mini-chunk
-// minimum is a screened value of the row, so at least k screened values are
-// <= tau1 and the row's k-th smallest screened value tau^ <= tau1.
+// row's lists into tau1, the k-th smallest of their union rounded up to 2^-13
+// of its binade.  Every mini-chunk minimum is a screened value of the row, so
+// at least k screened values are <= tau1 and the row's k-th smallest screened
+// value tau^ <= tau1.
 //
 // rerank: one warp per 8 consecutive group rows (always of one job: each job's
 // rows start 32-aligned in the group), in three phases.
-//   1. select, per row: tau^ is recomputed exactly as the k-th smallest
-//      screened value among the emitted candidates (the emission pass wrote
-//      every column with c^ <= tau1 + band, which includes the k smallest),
-//      and the candidates with c^ <= tau^ + band are compacted in place to the
+//   1. select, per row: tau^ is recomputed as the k-th smallest screened
+//      value among the emitted candidates (the emission pass wrote every
+//      column with c^ <= tau1 + band, which includes the k smallest), rounded
+//      up to 2^-15 of its binade (a larger threshold keeps a superset), and
+//      the candidates with c^ <= tau^ + band are compacted in place to the
 //      front of the row's own list region.  Rows whose list overflowed, or that
 //      the screen cannot bound (zero vectors under cosine), are appended to the
 //      overflow list for the exact plain path.
@@ -30,6 +32,7 @@
 #include <cuda_runtime.h>
 
 #include "hm_internal.cuh"
+#include "mbarrier.cuh"
 #include "screen.cuh"
 
 namespace hm {
@@ -45,11 +48,16 @@ __device__ __forceinline__ double step(double acc, double x, double y) {
     return __dadd_rn(acc, __dmul_rn(x, y));
 }
 
-// k-th smallest of a warp's `total` keys (at most 32 * NQ; lane l holds keys
-// l, l + 32, ...; absent keys are ~0): the largest r with fewer than k keys
-// below it, found bit by bit from the highest bit where the keys differ.
+// Upper bound of the k-th smallest of a warp's `total` keys (at most 32 * NQ;
+// lane l holds keys l, l + 32, ...; absent keys are ~0) that is exact but for
+// the key bits below `lo`: the largest r with fewer than k keys below it is
+// found bit by bit from the highest bit where the keys differ down to bit lo,
+// so r holds the k-th smallest key's bits from lo up; the bits below lo are
+// returned as ones (capped at the largest key).  lo = 0 gives the k-th
+// smallest itself.
 template <int NQ>
-__device__ __forceinline__ uint32_t kth_key(const uint32_t (&ov)[NQ], uint32_t total, uint32_t k, int lane) {
+__device__ __forceinline__ uint32_t kth_key(const uint32_t (&ov)[NQ], uint32_t total, uint32_t k, int lo,
+                                            int lane) {
     uint32_t mn = 0xffffffffu, mx = 0u;
 #pragma unroll
     for (int q = 0; q < NQ; ++q) {
@@ -63,7 +71,7 @@ __device__ __forceinline__ uint32_t kth_key(const uint32_t (&ov)[NQ], uint32_t t
     if (mn == mx) return mn;
     const int top = 31 - __clz(mn ^ mx);
     uint32_t r = top == 31 ? 0u : (mn & ~((2u << top) - 1u));  // the keys' common high bits
-    for (int b = top; b >= 0; --b) {
+    for (int b = top; b >= lo; --b) {
         const uint32_t t = r | (1u << b);
         uint32_t c = 0;
 #pragma unroll
@@ -71,29 +79,29 @@ __device__ __forceinline__ uint32_t kth_key(const uint32_t (&ov)[NQ], uint32_t t
         c = __reduce_add_sync(0xffffffffu, c);
         if (c < k) r = t;
     }
-    return r;
+    return min(r | ((1u << lo) - 1u), mx);
 }
 
 // kth_key over keys key(e), e < total <= 512, with the register count
 // chosen by the total
 template <int NQ, typename KeyFn>
-__device__ __forceinline__ uint32_t kth_load(KeyFn key, uint32_t total, uint32_t k, int lane) {
+__device__ __forceinline__ uint32_t kth_load(KeyFn key, uint32_t total, uint32_t k, int lo, int lane) {
     uint32_t ov[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; ++q) {
         const uint32_t e = q * 32 + lane;
         ov[q] = e < total ? key(e) : 0xffffffffu;
     }
-    return kth_key<NQ>(ov, total, k, lane);
+    return kth_key<NQ>(ov, total, k, lo, lane);
 }
 
 template <typename KeyFn>
-__device__ __forceinline__ uint32_t kth_of(KeyFn key, uint32_t total, uint32_t k, int lane) {
-    if (total <= 32) return kth_load<1>(key, total, k, lane);
-    if (total <= 64) return kth_load<2>(key, total, k, lane);
-    if (total <= 128) return kth_load<4>(key, total, k, lane);
-    if (total <= 256) return kth_load<8>(key, total, k, lane);
-    return kth_load<16>(key, total, k, lane);
+__device__ __forceinline__ uint32_t kth_of(KeyFn key, uint32_t total, uint32_t k, int lo, int lane) {
+    if (total <= 32) return kth_load<1>(key, total, k, lo, lane);
+    if (total <= 64) return kth_load<2>(key, total, k, lo, lane);
+    if (total <= 128) return kth_load<4>(key, total, k, lo, lane);
+    if (total <= 256) return kth_load<8>(key, total, k, lo, lane);
+    return kth_load<16>(key, total, k, lo, lane);
 }
 
 constexpr int RR_ROWS = 8;        // group rows per warp of the exact phase
@@ -125,15 +133,13 @@ struct RsWarpSmem {
     uint32_t loff[32];  // first staged position of each list
 };
 
-__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
 // global -> shared copies that zero-fill the bytes past src_bytes (0 reads nothing)
 __device__ __forceinline__ void cp_async16(void *dst, const void *src, uint32_t src_bytes) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_addr(dst)), "l"(src), "r"(src_bytes)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
                  : "memory");
 }
 __device__ __forceinline__ void cp_async4(void *dst, const void *src, uint32_t src_bytes) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_addr(dst)), "l"(src), "r"(src_bytes)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
@@ -154,11 +160,14 @@ __device__ __forceinline__ uint32_t list_cap(const JobDev &J, uint32_t s) {
     return (J.sym && s == J.elists - 2) ? 2 * J.cap : J.cap;
 }
 
-// k-th smallest (1-based k <= total) of the order-preserving keys held in
-// registers (lane l: keys l, l + 32, ...; NQ per lane), by a most-significant-
-// byte-first radix select: each pass counts the keys that share the bytes
-// chosen so far in 256 shared-memory bins, and the bin holding the k-th
-// fixes the next byte.  Bytes the keys all share are skipped.
+// Upper bound of the k-th smallest (1-based k <= total) of the order-
+// preserving keys held in registers (lane l: keys l, l + 32, ...; NQ per
+// lane), exact but for its lowest byte, which is returned as ones (capped at
+// the largest key): a most-significant-byte-first radix select, each pass
+// counting the keys that share the bytes chosen so far in 256 shared-memory
+// bins, the bin holding the k-th fixing the next byte.  Bytes the keys all
+// share are skipped, and so is the last byte: a threshold above the k-th
+// smallest by less than 2^-15 of its binade only keeps a superset.
 template <int NQ>
 __device__ __forceinline__ uint32_t radix_kth(const uint32_t (&key)[NQ], uint32_t total, uint32_t k,
                                               uint32_t *hist, int lane) {
@@ -176,7 +185,7 @@ __device__ __forceinline__ uint32_t radix_kth(const uint32_t (&key)[NQ], uint32_
     const int hb = (31 - __clz(mn ^ mx)) >> 3;  // highest byte where the keys differ
     uint32_t mask = hb == 3 ? 0u : ~((1u << (8 * hb + 8)) - 1u);
     uint32_t prefix = mn & mask, kk = k;
-    for (int shift = 8 * hb; shift >= 0; shift -= 8) {
+    for (int shift = 8 * hb; shift >= 8; shift -= 8) {
         for (int b = lane; b < 256; b += 32) hist[b] = 0u;
         __syncwarp();
 #pragma unroll
@@ -216,7 +225,7 @@ __device__ __forceinline__ uint32_t radix_kth(const uint32_t (&key)[NQ], uint32_
         mask |= 255u << shift;
         __syncwarp();
     }
-    return prefix;
+    return min(prefix | 0xffu, mx);
 }
 
 template <int NQ>
@@ -257,11 +266,11 @@ __device__ __forceinline__ uint32_t select_row(const JobDev &J, const GroupDev &
     }
     const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
     unsigned long long *region = row_region(J, G, row);
-    // Threshold: the exact k-th smallest screened value of the row, over the
-    // emitted candidates (they include the row's k smallest).  Up to RR_CBUF
+    // Threshold: the k-th smallest screened value of the row over the emitted
+    // candidates (they include the row's k smallest).  Up to RR_CBUF
     // candidates are staged in shared memory (every list's chunk c loaded
-    // before any is stored) and the k-th found by a radix select; longer rows
-    // use a warp top-k.
+    // before any is stored) and the k-th bounded from above by a radix select
+    // (to its lowest key byte); longer rows use a warp top-k (exact).
     const bool staged = total <= RR_CBUF;
     float tau = __int_as_float(0x7f800000);
     if (staged) {
@@ -379,6 +388,24 @@ __global__ void __launch_bounds__(RS_WARPS * 32, 4) rr_select_kernel(const JobDe
     }
 }
 
+// The (distance bits, index) key of pair (row, j) from its binary64
+// accumulation: the reference's final step of each metric, the self pair
+// forced to 0 (src/knn.rs:38-39).
+template <int METRIC>
+__device__ __forceinline__ unsigned long long pair_key(const JobDev &J, uint32_t row, uint32_t j, double acc) {
+    float dist;
+    if (j == row) {
+        dist = 0.0f;
+    } else if (METRIC == HM_METRIC_EUCLIDEAN) {
+        dist = __double2float_rn(__dsqrt_rn(acc));
+    } else {
+        const double q = __ddiv_rn(acc, __dmul_rn(J.rnorm[row], J.rnorm[j]));
+        const double r = __dsub_rn(1.0, q);
+        dist = (r > 0.0) ? __double2float_rn(r) : 0.0f;
+    }
+    return make_key(dist, j);
+}
+
 // Phase 2: exact distances of the flat survivor sequence of the warp's rows
 // (group rows gr0 .. gr0 + 7; lane r < 8 holds row r's count in `cnt_l`).
 template <int METRIC>
@@ -492,19 +519,7 @@ __device__ __forceinline__ void exact_pairs(const JobDev &J, const GroupDev &G, 
             }
             __syncwarp();
         }
-        if (active) {
-            float dist;
-            if (j == row) {
-                dist = 0.0f;  // src/knn.rs:38-39
-            } else if (METRIC == HM_METRIC_EUCLIDEAN) {
-                dist = __double2float_rn(__dsqrt_rn(acc));
-            } else {
-                const double q = __ddiv_rn(acc, __dmul_rn(J.rnorm[row], J.rnorm[j]));
-                const double r = __dsub_rn(1.0, q);
-                dist = (r > 0.0) ? __double2float_rn(r) : 0.0f;
-            }
-            *slot = make_key(dist, j);
-        }
+        if (active) *slot = pair_key<METRIC>(J, row, j, acc);
         __syncwarp();
         s = end;
     }
@@ -665,6 +680,7 @@ int launch_column_scatter(const JobDev *jobs, const GroupDev &G, const GroupDev 
 
 // tau1 of every row: the k-th smallest of the union of its lists' k smallest
 // mini-chunk minima (an upper bound of the row's k-th screened value).
+constexpr int TAU1_LOW_BITS = 10;
 template <int KPL>
 __global__ void __launch_bounds__(256) threshold_kernel(const JobDev *__restrict__ jobs,
                                                        const GroupDev *__restrict__ Gp) {
@@ -681,7 +697,10 @@ __global__ void __launch_bounds__(256) threshold_kernel(const JobDev *__restrict
     const float *base = G.topk + J.topk0 + (l0 - J.slot0) * k;
     const uint32_t total = lists * k;
     if (total <= 256) {
-        const uint32_t r = kth_of([&](uint32_t e) { return ord32(base[e]); }, total, k, lane);
+        // tau1 is an upper bound in any case: resolving it to 2^-13 of its
+        // binade (ten low key bits left as ones) emits no measurable extra
+        // candidates and halves the bit loop
+        const uint32_t r = kth_of([&](uint32_t e) { return ord32(base[e]); }, total, k, TAU1_LOW_BITS, lane);
         if (lane == 0) G.rowthr[gr] = r;
         return;
     }

@@ -110,28 +110,51 @@ __device__ __forceinline__ uint32_t to_tf32_bits(double v, double *rounded) {
     return b;
 }
 
-// Group rows per operand_kernel block (one per warp: the rows' loads and
-// binary64 sums are latency-bound, so more warps in flight pay; a divisor of
-// 32, so a block's rows are of one job, whose rows start 32-aligned).
-constexpr uint32_t OP_ROWS = 8;
+// operand_kernel: one warp per group row, the warps striding over the rows
+// (a persistent grid of OP_BLOCKS_PER_SM blocks per SM).  A row's loads (up to
+// 512 elements; 256 in the split form) are all issued before its first store,
+// so a row costs one memory round trip; the job's maxima are kept per warp and written (one
+// atomic each) when the warp's next row belongs to another job, or at its end.
+constexpr uint32_t OP_WARPS = 8;
+constexpr int OP_BLOCKS_PER_SM = 3;
+constexpr int OP_TF32 = 0, OP_BF16 = 1, OP_SPLIT = 2;
+// elements per lane in flight (the split form's six stores per element need
+// the registers of half of them)
+__host__ __device__ constexpr uint32_t op_per_lane(int mode) { return mode == OP_SPLIT ? 8u : 16u; }
 
 // Operand row(s), binary64 error statistics, additive terms of the screen
-// epilogue, and the row's shared threshold.  A block covers OP_ROWS group
-// rows of one job; the job's maxima take one atomic per block.
-__global__ void __launch_bounds__(256) operand_kernel(const JobDev *__restrict__ jobs,
-                                                     const GroupDev *__restrict__ Gp) {
-    __shared__ double s_max[8][6];
-    __shared__ unsigned long long s_zero[8];
+// epilogue, and the row's shared threshold.  Every lane accumulates its
+// elements t = lane, lane + 32, ... in ascending order.
+template <int MODE>  // OP_TF32, OP_BF16 or OP_SPLIT: the group's operand format
+__global__ void __launch_bounds__(OP_WARPS * 32, OP_BLOCKS_PER_SM) operand_kernel(const JobDev *__restrict__ jobs,
+                                                               const GroupDev *__restrict__ Gp) {
+    // the warp's maxima live in shared memory (lane 0 alone updates them)
+    __shared__ double s_wmax[OP_WARPS][6];
+    __shared__ unsigned long long s_wzero[OP_WARPS];
     const GroupDev &G = *Gp;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t gr0 = blockIdx.x * OP_ROWS;
-    const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr0)]];
-    if (!job_active(J)) return;  // uniform over the block (its rows are of one job)
-    unsigned long long *maxb = J.cnt->maxb;
-    double wmax[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-    unsigned long long wzero = 0;
-    for (uint32_t wr = 0; wr < OP_ROWS / 8; ++wr) {
-        const uint32_t gr = gr0 + warp * (OP_ROWS / 8) + wr;
+    double *wmax = s_wmax[warp];
+    const JobDev *cur = nullptr;  // the job whose maxima the warp holds
+    auto reset = [&]() {
+        if (lane == 0) {
+            for (int q = 0; q < 6; ++q) wmax[q] = 0.0;
+            s_wzero[warp] = 0;
+        }
+    };
+    auto flush = [&]() {
+        if (cur != nullptr && lane == 0) {
+            unsigned long long *maxb = cur->cnt->maxb;
+            for (int q = 0; q < 6; ++q) atomic_max_pos(&maxb[q], wmax[q]);
+            if (s_wzero[warp]) atomicAdd(&maxb[7], s_wzero[warp]);
+        }
+        reset();
+        cur = nullptr;
+    };
+    reset();
+    const uint32_t stride = gridDim.x * OP_WARPS;
+    for (uint32_t gr = blockIdx.x * OP_WARPS + warp; gr < G.rows; gr += stride) {
+        const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
+        if (!job_active(J)) continue;
         const uint32_t row = gr - J.row0;
         if (row >= J.n) {  // padding between jobs: zero operands (read only as masked rows/columns)
             for (uint32_t t = lane; t < G.kpmax; t += 32) {
@@ -144,11 +167,16 @@ __global__ void __launch_bounds__(256) operand_kernel(const JobDev *__restrict__
             }
             continue;
         }
+        if (&J != cur) {
+            flush();
+            cur = &J;
+        }
 
+        const bool euc = J.metric == HM_METRIC_EUCLIDEAN;
         double scale = 1.0;
         bool zero_row = false;
-        if (J.metric == HM_METRIC_EUCLIDEAN) {
-            const double m = sqrt(__longlong_as_double((long long)maxb[6]));
+        if (euc) {
+            const double m = sqrt(__longlong_as_double((long long)J.cnt->maxb[6]));
             if (m > 0.0) {
                 int e;
                 frexp(m, &e);  // m = f * 2^e, f in [0.5, 1)
@@ -161,35 +189,34 @@ __global__ void __launch_bounds__(256) operand_kernel(const JobDev *__restrict__
         }
 
         const size_t kp = G.kpmax;
+        const uint32_t d = J.d, kp1 = J.kp1;
         double uu = 0.0, ee = 0.0, rr = 0.0, aa = 0.0;
-        const float *xr = J.x + (size_t)row * J.d;
+        const float *xr = J.x + (size_t)row * d;
         // cosine rows are scaled by 1 / ||x|| (the operand u is whatever this
         // arithmetic forms: the band is measured from it)
-        const bool euc = J.metric == HM_METRIC_EUCLIDEAN;
         const double mul = scale;
-        // the row's elements four at a time, their loads issued together
-        for (uint32_t t0 = 0; t0 < J.kp1; t0 += 128) {
-            float xs[4];
-            double ms[4];
+        constexpr uint32_t PER_LANE = op_per_lane(MODE);
+        for (uint32_t t0 = 0; t0 < kp1; t0 += 32 * PER_LANE) {
+            float xs[PER_LANE];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (uint32_t q = 0; q < PER_LANE; ++q) {
                 const uint32_t t = t0 + 32 * q + lane;
-                xs[q] = t < J.d ? xr[t] : 0.0f;
-                ms[q] = (euc && t < J.d) ? J.mu[t] : 0.0;
+                xs[q] = t < d ? __ldg(xr + t) : 0.0f;
             }
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
+            for (uint32_t q = 0; q < PER_LANE; ++q) {
                 const uint32_t t = t0 + 32 * q + lane;
-                if (t >= J.kp1) break;
-                const double u = t < J.d ? (euc ? ((double)xs[q] - ms[q]) * mul : (double)xs[q] * mul) : 0.0;
+                if (t >= kp1) break;
+                double u = 0.0;
+                if (t < d) u = euc ? ((double)xs[q] - __ldg(J.mu + t)) * mul : (double)xs[q] * mul;
                 uu += u * u;
-                if (G.kind == SCREEN_KIND_TF32) {
+                if (MODE == OP_TF32) {
                     double r;
                     const uint32_t b = to_tf32_bits(u, &r);
                     reinterpret_cast<uint32_t *>(G.opa)[(size_t)gr * kp + t] = b;
                     ee += (r - u) * (r - u);
                     aa += r * r;
-                } else if (!G.split) {
+                } else if (MODE == OP_BF16) {
                     double r;
                     const uint16_t b = to_bf16_bits(u, &r);
                     reinterpret_cast<uint16_t *>(G.opa)[(size_t)gr * kp + t] = b;
@@ -203,11 +230,11 @@ __global__ void __launch_bounds__(256) operand_kernel(const JobDev *__restrict__
                     uint16_t *A = reinterpret_cast<uint16_t *>(G.opa) + (size_t)gr * kp;
                     uint16_t *B = reinterpret_cast<uint16_t *>(G.opb) + (size_t)gr * kp;
                     A[t] = bh;
-                    A[J.kp1 + t] = bh;
-                    A[2 * J.kp1 + t] = bl;
+                    A[kp1 + t] = bh;
+                    A[2 * kp1 + t] = bl;
                     B[t] = bh;
-                    B[J.kp1 + t] = bl;
-                    B[2 * J.kp1 + t] = bh;
+                    B[kp1 + t] = bl;
+                    B[2 * kp1 + t] = bh;
                     ee += lo * lo;
                     rr += res * res;
                     aa += 2.0 * hi * hi + lo * lo;
@@ -233,7 +260,7 @@ __global__ void __launch_bounds__(256) operand_kernel(const JobDev *__restrict__
             wmax[3] = fmax(wmax[3], st.anorm);
             wmax[4] = fmax(wmax[4], st.bnorm);
             wmax[5] = fmax(wmax[5], st.sqnorm);
-            if (J.metric == HM_METRIC_EUCLIDEAN) {
+            if (euc) {
                 const float nsq = __double2float_rn(uu);
                 G.rowterm[gr] = nsq;
                 G.colterm[gr] = nsq;
@@ -242,24 +269,11 @@ __global__ void __launch_bounds__(256) operand_kernel(const JobDev *__restrict__
                 G.colterm[gr] = zero_row ? 0.0f : 1.0f;
             }
             G.force[gr] = zero_row ? 1 : 0;
-            if (zero_row) ++wzero;
+            if (zero_row) ++s_wzero[warp];
             G.rowthr[gr] = 0xff800000u;  // the row's shared threshold starts at +inf
         }
     }
-    if (lane == 0) {
-        for (int q = 0; q < 6; ++q) s_max[warp][q] = wmax[q];
-        s_zero[warp] = wzero;
-    }
-    __syncthreads();
-    if (threadIdx.x < 6) {
-        double m = s_max[0][threadIdx.x];
-        for (int w = 1; w < 8; ++w) m = fmax(m, s_max[w][threadIdx.x]);
-        atomic_max_pos(&maxb[threadIdx.x], m);
-    } else if (threadIdx.x == 6) {
-        unsigned long long z = 0;
-        for (int w = 0; w < 8; ++w) z += s_zero[w];
-        if (z) atomicAdd(&maxb[7], z);
-    }
+    flush();
 }
 
 // Keep band of one row (binary32 bits, rounded up), written to G.band.
@@ -316,7 +330,15 @@ int launch_screen_prep(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd
     colmean_kernel<<<G.njobs, 128, 0, s>>>(jobs, Gd);
     // G.rows is a multiple of 32: 32 group rows per block
     centred_norm_max_kernel<<<G.rows / 32, 256, 0, s>>>(jobs, Gd);
-    operand_kernel<<<G.rows / OP_ROWS, 256, 0, s>>>(jobs, Gd);
+    const uint32_t op_blocks = (G.rows + OP_WARPS - 1) / OP_WARPS;
+    const uint32_t op_cap = (uint32_t)device_sm_count() * OP_BLOCKS_PER_SM;
+    const uint32_t op_grid = op_blocks < op_cap ? op_blocks : op_cap;
+    if (G.kind == SCREEN_KIND_TF32)
+        operand_kernel<OP_TF32><<<op_grid, OP_WARPS * 32, 0, s>>>(jobs, Gd);
+    else if (!G.split)
+        operand_kernel<OP_BF16><<<op_grid, OP_WARPS * 32, 0, s>>>(jobs, Gd);
+    else
+        operand_kernel<OP_SPLIT><<<op_grid, OP_WARPS * 32, 0, s>>>(jobs, Gd);
     HM_CUDA_TRY(cudaGetLastError());
     count_launch(4);
     return HM_OK;
