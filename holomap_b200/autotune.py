@@ -189,8 +189,8 @@ def sweep(grid_n=GRID_N, grid_d=GRID_D, grid_k=GRID_K, metrics=METRICS, verbose=
                             del p
                         finally:
                             _lib.check(lib.hm_tuning_override(0))
-                            _lib.check(lib.hm_tuning_symmetric(1))
-                            _lib.check(lib.hm_tuning_pair(1))
+                            _lib.check(lib.hm_tuning_symmetric(-1))
+                            _lib.check(lib.hm_tuning_pair(-1))
                         return t if same else None
 
                     for path in SCREENS:

@@ -357,21 +357,20 @@ static int plan_batch(const hm_job *user_specs, uint32_t user_jobs, hm_batch &B,
                 uint64_t tiles = 0;
                 for (uint32_t rb = 0; rb < P.row_blocks; ++rb) tiles += P.col_tiles - rb / 2;
                 P.ept = (uint32_t)std::max<uint64_t>(4, (tiles + 4ull * G - 1) / (4ull * G));
-                P.ept = std::max<uint32_t>(P.ept, (P.col_tiles + 7) / 8);  // at most 8 parts: 18 lists
+                P.ept = std::max<uint32_t>(P.ept, (P.col_tiles + 6) / 7);  // at most 7 parts: 30 lists
                 Gp.any_sym = true;
             } else {
                 P.ept = P.part_tiles;
             }
         }
-        // Candidate lists per row: a group with symmetric jobs runs the
-        // symmetric emission pass (two lists per column part, and for a
-        // symmetric job the column list, which takes two lists' room);
-        // otherwise the full pass writes SC_FULL_LISTS lists per part.  The
-        // cap of a list grows with the columns it covers.
+        // Candidate lists per row: SC_FULL_LISTS per column part (one per
+        // epilogue segment of the emission pass), and for a symmetric job the
+        // column list, which takes two lists' room.  The cap of a list grows
+        // with the columns it covers.
         for (uint32_t j : Gp.jobs) {
             JobPlan &P = B.jobs[j];
             const uint32_t eparts = (P.col_tiles + P.ept - 1) / P.ept;
-            const uint32_t per_part = Gp.any_sym ? 2u : (uint32_t)SC_FULL_LISTS;
+            const uint32_t per_part = (uint32_t)SC_FULL_LISTS;
             P.elists = per_part * eparts + (P.sym ? 2u : 0u);
             const double per_list = (double)P.spec.n / ((double)per_part * eparts);
             const double expect = 1.5 * P.spec.k * (2.0 + std::log(std::fmax(1.0, per_list / P.spec.k)));
@@ -386,18 +385,19 @@ static int plan_batch(const hm_job *user_specs, uint32_t user_jobs, hm_batch &B,
             Gp.cand += P.spec.n * (uint64_t)P.elists * P.cap;
         }
         // The emission pass takes the 2-SM form (a cluster of two CTAs per
-        // block of 256 rows, each loading half of every column tile) when no
-        // job is symmetric, every job's K slices fit the resident A block and
-        // the autotuner table prefers it for every job.
-        Gp.pair = tuning_pair() && !Gp.pair_vetoed && !Gp.any_sym && Gp.kpmax / Gp.kslice <= SC_ARES_STAGES;
+        // block of 256 rows, each loading half of every column tile) when
+        // every job's K slices fit the resident A block and the autotuner
+        // table prefers it for every job.
+        Gp.pair = !Gp.pair_vetoed && Gp.kpmax / Gp.kslice <= SC_ARES_STAGES;
         // emission units of the group: (job slot | sym, row block (2-SM form:
-        // block of 256 rows), first tile, end tile | part)
+        // block of 256 rows), first tile, end tile | part); a symmetric unit
+        // starts at the tile holding its diagonal block
         const uint32_t ubm = Gp.pair ? 2 * SC_BM : SC_BM;
         for (uint32_t gj = 0; gj < Gp.jobs.size(); ++gj) {
             const JobPlan &P = B.jobs[Gp.jobs[gj]];
             const uint32_t ub0 = P.q0 / ubm, ub1 = (P.q1 + ubm - 1) / ubm;
             for (uint32_t rb = ub0; rb < ub1; ++rb) {
-                const uint32_t first = P.sym ? rb / 2 : 0u;
+                const uint32_t first = P.sym ? rb * ubm / SC_BN : 0u;
                 for (uint32_t part = 0, t0 = first; t0 < P.col_tiles; ++part, t0 += P.ept) {
                     const uint32_t t1 = std::min<uint32_t>(P.col_tiles, t0 + P.ept);
                     Gp.eunits.push_back(make_uint4(gj | (P.sym ? 0x80000000u : 0u), rb, t0, t1 | (part << 24)));
@@ -410,15 +410,20 @@ static int plan_batch(const hm_job *user_specs, uint32_t user_jobs, hm_batch &B,
             std::stable_sort(Gp.eunits.begin(), Gp.eunits.end(), [](const uint4 &a, const uint4 &b) {
                 return (a.w & 0xffffffu) - a.z > (b.w & 0xffffffu) - b.z;
             });
-        Gp.egrid = std::min<uint32_t>((uint32_t)Gp.eunits.size(), G);
+        // CTAs of the emission pass (the 2-SM form runs two per unit, at most
+        // one per SM): the column-side stages are per CTA
+        const uint64_t eunits_n = Gp.eunits.size();
+        Gp.egrid = (uint32_t)std::min<uint64_t>(Gp.pair ? 2 * eunits_n : eunits_n, G);
         if (Gp.any_sym) {
-            // column-side candidates staged per CTA: room for half of every
-            // sym row's expected list share (a full stage sends the affected
+            // column-side candidates staged per epilogue warp of every CTA
+            // (SC_STAGE_SLOTS stages per CTA): room for half of every sym
+            // row's expected list share (a full stage sends the affected
             // rows to the exact path, it never loses a candidate silently)
             uint64_t want = 0;
             for (uint32_t j : Gp.jobs)
                 if (B.jobs[j].sym) want += B.jobs[j].spec.n * (uint64_t)B.jobs[j].cap / 2;
-            Gp.stage_cap = (uint32_t)std::min<uint64_t>(0x7fffffffull, (want + Gp.egrid - 1) / Gp.egrid + 4096);
+            const uint64_t slots = (uint64_t)Gp.egrid * SC_STAGE_SLOTS;
+            Gp.stage_cap = (uint32_t)std::min<uint64_t>(0x7fffffffull, (want + slots - 1) / slots + 512);
         }
     }
 
@@ -532,9 +537,10 @@ static int plan_batch(const hm_job *user_specs, uint32_t user_jobs, hm_batch &B,
             const size_t padded = round_up(rows, SC_BN) + SC_BN;
             Gp.off_ethr = take(padded * sizeof(float));
             Gp.off_evstar = take(padded * sizeof(float));
-            Gp.off_stage_row = take((size_t)Gp.egrid * Gp.stage_cap * sizeof(uint32_t));
-            Gp.off_stage_key = take((size_t)Gp.egrid * Gp.stage_cap * sizeof(unsigned long long));
-            Gp.off_stage_cnt = take((size_t)Gp.egrid * sizeof(uint32_t));
+            const size_t slots = (size_t)Gp.egrid * SC_STAGE_SLOTS;
+            Gp.off_stage_row = take(slots * Gp.stage_cap * sizeof(uint32_t));
+            Gp.off_stage_key = take(slots * Gp.stage_cap * sizeof(unsigned long long));
+            Gp.off_stage_cnt = take(slots * sizeof(uint32_t));
         }
     }
     B.total = off;
@@ -759,10 +765,13 @@ static int run_batch(hm_batch &B, cudaStream_t s) {
         // lists no unit writes (parts a row block does not have) and the
         // column lists the scatter fills start empty
         HM_CUDA_TRY(cudaMemsetAsync(Gp.host.cand_cnt, 0, Gp.elists * sizeof(uint32_t), s));
+        // (stages of CTAs the emission pass does not launch stay empty)
+        if (Gp.any_sym)
+            HM_CUDA_TRY(cudaMemsetAsync(Gp.host.stage_cnt, 0, (size_t)Gp.egrid * SC_STAGE_SLOTS * sizeof(uint32_t), s));
         if (Gp.any_sym) HM_TRY(launch_emit_limits(jobs, Gp.host, Gd, s));
         HM_TRY(launch_screen_gemm(jobs, Gp.host, Gd, Gp.kp, Gp.ta, Gp.pair ? Gp.tb_half : Gp.tb, nullptr,
                                   Gp.any_sym ? 2 : 1, s));
-        if (Gp.any_sym) HM_TRY(launch_column_scatter(jobs, Gp.host, Gd, Gp.egrid, s));
+        if (Gp.any_sym) HM_TRY(launch_column_scatter(jobs, Gp.host, Gd, Gp.egrid * SC_STAGE_SLOTS, s));
         HM_TRY(launch_rerank(jobs, Gp.host, Gd, Gp.kpl, Gp.dmax, Gp.metric_mask, s));
     }
     if (B.any_screen) {

@@ -22,8 +22,9 @@
 namespace hm {
 
 static thread_local uint32_t g_seed_override = 0;
-static thread_local bool g_symmetric = true;
-static thread_local bool g_pair = true;
+// emission forms: -1 the table's choice, 0 never, 1 wherever a job can take it
+static thread_local int g_symmetric = -1;
+static thread_local int g_pair = -1;
 static thread_local bool g_escalation = true;
 
 template <size_t N>
@@ -58,12 +59,11 @@ int autotune_choice(uint64_t n, uint32_t d, uint32_t k, int metric, uint32_t *se
     }
     const uint16_t e = table_entry(n, d, k, metric, batched);
     if (seed_div) *seed_div = g_seed_override ? g_seed_override : (uint32_t)((e >> 8) & 0x7f);
-    if (symmetric) *symmetric = g_symmetric && (e >> 15) != 0;
-    if (pair) *pair = ((e >> 4) & 1) != 0;
+    if (symmetric) *symmetric = g_symmetric < 0 ? (e >> 15) != 0 : g_symmetric != 0;
+    if (pair) *pair = g_pair < 0 ? ((e >> 4) & 1) != 0 : g_pair != 0;
     return (int)(e & 0xf);
 }
 
-bool tuning_pair() { return g_pair; }
 bool tuning_escalation() { return g_escalation; }
 
 }  // namespace hm
@@ -86,13 +86,15 @@ int hm_tuning_override(int seed_div) {
     return HM_OK;
 }
 
-int hm_tuning_symmetric(int on) {
-    g_symmetric = on != 0;
+int hm_tuning_symmetric(int mode) {
+    if (mode < -1 || mode > 1) return set_error(HM_ERR_INVALID, "symmetric mode %d outside [-1, 1]", mode);
+    g_symmetric = mode;
     return HM_OK;
 }
 
-int hm_tuning_pair(int on) {
-    g_pair = on != 0;
+int hm_tuning_pair(int mode) {
+    if (mode < -1 || mode > 1) return set_error(HM_ERR_INVALID, "pair mode %d outside [-1, 1]", mode);
+    g_pair = mode;
     return HM_OK;
 }
 

@@ -239,14 +239,11 @@ __device__ __forceinline__ uint32_t find_job(const uint32_t *starts, uint32_t nj
 int kpl_for_k(uint32_t k);  // 1, 2, 4, 8 or 0 if k > 256
 
 // The autotuner table's path for a problem, (seed_div) the fraction
-// 1/seed_div of the columns the screen's threshold pass samples, and
-// (symmetric) whether its emission pass takes the symmetric form (never when
-// hm_tuning_symmetric(0) is in force on this thread).
+// 1/seed_div of the columns the screen's threshold pass samples, and whether
+// its emission pass takes the symmetric form and the 2-SM form (unless
+// hm_tuning_symmetric / hm_tuning_pair force either on this thread).
 int autotune_choice(uint64_t n, uint32_t d, uint32_t k, int metric, uint32_t *seed_div, bool *symmetric,
                     bool *pair, bool batched);
-// Whether screened plans made on this thread may run the emission pass in
-// the 2-SM form (hm_tuning_pair).
-bool tuning_pair();
 // Whether jobs left to the autotuner on the BF16 or TF32 screen carry a
 // split-BF16 escalation copy (hm_tuning_escalation).
 bool tuning_escalation();

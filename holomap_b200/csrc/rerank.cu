@@ -644,10 +644,10 @@ int launch_emit_limits(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd
 }
 
 // Symmetric emission: the column-side candidates the emission pass staged
-// (per CTA: the column's group row, the raw product and the candidate row)
-// move into the rows' column lists with their exact screened values
-// c^_ji = rowterm_j + colterm_i - scale v, the arithmetic row j's own tiles
-// use.  blockIdx.y is the staging CTA.
+// (per epilogue warp: the column's group row, the raw product and the
+// candidate row) move into the rows' column lists with their exact screened
+// values c^_ji = rowterm_j + colterm_i - scale v, the arithmetic row j's own
+// tiles use.  blockIdx.y is the stage (CTA x SC_STAGE_SLOTS + warp).
 __global__ void __launch_bounds__(256) column_scatter_kernel(const JobDev *__restrict__ jobs,
                                                             const GroupDev *__restrict__ Gp) {
     const GroupDev &G = *Gp;

@@ -43,17 +43,20 @@ constexpr uint32_t SC_ARES_STAGES = 6;
 // Epilogue warps per CTA: warp 0 issues the TMA loads, warp 1 the MMAs, the
 // rest read the accumulator, (warp & 3) naming their TMEM lane quadrant (32
 // query rows) and (warp - 2) / 4 their segment of the tile's 256 columns.
-// The full emission pass takes 16 (four segments of 64 columns: twice the
+// Both emission passes take 16 (four segments of 64 columns: twice the
 // warps to hide the latency of the per-row tests; each warp writes its own
 // list, so a row has four lists per column part); the threshold pass (its
-// sorted arrays need the registers) and the symmetric emission pass take 8
-// (two segments of 128 columns).  A 16-warp threshold pass for k <= 32
-// (96 registers, some spilled, four k-arrays per part) measured slower.
+// sorted arrays need the registers) takes 8 (two segments of 128 columns).
+// A 16-warp threshold pass for k <= 32 (96 registers, some spilled, four
+// k-arrays per part) measured slower.
 __host__ __device__ constexpr int sc_epi_warps(int pass, int kp = 32) {
-    return (pass == 1 && kp > 0) ? 16 : 8;
+    return (pass >= 1 && kp > 0) ? 16 : 8;
 }
 __host__ __device__ constexpr int sc_threads(int pass, int kp = 32) { return 64 + 32 * sc_epi_warps(pass, kp); }
-constexpr int SC_FULL_LISTS = 4;  // candidate lists per row and column part of the full emission pass
+constexpr int SC_FULL_LISTS = 4;  // candidate lists per row and column part of the emission passes
+// column-side candidate stages per CTA of the symmetric emission pass (one
+// per epilogue warp)
+constexpr int SC_STAGE_SLOTS = 16;
 
 enum ScreenKind { SCREEN_KIND_BF16 = 0, SCREEN_KIND_TF32 = 1 };
 

@@ -27,8 +27,8 @@
 //   2  the emission pass of a group whose whole datasets take the symmetric
 //      form: a row block walks only the tiles from its diagonal on, with the
 //      limit tau1 + 2 band, and each value above the diagonal is also tested
-//      for its column's row (staged per CTA, moved to that row's column list
-//      by column_scatter_kernel).
+//      for its column's row (one ballot per column; staged per epilogue
+//      warp, moved to that row's column list by column_scatter_kernel).
 // Work units are (row block of 128, column part); the columns of a unit are
 // walked in 256-wide tiles with the two accumulators double buffered, so the
 // epilogue of one tile overlaps the MMAs of the next.
@@ -284,7 +284,6 @@ __global__ void __launch_bounds__(sc_threads(PASS, KP), 1)
     uint64_t *aempty = afull + 1;           // resident A consumed by the unit's MMAs
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(aempty + 1);
     volatile uint32_t *abort_flag = tmem_slot + 1;
-    uint32_t *s_colcnt = tmem_slot + 2;  // column-side candidates this CTA staged
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t nunits = PASS >= 1 ? G.neunits : G.units;
@@ -298,6 +297,7 @@ __global__ void __launch_bounds__(sc_threads(PASS, KP), 1)
     // column-side tests exist only in that instantiation)
     constexpr bool SYMK = PASS == 2;
     constexpr uint32_t EW = sc_epi_warps(PASS, KP);  // epilogue warps
+    static_assert(!SYMK || EW == SC_STAGE_SLOTS, "one column-side stage per epilogue warp");
     constexpr uint32_t NSEG = EW / 4;             // column segments per tile (= lists per part)
     constexpr uint32_t SEGW = SC_BN / NSEG;       // columns per segment
 
@@ -314,7 +314,6 @@ __global__ void __launch_bounds__(sc_threads(PASS, KP), 1)
         mbar_init(smem_u32(afull), 1);
         mbar_init(smem_u32(aempty), 1);
         *abort_flag = 0;
-        *s_colcnt = 0;
         mbar_init_fence();
     }
     if (warp == 1) {
@@ -492,6 +491,10 @@ __global__ void __launch_bounds__(sc_threads(PASS, KP), 1)
         const uint32_t seg = (uint32_t)(warp - 2) >> 2;
         const uint32_t row_in_tile = quad * 32 + lane;
         const float INF = __int_as_float(0x7f800000);
+        // symmetric pass: this warp's stage of column-side candidates
+        const uint32_t stage_slot = blockIdx.x * EW + (uint32_t)(warp - 2);
+        const size_t stage0 = (size_t)stage_slot * G.stage_cap;
+        uint32_t staged = 0;
         uint32_t tile = 0;
         bool ok = true;
         for (uint32_t u = wid; ok && u < nunits; u += nworkers) {
@@ -541,24 +544,39 @@ __global__ void __launch_bounds__(sc_threads(PASS, KP), 1)
 
             for (uint32_t ct = ut.ct_begin; ct < ut.ct_end; ++ct, ++tile) {
                 const uint32_t buf = tile & 1, use = tile >> 1;
-                // symmetric emission: this warp's 128 columns form block jb of
-                // the job; below the row block's diagonal its pairs belong to
-                // another unit's column side, above it they also serve the
-                // columns' rows
-                const uint32_t jb = 2 * ct + seg;  // (NSEG = 2 here)
-                const bool skip = SYMK && ut.sym && jb < myrb;
-                const bool colside = SYMK && ut.sym && jb > myrb && jb * (uint32_t)(SC_BN / 2) < n;
+                // symmetric emission: this warp's 64 columns lie in 128-column
+                // block jb of the job; below the row block's diagonal its pairs
+                // belong to another unit's column side, above it they also
+                // serve the columns' rows
                 const uint32_t c_base = ct * SC_BN + seg * SEGW;
+                const uint32_t jb = c_base / SC_BM;
+                const bool skip = SYMK && ut.sym && jb < myrb;
+                const bool colside = SYMK && ut.sym && jb > myrb && c_base < n;
                 // the columns' limits (lane t holds column c_base + 32 q + t),
                 // loaded while the accumulator is still being filled
-                float cthr[4] = {-INF, -INF, -INF, -INF}, cvs[4] = {INF, INF, INF, INF}, cterm[4] = {0, 0, 0, 0};
+                constexpr int CQ = SEGW / 32;
+                float cthr[CQ], cvs[CQ], cterm[CQ];
+#pragma unroll
+                for (int q = 0; q < CQ; ++q) {
+                    cthr[q] = -INF;
+                    cvs[q] = INF;
+                    cterm[q] = 0.0f;
+                }
+                // and each 8-column group's smallest v* (lane t: its group's)
+                float cgmin[CQ];
+#pragma unroll
+                for (int q = 0; q < CQ; ++q) cgmin[q] = INF;
                 if (SYMK && colside) {
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
+                    for (int q = 0; q < CQ; ++q) {
                         const size_t gc = (size_t)J.row0 + c_base + 32 * q + lane;
                         cthr[q] = G.ethr[gc];
                         cvs[q] = G.evstar[gc];
                         cterm[q] = G.colterm[gc];
+                        float m = cvs[q];
+                        m = fminf(m, __shfl_xor_sync(0xffffffffu, m, 1));
+                        m = fminf(m, __shfl_xor_sync(0xffffffffu, m, 2));
+                        cgmin[q] = fminf(m, __shfl_xor_sync(0xffffffffu, m, 4));
                     }
                 }
                 const bool got = mbar_wait(smem_u32(&accf[buf]), use & 1, abort_flag);
@@ -586,8 +604,8 @@ __global__ void __launch_bounds__(sc_threads(PASS, KP), 1)
                 }
                 const bool diag = (ct * SC_BN < myrb * SC_BM + SC_BM) && (myrb * SC_BM < ct * SC_BN + SC_BN);
                 const uint32_t t_base = tmem_base + ((quad * 32) << 16) + buf * SC_BN + seg * SEGW;
-                // one chunk = 32 columns; the accumulator registers are
-                // overwritten in place by the screened values
+                // the threshold pass's chunk = 32 columns; the accumulator
+                // registers are overwritten in place by the screened values
                 auto process = [&](uint32_t (&v)[32], uint32_t ch) {
                     float (&c)[32] = reinterpret_cast<float (&)[32]>(v);
                     const uint32_t j0 = c_base + ch * 32;  // job-local column
@@ -622,80 +640,9 @@ __global__ void __launch_bounds__(sc_threads(PASS, KP), 1)
                                 if (j0 + t == row) c[t] = 0.0f;
                         }
                     };
-                    // symmetric emission, column side, on the raw products:
-                    // column j of the chunk takes this row as a candidate when
-                    // c^_ji <= its limit (cosine without zero rows: the raw
-                    // product against the column's v* form, a superset)
-                    if (SYMK && colside) {
-                        const float cl_thr = ch == 0 ? cthr[0] : ch == 1 ? cthr[1] : ch == 2 ? cthr[2] : cthr[3];
-                        const float cl_vs = ch == 0 ? cvs[0] : ch == 1 ? cvs[1] : ch == 2 ? cvs[2] : cvs[3];
-                        const float cl_term = ch == 0 ? cterm[0] : ch == 1 ? cterm[1] : ch == 2 ? cterm[2] : cterm[3];
-                        uint32_t colmask = 0;
-                        if (fast_cos) {
-                            float m = cl_vs;  // smallest v* of each 8-column group
-                            m = fminf(m, __shfl_xor_sync(0xffffffffu, m, 1));
-                            m = fminf(m, __shfl_xor_sync(0xffffffffu, m, 2));
-                            m = fminf(m, __shfl_xor_sync(0xffffffffu, m, 4));
-#pragma unroll
-                            for (int g = 0; g < 4; ++g) {
-                                const float cm = __shfl_sync(0xffffffffu, m, 8 * g);
-                                float x = c[8 * g];
-#pragma unroll
-                                for (int e = 1; e < 8; ++e) x = fmaxf(x, c[8 * g + e]);
-                                if (__any_sync(0xffffffffu, valid && x >= cm)) {
-#pragma unroll
-                                    for (int e = 0; e < 8; ++e) {
-                                        const float vs = __shfl_sync(0xffffffffu, cl_vs, 8 * g + e);
-                                        if (valid && c[8 * g + e] >= vs && j0 + 8 * g + e < n)
-                                            colmask |= 1u << (8 * g + e);
-                                    }
-                                }
-                            }
-                        } else {
-                            const bool euc = J.metric == HM_METRIC_EUCLIDEAN;
-#pragma unroll
-                            for (int t = 0; t < 32; ++t) {
-                                const float lim = __shfl_sync(0xffffffffu, cl_thr, t);
-                                const float rt = __shfl_sync(0xffffffffu, cl_term, t);
-                                const float c2 = __fsub_rn(__fadd_rn(euc ? rt : 0.0f, own_ct), __fmul_rn(scale, c[t]));
-                                if (valid && j0 + t < n && !(c2 > lim)) colmask |= 1u << t;
-                            }
-                        }
-                        // stage them: one shared-memory atomic per warp and chunk
-                        const uint32_t mine = __popc(colmask);
-                        uint32_t inc = mine;
-#pragma unroll
-                        for (int o = 1; o < 32; o <<= 1) {
-                            const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
-                            if (lane >= o) inc += y;
-                        }
-                        const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
-                        if (total) {
-                            uint32_t base = 0;
-                            if (lane == 0) base = atomicAdd(s_colcnt, total);
-                            uint32_t pos = __shfl_sync(0xffffffffu, base, 0) + inc - mine;
-                            colsum += mine;
-                            while (colmask) {
-                                const int t = __ffs(colmask) - 1;
-                                colmask &= colmask - 1;
-                                float x = c[0];
-#pragma unroll
-                                for (int q = 1; q < 32; ++q) x = (t == q) ? c[q] : x;
-                                if (pos < G.stage_cap) {
-                                    const size_t at = (size_t)blockIdx.x * G.stage_cap + pos;
-                                    G.stage_row[at] = J.row0 + j0 + t;
-                                    G.stage_key[at] = ((unsigned long long)__float_as_uint(x) << 32) | row;
-                                } else {
-                                    // a full stage: the column's row goes to the exact path
-                                    atomicMax(&G.cand_cnt[cand_list(J, j0 + t, J.elists - 2)], 2 * J.cap + 1);
-                                }
-                                ++pos;
-                            }
-                        }
-                    }
                     // cosine fast path: c = 1 - v is monotone in v, so a
                     // minimum of c is 1 - (the maximum of v), bit for bit
-                    const bool quick = fast_cos && full && !self_here && (PASS >= 1 || !dump);
+                    const bool quick = fast_cos && full && !self_here && !dump;
                     if (PASS == 0) {
                         // mini-chunk minima: columns {t, t+8, t+16, t+24}
                         float m[8];
@@ -750,78 +697,78 @@ __global__ void __launch_bounds__(sc_threads(PASS, KP), 1)
                                 published = tl;
                             }
                         }
-                    } else {
-                        // emission: 8-column groups gate the per-column work,
-                        // which is divergent (the warp's lanes are 32 rows)
-                        auto emit_group = [&](uint32_t pm, int g, bool raw) {
-                            while (pm) {
-                                const int e = __ffs(pm) - 1;
-                                pm &= pm - 1;
-                                const float a0 = (e & 1) ? c[8 * g + 1] : c[8 * g];
-                                const float a1 = (e & 1) ? c[8 * g + 3] : c[8 * g + 2];
-                                const float a2 = (e & 1) ? c[8 * g + 5] : c[8 * g + 4];
-                                const float a3 = (e & 1) ? c[8 * g + 7] : c[8 * g + 6];
-                                const float b0 = (e & 2) ? a1 : a0, b1 = (e & 2) ? a3 : a2;
-                                float x = (e & 4) ? b1 : b0;
-                                if (raw) x = __fsub_rn(1.0f, x);
-                                if (cnt < J.cap)
-                                    cand[cnt] = ((unsigned long long)__float_as_uint(x) << 32) | (j0 + 8 * g + e);
-                                ++cnt;
-                            }
-                        };
-                        if (quick) {
-                            // c = 1 - v <= thr  <=>  v >= vstar (vstar a hair low:
-                            // a superset, the rerank filters exactly)
-                            float gm[4];
-#pragma unroll
-                            for (int g = 0; g < 4; ++g) {
-                                float x = c[8 * g];
-#pragma unroll
-                                for (int e = 1; e < 8; ++e) x = fmaxf(x, c[8 * g + e]);
-                                gm[g] = x;
-                            }
-                            if (valid && fmaxf(fmaxf(gm[0], gm[1]), fmaxf(gm[2], gm[3])) >= vstar) {
-#pragma unroll
-                                for (int g = 0; g < 4; ++g) {
-                                    if (gm[g] >= vstar) {
-                                        uint32_t pm = 0;
-#pragma unroll
-                                        for (int e = 0; e < 8; ++e) pm |= (c[8 * g + e] >= vstar) ? (1u << e) : 0u;
-                                        emit_group(pm, g, true);
-                                    }
-                                }
-                            }
-                        } else {
-                            values();
-                            float gm[4];
-#pragma unroll
-                            for (int g = 0; g < 4; ++g) {
-                                float x = c[8 * g];
-#pragma unroll
-                                for (int e = 1; e < 8; ++e) x = fminf(x, c[8 * g + e]);
-                                gm[g] = x;
-                            }
-                            if (valid && !(fminf(fminf(gm[0], gm[1]), fminf(gm[2], gm[3])) > thr)) {
-#pragma unroll
-                                for (int g = 0; g < 4; ++g) {
-                                    if (!(gm[g] > thr)) {
-                                        uint32_t pm = 0;
-#pragma unroll
-                                        for (int e = 0; e < 8; ++e)
-                                            pm |= (!(c[8 * g + e] > thr) && j0 + 8 * g + e < n) ? (1u << e) : 0u;
-                                        emit_group(pm, g, false);
-                                    }
-                                }
-                            }
-                        }
                     }
                 };
                 if constexpr (EW >= 16) {
                     // the full emission pass (96 registers a thread): 16-column
                     // loads, the next in flight while this one is tested
                     const uint32_t cap = J.cap;
+                    // symmetric emission, column side, on the raw products:
+                    // column j of the chunk takes this row as a candidate when
+                    // c^_ji <= its limit (cosine without zero rows: the raw
+                    // product against the column's v* form, a superset); one
+                    // ballot per column names the warp's rows that it takes,
+                    // staged for column_scatter_kernel
+                    static_assert(!SYMK || CQ == 2, "two 32-column register slices per 64-column segment");
+                    auto colside16 = [&](const float (&c)[16], uint32_t j0) {
+                        const uint32_t cc = (j0 - c_base) >> 4;  // chunk of the segment
+                        const bool hi = (cc >> 1) != 0;
+                        const float thr_q = hi ? cthr[CQ - 1] : cthr[0];
+                        const float vs_q = hi ? cvs[CQ - 1] : cvs[0];
+                        const float term_q = hi ? cterm[CQ - 1] : cterm[0];
+                        const float gmin_q = hi ? cgmin[CQ - 1] : cgmin[0];
+                        const uint32_t lb = 16u * (cc & 1u);  // the chunk's first column's lane
+                        const bool euc = J.metric == HM_METRIC_EUCLIDEAN;
+                        // the warp's own stage (no atomics): its count is
+                        // uniform over the warp
+                        auto stage = [&](uint32_t m, int t) {
+                            const uint32_t base = staged;
+                            staged += (uint32_t)__popc(m);
+                            if (lane == 0) colsum += (uint32_t)__popc(m);
+                            if (m & (1u << lane)) {
+                                const uint32_t pos = base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+                                if (pos < G.stage_cap) {
+                                    const size_t at = stage0 + pos;
+                                    G.stage_row[at] = J.row0 + j0 + t;
+                                    G.stage_key[at] = ((unsigned long long)__float_as_uint(c[t]) << 32) | row;
+                                } else {
+                                    // a full stage: the column's row goes to the exact path
+                                    atomicMax(&G.cand_cnt[cand_list(J, j0 + t, J.elists - 2)], 2 * J.cap + 1);
+                                }
+                            }
+                        };
+                        if (fast_cos) {
+#pragma unroll
+                            for (int g = 0; g < 2; ++g) {
+                                float x = c[8 * g];
+#pragma unroll
+                                for (int e = 1; e < 8; ++e) x = fmaxf(x, c[8 * g + e]);
+                                const float cm = __shfl_sync(0xffffffffu, gmin_q, (int)lb + 8 * g);
+                                if (!__any_sync(0xffffffffu, valid && x >= cm)) continue;
+#pragma unroll
+                                for (int e = 0; e < 8; ++e) {
+                                    const int t = 8 * g + e;
+                                    const float vs = __shfl_sync(0xffffffffu, vs_q, (int)lb + t);
+                                    const uint32_t m = __ballot_sync(0xffffffffu, valid && c[t] >= vs && j0 + t < n);
+                                    if (m) stage(m, t);
+                                }
+                            }
+                        } else {
+#pragma unroll
+                            for (int t = 0; t < 16; ++t) {
+                                const float lim = __shfl_sync(0xffffffffu, thr_q, (int)lb + t);
+                                const float rt = __shfl_sync(0xffffffffu, term_q, (int)lb + t);
+                                const float c2 = __fsub_rn(__fadd_rn(euc ? rt : 0.0f, own_ct), __fmul_rn(scale, c[t]));
+                                const uint32_t m = __ballot_sync(0xffffffffu, valid && j0 + t < n && !(c2 > lim));
+                                if (m) stage(m, t);
+                            }
+                        }
+                    };
                     auto emit16 = [&](uint32_t (&v)[16], uint32_t j0) {
                         float (&c)[16] = reinterpret_cast<float (&)[16]>(v);
+                        if constexpr (SYMK) {
+                            if (colside) colside16(c, j0);
+                        }
                         const bool full = j0 + 16 <= n;
                         const bool self_here = diag && (row - j0 < 16u);
                         auto put = [&](uint32_t pm, int g, bool raw) {
@@ -961,6 +908,7 @@ __global__ void __launch_bounds__(sc_threads(PASS, KP), 1)
                 if (lane == 0 && e) atomicAdd(&J.out->emitted, (unsigned long long)e);
             }
         }
+        if (SYMK && lane == 0 && G.stage_cnt) G.stage_cnt[stage_slot] = staged;
     }
 
     fence_before_sync();
@@ -975,7 +923,7 @@ __global__ void __launch_bounds__(sc_threads(PASS, KP), 1)
             asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
                          "r"(SC_TMEM_COLS));
     }
-    if (SYMK && threadIdx.x == 0 && G.stage_cnt) G.stage_cnt[blockIdx.x] = *s_colcnt;
+
 }
 
 // clusters of two screen CTAs the device can hold at once (per device,
@@ -1006,12 +954,12 @@ static uint32_t pair_slots(const void *func) {
     return (uint32_t)clusters;
 }
 
-// the emission pass in the 2-SM form: clusters of two, the A block resident
+// an emission pass in the 2-SM form: clusters of two, the A block resident
 // in each CTA, one MMA of M = 256 per K step
-template <int KIND>
+template <int KIND, int PASS>
 static int launch_pair(const JobDev *jobs, const GroupDev &G, const CUtensorMap &ta, const CUtensorMap &tb,
                        uint32_t idesc, cudaStream_t s) {
-    const void *func = (const void *)screen_gemm_kernel<KIND, 32, 1, true>;
+    const void *func = (const void *)screen_gemm_kernel<KIND, 32, PASS, true>;
     HM_TRY(ensure_dynamic_smem(func, (int)SC_SMEM_BYTES));
     const uint32_t slots = pair_slots(func);
     if (slots == 0) return set_error(HM_ERR_CUDA, "no room for a cluster of two screen CTAs");
@@ -1019,7 +967,7 @@ static int launch_pair(const JobDev *jobs, const GroupDev &G, const CUtensorMap 
     if (clusters == 0) return HM_OK;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(2 * clusters, 1, 1);
-    cfg.blockDim = dim3(sc_threads(1), 1, 1);
+    cfg.blockDim = dim3(sc_threads(PASS), 1, 1);
     cfg.dynamicSmemBytes = SC_SMEM_BYTES;
     cfg.stream = s;
     cudaLaunchAttribute attr;
@@ -1030,7 +978,7 @@ static int launch_pair(const JobDev *jobs, const GroupDev &G, const CUtensorMap 
     cfg.attrs = &attr;
     cfg.numAttrs = 1;
     const uint32_t pidesc = (idesc & ~(0x1fu << 24)) | (((uint32_t)(2 * SC_BM) >> 4) << 24);  // M = 256
-    HM_CUDA_TRY(cudaLaunchKernelEx(&cfg, screen_gemm_kernel<KIND, 32, 1, true>, ta, tb, jobs, G,
+    HM_CUDA_TRY(cudaLaunchKernelEx(&cfg, screen_gemm_kernel<KIND, 32, PASS, true>, ta, tb, jobs, G,
                                    (float *)nullptr, pidesc, 1u));
     count_launch();
     return HM_OK;
@@ -1039,8 +987,8 @@ static int launch_pair(const JobDev *jobs, const GroupDev &G, const CUtensorMap 
 template <int KIND, int KP, int PASS>
 static int launch_kind(const JobDev *jobs, const GroupDev &G, const CUtensorMap &ta,
                        const CUtensorMap &tb, float *dump, uint32_t idesc, cudaStream_t s) {
-    if constexpr (PASS == 1 && KP == 32) {
-        if (G.pair) return launch_pair<KIND>(jobs, G, ta, tb, idesc, s);
+    if constexpr (PASS >= 1 && KP == 32) {
+        if (G.pair) return launch_pair<KIND, PASS>(jobs, G, ta, tb, idesc, s);
     }
     HM_TRY(ensure_dynamic_smem((const void *)screen_gemm_kernel<KIND, KP, PASS, false>, (int)SC_SMEM_BYTES));
     const uint32_t sms = (uint32_t)device_sm_count();

@@ -396,18 +396,19 @@ HM_API int hm_autotune_path_batched(uint64_t n, uint32_t d, uint32_t k, int metr
  * screen's threshold pass instead of the table's fraction; 0 restores the
  * table.  The results do not depend on it, only the speed. */
 HM_API int hm_tuning_override(int seed_div);
-/* Sweep and test hook (no reference counterpart): with on = 0, screened plans
- * made on this thread run the emission pass over every column tile instead of
- * only the tiles on and above the diagonal (each tile's values then serve its
- * rows only).  Same results; on = 1 (the default) restores the symmetric
- * form. */
-HM_API int hm_tuning_symmetric(int on);
-/* Sweep and test hook (no reference counterpart): with on = 0, screened plans
- * made on this thread run the emission pass with one CTA per 128-row block
- * instead of the 2-SM form (a cluster of two CTAs sharing one 256-row MMA,
- * each CTA loading half of every column tile).  Same results; on = 1 (the
- * default) restores the 2-SM form where a group can take it. */
-HM_API int hm_tuning_pair(int on);
+/* Sweep and test hook (no reference counterpart): the emission form of the
+ * screened plans made on this thread.  mode = 0: the pass runs over every
+ * column tile; mode = 1: the symmetric form wherever a job can take it (a
+ * whole dataset of at least two column tiles: only the tiles on and above
+ * the diagonal, each value also serving its column's row); mode = -1 (the
+ * default): the autotuner table's choice.  Same results in every mode. */
+HM_API int hm_tuning_symmetric(int mode);
+/* Sweep and test hook (no reference counterpart): mode = 0: the emission pass
+ * runs with one CTA per 128-row block; mode = 1: the 2-SM form (a cluster of
+ * two CTAs sharing one 256-row MMA, each CTA loading half of every column
+ * tile) wherever a group can take it; mode = -1 (the default): the
+ * autotuner table's choice.  Same results in every mode. */
+HM_API int hm_tuning_pair(int mode);
 /* Test hook (no reference counterpart): with on = 0, jobs planned on this
  * thread with HM_PATH_AUTO carry no escalation copy.  By default a job the
  * autotuner sends to the BF16 or TF32 screen also carries a split-BF16 copy:

@@ -149,6 +149,26 @@ def test_tuning_override_bounds():
     assert lib.hm_tuning_override(0) == 0
     assert lib.hm_tuning_override(-1) == hm.HM_ERR_INVALID
     assert lib.hm_tuning_override(65) == hm.HM_ERR_INVALID
+    for hook in (lib.hm_tuning_symmetric, lib.hm_tuning_pair):
+        for mode in (0, 1, -1):  # -1 (the table's choice) restores the default
+            assert hook(mode) == 0
+        assert hook(2) == hm.HM_ERR_INVALID
+        assert hook(-2) == hm.HM_ERR_INVALID
+
+
+def test_symmetric_and_pair_forms_plan_for_the_benchmark_shape():
+    """Every emission form plans for the 50,000 x 384 cosine shape (the
+    symmetric form's lists: at most 7 column parts, 30 lists per row)."""
+    lib = hm.lib()
+    try:
+        for sym in (0, 1):
+            for pair in (0, 1):
+                assert lib.hm_tuning_symmetric(sym) == 0
+                assert lib.hm_tuning_pair(pair) == 0
+                assert hm.workspace_bytes(50000, 384, 30, "cosine", "screen_bf16") > 0
+    finally:
+        lib.hm_tuning_symmetric(-1)
+        lib.hm_tuning_pair(-1)
 
 
 def test_every_screened_path_plans_for_the_benchmark_shapes():

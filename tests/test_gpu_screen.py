@@ -131,35 +131,42 @@ def test_device_data_at_a_4_byte_offset(oracle, path):
 
 @pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("metric", ["euclidean", "cosine"])
-def test_full_and_symmetric_emission_agree_with_the_oracle(oracle, path, metric):
+@pytest.mark.parametrize("n", [2600, 3000])
+def test_full_and_symmetric_emission_agree_with_the_oracle(oracle, path, metric, n):
     """The emission pass over every column tile (hm_tuning_symmetric(0)) and
-    over the tiles on and above the diagonal only (the default, whose rows
-    also take candidates as columns) return the oracle's bytes; the zero rows
-    under cosine exercise the column side's general (non raw-product) test."""
+    over the tiles on and above the diagonal only (hm_tuning_symmetric(1),
+    whose rows also take candidates as columns), each with one CTA per
+    128-row block and in the 2-SM form, return the oracle's bytes; the zero
+    rows under cosine exercise the column side's general (non raw-product)
+    test, and n = 3000 ends inside a 256-row block's second half."""
     lib = hm.lib()
-    x = edge_case("zeros" if metric == "cosine" else "duplicates", 2600, 40, seed=5)
+    x = edge_case("zeros" if metric == "cosine" else "duplicates", n, 40, seed=5)
     x[::7] += 0.5  # keep most rows non-zero
     oi, od = oracle.exact_knn(x, 15, metric)
     osig, orho = oracle.smooth_knn(od, 15)
     for sym in (0, 1):
-        assert lib.hm_tuning_symmetric(sym) == 0
-        try:
-            st = hm.HmStats()
-            knn, sm = hm.knn_smooth(x, 40, 15, metric, path, stats=st)
-        finally:
-            lib.hm_tuning_symmetric(1)
-        assert_same_bytes(knn.indices, oi, f"sym={sym} indices")
-        assert_same_bytes(knn.dists, od, f"sym={sym} dists")
-        assert_same_bytes(sm.sigmas, osig, f"sym={sym} sigma")
-        assert_same_bytes(sm.rhos, orho, f"sym={sym} rho")
+        for pair in (0, 1):
+            assert lib.hm_tuning_symmetric(sym) == 0
+            assert lib.hm_tuning_pair(pair) == 0
+            try:
+                st = hm.HmStats()
+                knn, sm = hm.knn_smooth(x, 40, 15, metric, path, stats=st)
+            finally:
+                lib.hm_tuning_symmetric(-1)
+                lib.hm_tuning_pair(-1)
+            what = f"sym={sym} pair={pair}"
+            assert_same_bytes(knn.indices, oi, f"{what} indices")
+            assert_same_bytes(knn.dists, od, f"{what} dists")
+            assert_same_bytes(sm.sigmas, osig, f"{what} sigma")
+            assert_same_bytes(sm.rhos, orho, f"{what} rho")
 
 
 @pytest.mark.parametrize("path", PATHS)
 @pytest.mark.parametrize("n", [200, 1000, 2600])
 def test_pair_and_single_cta_emission_agree_with_the_oracle(oracle, path, n):
-    """The emission pass in the 2-SM form (the default: a cluster of two CTAs
-    shares one 256-row MMA, each loading half of every column tile) and with
-    one CTA per 128-row block (hm_tuning_pair(0)) return the oracle's bytes,
+    """The emission pass in the 2-SM form (hm_tuning_pair(1): a cluster of two
+    CTAs shares one 256-row MMA, each loading half of every column tile) and
+    with one CTA per 128-row block (hm_tuning_pair(0)) return the oracle's bytes,
     including a last 256-row block that ends inside its first half (n = 200,
     1000) and one whose second half lies past every row (n = 2600)."""
     lib = hm.lib()
@@ -171,7 +178,7 @@ def test_pair_and_single_cta_emission_agree_with_the_oracle(oracle, path, n):
         try:
             knn, sm = hm.knn_smooth(x, 40, 15, "euclidean", path)
         finally:
-            lib.hm_tuning_pair(1)
+            lib.hm_tuning_pair(-1)
         assert_same_bytes(knn.indices, oi, f"pair={pair} indices")
         assert_same_bytes(knn.dists, od, f"pair={pair} dists")
         assert_same_bytes(sm.sigmas, osig, f"pair={pair} sigma")
