@@ -57,7 +57,7 @@ def parse_args():
                     help="use only the first ROWS points of the workload (a smaller case "
                          "of the same kernels, e.g. for profiling)")
     ap.add_argument("--e2e-steps", type=int, default=None)
-    ap.add_argument("--e2e-window", type=int, default=3,
+    ap.add_argument("--e2e-window", type=int, default=4,
                     help="requests in flight in the pipelined end-to-end measurement")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the oracle baseline sample")
@@ -448,7 +448,13 @@ class SingleRunner:
         fp = (window + 1) * (lib_workspace(wl, self.path) + wl.n * (wl.d + 2 * wl.k + 2) * 4) + (256 << 20)
         ref_idx = self.prob.idx.cpu().numpy().view(np.uint32).reshape(wl.n, wl.k)
         same = True
-        with Server(memory_bytes=fp, max_inflight=window, max_batch_jobs=1, small_work=1e300) as srv:
+        # the requests are one class (every one counts as large, so every
+        # batch runs at the same stream priority and they finish in order):
+        # 2 x window slots, half of them the low-priority ones large requests
+        # take.  With the classes mixed (all small: two high-priority slots
+        # and one low one for three in flight) C3 measured 317-321 graphs/s
+        # against 339-340 with one class.
+        with Server(memory_bytes=fp, max_inflight=2 * window, max_batch_jobs=1, small_work=1.0) as srv:
             for _ in range(2):  # warm
                 srv.wait(srv.submit(x, wl.k, wl.metric, self.path, outputs=outs[0]))
             pending, done = [], []
@@ -742,7 +748,7 @@ class BatchRunner:
                 ev_out[b].record(s_out)
         torch.cuda.synchronize(dev)
         elapsed = time.perf_counter() - t0
-        same = all(torch_equal(o, self.batch.out) for o in outs)
+        same = all(torch_equal(o, self.batch.out) for o in outs[:min(steps, len(outs))])  # the sets written
         return elapsed, same
 
     def io_bytes(self):
