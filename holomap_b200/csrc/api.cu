@@ -700,6 +700,11 @@ static int bind_batch(hm_batch &B, void *d_ws, size_t bytes, cudaStream_t s) {
         D.eunits = at<uint4>(ws, Gp.off_eunits);
         D.neunits = (uint32_t)Gp.eunits.size();
         D.pair = Gp.pair ? 1u : 0u;
+        for (uint32_t j : Gp.jobs) {
+            const bool short_rows = B.jobs[j].kp1 <= operand_short_k1();
+            D.any_short_rows |= short_rows ? 1u : 0u;
+            D.any_long_rows |= short_rows ? 0u : 1u;
+        }
         if (Gp.any_sym) {
             D.ethr = at<float>(ws, Gp.off_ethr);
             D.evstar = at<float>(ws, Gp.off_evstar);

@@ -238,6 +238,9 @@ __device__ __forceinline__ uint32_t find_job(const uint32_t *starts, uint32_t nj
 
 int kpl_for_k(uint32_t k);  // 1, 2, 4, 8 or 0 if k > 256
 
+// Rows of padded length K1 at most this take the packed operand kernel
+// (several rows per warp); the group's plan records which kernels run.
+uint32_t operand_short_k1();
 // The autotuner table's path for a problem, (seed_div) the fraction
 // 1/seed_div of the columns the screen's threshold pass samples, and whether
 // its emission pass takes the symmetric form and the 2-SM form (unless

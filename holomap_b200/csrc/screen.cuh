@@ -99,6 +99,9 @@ struct GroupDev {
     // emission pass in the 2-SM form (a cluster of two CTAs per unit, one
     // MMA of 256 rows; eunits' y is then a block of 256 rows)
     uint32_t pair;
+    // the group has jobs whose padded row length K1 is at most / above the
+    // packed operand kernel's limit (which operand kernels run)
+    uint32_t any_short_rows, any_long_rows;
     // symmetric emission: per group row (padded like colterm) the emission
     // limit tau1 + 2 band and its cosine raw-product form; the column-side
     // candidates each CTA staged (group row of the column, raw product bits

@@ -110,13 +110,20 @@ __device__ __forceinline__ uint32_t to_tf32_bits(double v, double *rounded) {
     return b;
 }
 
-// operand_kernel: one warp per group row, the warps striding over the rows
-// (a persistent grid of OP_BLOCKS_PER_SM blocks per SM).  A row's loads (up to
-// 512 elements; 256 in the split form) are all issued before its first store,
-// so a row costs one memory round trip; the job's maxima are kept per warp and written (one
-// atomic each) when the warp's next row belongs to another job, or at its end.
+// Operand rows come in two kernels by the padded row length K1 of their job:
+// operand_kernel (K1 > OP_SHORT_K1) gives every row a warp, the warps striding
+// over the rows; operand_packed_kernel (K1 <= OP_SHORT_K1) gives a row 8 or 16
+// lanes, so a warp works on two or four short rows at once.  Both run a
+// persistent grid of OP_BLOCKS_PER_SM blocks per SM; each skips the other's
+// jobs.  A row's loads (up to 512 elements with 32 lanes; 256 in the split
+// form) are all issued before its first store, so a row costs one memory
+// round trip; a job's maxima are kept per warp (per row group) and written,
+// one atomic each, when the warp's next rows belong to another job, or at
+// its end.
 constexpr uint32_t OP_WARPS = 8;
 constexpr int OP_BLOCKS_PER_SM = 3;
+constexpr uint32_t OP_SHORT_K1 = 64;
+uint32_t operand_short_k1() { return OP_SHORT_K1; }
 constexpr int OP_TF32 = 0, OP_BF16 = 1, OP_SPLIT = 2;
 // elements per lane in flight (the split form's six stores per element need
 // the registers of half of them)
@@ -154,7 +161,7 @@ __global__ void __launch_bounds__(OP_WARPS * 32, OP_BLOCKS_PER_SM) operand_kerne
     const uint32_t stride = gridDim.x * OP_WARPS;
     for (uint32_t gr = blockIdx.x * OP_WARPS + warp; gr < G.rows; gr += stride) {
         const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr)]];
-        if (!job_active(J)) continue;
+        if (!job_active(J) || J.kp1 <= OP_SHORT_K1) continue;  // inactive, or operand_packed_kernel's
         const uint32_t row = gr - J.row0;
         if (row >= J.n) {  // padding between jobs: zero operands (read only as masked rows/columns)
             for (uint32_t t = lane; t < G.kpmax; t += 32) {
@@ -276,6 +283,191 @@ __global__ void __launch_bounds__(OP_WARPS * 32, OP_BLOCKS_PER_SM) operand_kerne
     flush();
 }
 
+// The same for the jobs with K1 <= OP_SHORT_K1: the warps stride over tiles
+// of OP_TILE consecutive group rows (a tile lies in one job, whose rows start
+// 32-aligned), a row taking 16 lanes when K1 > 32, else 8.  Every lane
+// accumulates its elements t = s, s + L, ... (s its place among the row's L
+// lanes) in ascending order.
+constexpr uint32_t OP_TILE = 4;  // rows per tile: the most a warp holds at once
+template <int MODE>
+__global__ void __launch_bounds__(OP_WARPS * 32, OP_BLOCKS_PER_SM)
+    operand_packed_kernel(const JobDev *__restrict__ jobs, const GroupDev *__restrict__ Gp) {
+    // the maxima of each of the warp's row groups (a group's first lane alone
+    // updates them)
+    __shared__ double s_wmax[OP_WARPS][OP_TILE][6];
+    __shared__ unsigned long long s_wzero[OP_WARPS][OP_TILE];
+    const GroupDev &G = *Gp;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const JobDev *cur = nullptr;  // the job whose maxima the warp holds
+    auto reset = [&]() {
+        if (lane < (int)OP_TILE) {
+            for (int q = 0; q < 6; ++q) s_wmax[warp][lane][q] = 0.0;
+            s_wzero[warp][lane] = 0;
+        }
+        __syncwarp();
+    };
+    auto flush = [&]() {
+        __syncwarp();
+        if (cur != nullptr && lane == 0) {
+            unsigned long long *maxb = cur->cnt->maxb;
+            for (int q = 0; q < 6; ++q) {
+                double m = s_wmax[warp][0][q];
+                for (uint32_t g = 1; g < OP_TILE; ++g) m = fmax(m, s_wmax[warp][g][q]);
+                atomic_max_pos(&maxb[q], m);
+            }
+            unsigned long long z = 0;
+            for (uint32_t g = 0; g < OP_TILE; ++g) z += s_wzero[warp][g];
+            if (z) atomicAdd(&maxb[7], z);
+        }
+        __syncwarp();
+        reset();
+        cur = nullptr;
+    };
+    reset();
+    constexpr uint32_t PER_LANE = OP_SHORT_K1 / 16;  // a row's elements per lane: one chunk
+    const size_t kp = G.kpmax;
+    const uint32_t tiles = (G.rows + OP_TILE - 1) / OP_TILE;
+    const uint32_t stride = gridDim.x * OP_WARPS;
+    for (uint32_t ti = blockIdx.x * OP_WARPS + warp; ti < tiles; ti += stride) {
+        const uint32_t gr0 = ti * OP_TILE;
+        const JobDev &J = jobs[G.job_ids[find_job(G.row_starts, G.njobs, gr0)]];
+        // uniform over the warp (a tile is of one job); longer rows are operand_kernel's
+        if (!job_active(J) || J.kp1 > OP_SHORT_K1) continue;
+        if (&J != cur) {
+            flush();
+            cur = &J;
+        }
+        const uint32_t d = J.d, kp1 = J.kp1;
+        // padding rows between jobs: zero operands (read only as masked rows/columns)
+        for (uint32_t p = 0; p < OP_TILE; ++p) {
+            const uint32_t gr = gr0 + p;
+            if (gr < G.rows && gr - J.row0 >= J.n) {
+                for (uint32_t t = lane; t < G.kpmax; t += 32) {
+                    if (G.elem_bytes == 4) {
+                        reinterpret_cast<uint32_t *>(G.opa)[(size_t)gr * G.kpmax + t] = 0u;
+                    } else {
+                        reinterpret_cast<uint16_t *>(G.opa)[(size_t)gr * G.kpmax + t] = 0;
+                        reinterpret_cast<uint16_t *>(G.opb)[(size_t)gr * G.kpmax + t] = 0;
+                    }
+                }
+            }
+        }
+        const bool euc = J.metric == HM_METRIC_EUCLIDEAN;
+        const uint32_t lpr = kp1 > 32 ? 16u : 8u;  // lanes per row
+        const uint32_t g = (uint32_t)lane / lpr, sl = (uint32_t)lane % lpr;
+        for (uint32_t p0 = 0; p0 < OP_TILE; p0 += 32 / lpr) {
+            const uint32_t gr = gr0 + p0 + g;
+            const uint32_t row = gr - J.row0;
+            const bool real = gr < G.rows && row < J.n;  // padding rows compute zeros, write nothing
+            double scale = 1.0;
+            bool zero_row = false;
+            if (euc) {
+                const double m = sqrt(__longlong_as_double((long long)J.cnt->maxb[6]));
+                if (m > 0.0) {
+                    int e;
+                    frexp(m, &e);  // m = f * 2^e, f in [0.5, 1)
+                    scale = ldexp(1.0, -e);
+                }
+            } else if (real) {
+                const double rn = J.rnorm[row];
+                zero_row = !(rn > 0.0);
+                scale = zero_row ? 0.0 : 1.0 / rn;
+            }
+            double uu = 0.0, ee = 0.0, rr = 0.0, aa = 0.0;
+            const float *xr = J.x + (size_t)(real ? row : 0u) * d;
+            // cosine rows are scaled by 1 / ||x|| (the operand u is whatever this
+            // arithmetic forms: the band is measured from it)
+            const double mul = scale;
+            for (uint32_t t0 = 0; t0 < kp1; t0 += lpr * PER_LANE) {
+                float xs[PER_LANE];
+#pragma unroll
+                for (uint32_t q = 0; q < PER_LANE; ++q) {
+                    const uint32_t t = t0 + lpr * q + sl;
+                    xs[q] = (real && t < d) ? __ldg(xr + t) : 0.0f;
+                }
+#pragma unroll
+                for (uint32_t q = 0; q < PER_LANE; ++q) {
+                    const uint32_t t = t0 + lpr * q + sl;
+                    if (t >= kp1) break;
+                    double u = 0.0;
+                    if (t < d) u = euc ? ((double)xs[q] - __ldg(J.mu + t)) * mul : (double)xs[q] * mul;
+                    uu += u * u;
+                    if (MODE == OP_TF32) {
+                        double r;
+                        const uint32_t b = to_tf32_bits(u, &r);
+                        if (real) reinterpret_cast<uint32_t *>(G.opa)[(size_t)gr * kp + t] = b;
+                        ee += (r - u) * (r - u);
+                        aa += r * r;
+                    } else if (MODE == OP_BF16) {
+                        double r;
+                        const uint16_t b = to_bf16_bits(u, &r);
+                        if (real) reinterpret_cast<uint16_t *>(G.opa)[(size_t)gr * kp + t] = b;
+                        ee += (r - u) * (r - u);
+                        aa += r * r;
+                    } else {
+                        double hi, lo;
+                        const uint16_t bh = to_bf16_bits(u, &hi);
+                        const uint16_t bl = to_bf16_bits(u - hi, &lo);
+                        const double res = (u - hi) - lo;
+                        if (real) {
+                            uint16_t *A = reinterpret_cast<uint16_t *>(G.opa) + (size_t)gr * kp;
+                            uint16_t *B = reinterpret_cast<uint16_t *>(G.opb) + (size_t)gr * kp;
+                            A[t] = bh;
+                            A[kp1 + t] = bh;
+                            A[2 * kp1 + t] = bl;
+                            B[t] = bh;
+                            B[kp1 + t] = bl;
+                            B[2 * kp1 + t] = bh;
+                        }
+                        ee += lo * lo;
+                        rr += res * res;
+                        aa += 2.0 * hi * hi + lo * lo;
+                    }
+                }
+            }
+            // the row's sums over its lpr lanes (xor partners stay in the group)
+#pragma unroll
+            for (uint32_t o = 8; o > 0; o >>= 1) {
+                if (o < lpr) {
+                    uu += __shfl_xor_sync(0xffffffffu, uu, o);
+                    ee += __shfl_xor_sync(0xffffffffu, ee, o);
+                    rr += __shfl_xor_sync(0xffffffffu, rr, o);
+                    aa += __shfl_xor_sync(0xffffffffu, aa, o);
+                }
+            }
+            if (sl == 0 && real) {
+                double *wmax = s_wmax[warp][p0 + g];
+                RowStat st;
+                st.unorm = sqrt(uu);
+                st.enorm = sqrt(ee);
+                st.rnorm = sqrt(rr);
+                st.anorm = sqrt(aa);
+                st.bnorm = st.anorm;  // both operand layouts have the same row norm
+                st.sqnorm = uu;
+                G.rowstat[gr] = st;
+                wmax[0] = fmax(wmax[0], st.unorm);
+                wmax[1] = fmax(wmax[1], st.enorm);
+                wmax[2] = fmax(wmax[2], st.rnorm);
+                wmax[3] = fmax(wmax[3], st.anorm);
+                wmax[4] = fmax(wmax[4], st.bnorm);
+                wmax[5] = fmax(wmax[5], st.sqnorm);
+                if (euc) {
+                    const float nsq = __double2float_rn(uu);
+                    G.rowterm[gr] = nsq;
+                    G.colterm[gr] = nsq;
+                } else {
+                    G.rowterm[gr] = 0.0f;
+                    G.colterm[gr] = zero_row ? 0.0f : 1.0f;
+                }
+                G.force[gr] = zero_row ? 1 : 0;
+                if (zero_row) ++s_wzero[warp][p0 + g];
+                G.rowthr[gr] = 0xff800000u;  // the row's shared threshold starts at +inf
+            }
+        }
+    }
+    flush();
+}
+
 // Keep band of one row (binary32 bits, rounded up), written to G.band.
 __device__ __forceinline__ uint32_t band_of_row(const JobDev &J, const GroupDev &G, uint32_t gr) {
     const unsigned long long *maxb = J.cnt->maxb;
@@ -330,17 +522,23 @@ int launch_screen_prep(const JobDev *jobs, const GroupDev &G, const GroupDev *Gd
     colmean_kernel<<<G.njobs, 128, 0, s>>>(jobs, Gd);
     // G.rows is a multiple of 32: 32 group rows per block
     centred_norm_max_kernel<<<G.rows / 32, 256, 0, s>>>(jobs, Gd);
-    const uint32_t op_blocks = (G.rows + OP_WARPS - 1) / OP_WARPS;
     const uint32_t op_cap = (uint32_t)device_sm_count() * OP_BLOCKS_PER_SM;
-    const uint32_t op_grid = op_blocks < op_cap ? op_blocks : op_cap;
+    const uint32_t row_blocks = (G.rows + OP_WARPS - 1) / OP_WARPS;
+    const uint32_t row_grid = row_blocks < op_cap ? row_blocks : op_cap;
+    const uint32_t tile_blocks = (G.rows + OP_WARPS * OP_TILE - 1) / (OP_WARPS * OP_TILE);
+    const uint32_t tile_grid = tile_blocks < op_cap ? tile_blocks : op_cap;
+    auto both = [&](auto rows_kernel, auto packed_kernel) {
+        if (G.any_long_rows) rows_kernel<<<row_grid, OP_WARPS * 32, 0, s>>>(jobs, Gd);
+        if (G.any_short_rows) packed_kernel<<<tile_grid, OP_WARPS * 32, 0, s>>>(jobs, Gd);
+    };
     if (G.kind == SCREEN_KIND_TF32)
-        operand_kernel<OP_TF32><<<op_grid, OP_WARPS * 32, 0, s>>>(jobs, Gd);
+        both(operand_kernel<OP_TF32>, operand_packed_kernel<OP_TF32>);
     else if (!G.split)
-        operand_kernel<OP_BF16><<<op_grid, OP_WARPS * 32, 0, s>>>(jobs, Gd);
+        both(operand_kernel<OP_BF16>, operand_packed_kernel<OP_BF16>);
     else
-        operand_kernel<OP_SPLIT><<<op_grid, OP_WARPS * 32, 0, s>>>(jobs, Gd);
+        both(operand_kernel<OP_SPLIT>, operand_packed_kernel<OP_SPLIT>);
     HM_CUDA_TRY(cudaGetLastError());
-    count_launch(4);
+    count_launch(3 + (G.any_long_rows ? 1 : 0) + (G.any_short_rows ? 1 : 0));
     return HM_OK;
 }
 
