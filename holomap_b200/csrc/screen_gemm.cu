@@ -2,7 +2,7 @@
 // accumulators, fused with the per-row thresholds and the candidate emission,
 // so the N x N similarity matrix never leaves the SM.
 //
-// One CTA per SM (persistent), 10 warps (18 in the full emission pass):
+// One CTA per SM (persistent), 10 warps (18 in the emission passes):
 //   warp 0     TMA producer: the unit's 128-row A block stays resident in
 //              shared memory when its K slices fit 96 KB (else it streams
 //              with B), 256-row B slices per stage (128-byte K slices, 128B
@@ -10,9 +10,10 @@
 //   warp 1     allocates 512 TMEM columns (two 128 x 256 fp32 accumulators)
 //              and issues tcgen05.mma (one thread) + tcgen05.commit,
 //   warps 2-   epilogue: each thread owns one query row (its TMEM lane) and
-//              one segment of every tile's 256 columns (half; a quarter in
-//              the full emission pass), read 32 columns at a time.
-// The full emission pass can also run in the 2-SM form: a cluster of two
+//              one segment of every tile's 256 columns (half, read 32 columns
+//              at a time, in the threshold pass; a quarter, read 16 columns
+//              at a time, in the emission passes).
+// The emission passes can also run in the 2-SM form: a cluster of two
 // CTAs shares each 256 x 256 tile (one tcgen05.mma.cta_group::2 of M = 256
 // issued by the leader CTA), each CTA holding its own 128 rows of A and
 // loading half of the column tile into an 8-stage ring.
