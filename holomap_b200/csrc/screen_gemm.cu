@@ -37,7 +37,8 @@
 // Every wait on an mbarrier is bounded (wall clock via %globaltimer and an
 // iteration cap): on expiry the CTA records an error code, stops issuing,
 // waits (bounded) for its own copies and MMAs, frees TMEM and returns.
-#include <atomic>
+#include <mutex>
+#include <vector>
 
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -927,17 +928,30 @@ __global__ void __launch_bounds__(sc_threads(PASS, KP), 1)
 
 }
 
-// clusters of two screen CTAs the device can hold at once (per device,
-// computed on first use; 0 until then)
-static uint32_t pair_slots(const void *func) {
-    static std::atomic<int> cache[64];  // clusters + 1
+// clusters of two CTAs of `func` (a screen kernel launched with `threads`
+// threads) the device can hold at once; computed on first use per kernel and
+// device, 0 when none fits
+static uint32_t pair_slots(const void *func, uint32_t threads) {
+    struct Entry {
+        const void *func;
+        int dev;
+        uint32_t clusters;
+    };
+    static std::mutex mu;
+    static std::vector<Entry> cache;
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 0;
-    const int hit = cache[dev].load(std::memory_order_relaxed);
-    if (hit > 0) return (uint32_t)(hit - 1);
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return 0;
+    }
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (const Entry &e : cache)
+            if (e.func == func && e.dev == dev) return e.clusters;
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(2 * (uint32_t)device_sm_count(), 1, 1);
-    cfg.blockDim = dim3(sc_threads(1), 1, 1);
+    cfg.blockDim = dim3(threads, 1, 1);
     cfg.dynamicSmemBytes = SC_SMEM_BYTES;
     cudaLaunchAttribute attr;
     attr.id = cudaLaunchAttributeClusterDimension;
@@ -951,7 +965,8 @@ static uint32_t pair_slots(const void *func) {
         (void)cudaGetLastError();
         return 0;
     }
-    cache[dev].store(clusters + 1, std::memory_order_relaxed);
+    std::lock_guard<std::mutex> lk(mu);
+    cache.push_back({func, dev, (uint32_t)clusters});
     return (uint32_t)clusters;
 }
 
@@ -962,7 +977,7 @@ static int launch_pair(const JobDev *jobs, const GroupDev &G, const CUtensorMap 
                        uint32_t idesc, cudaStream_t s) {
     const void *func = (const void *)screen_gemm_kernel<KIND, 32, PASS, true>;
     HM_TRY(ensure_dynamic_smem(func, (int)SC_SMEM_BYTES));
-    const uint32_t slots = pair_slots(func);
+    const uint32_t slots = pair_slots(func, (uint32_t)sc_threads(PASS));
     if (slots == 0) return set_error(HM_ERR_CUDA, "no room for a cluster of two screen CTAs");
     const uint32_t clusters = G.neunits < slots ? G.neunits : slots;
     if (clusters == 0) return HM_OK;
